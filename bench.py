@@ -1,0 +1,407 @@
+#!/usr/bin/env python
+"""Benchmark of the Tsetlin-machine hot path on B200.
+
+Metric: "TM train+predict samples/s" -- one step is one training epoch of a
+machine from its initial state (`train{iterations = 1}`, capi.c:1484) plus
+predict over the held-out set (capi.c:1088), the unit of work the
+reference's search driver repeats per trial epoch (optimize.lua:586-653).
+
+Default workload (N = 1): the large sparse classifier -- 20 classes, 16,384
+features (flip-packed to 32,768 literal bits, 4 KB per sample), 2,048
+clauses per class, specificity 25, target 200, clause_tolerance 64,
+clause_maximum 64, 8-bit state; 100,000 train and 20,000 test samples of
+Zipf(1.1) features at ~1.5 % density with per-class boosted subsets
+(synthetic, seeded; datagen.sparse_classifier).
+
+Arms:
+  default           the CUDA library through the C ABI (santoku_tsetlin)
+  --impl reference  the reference's CPU implementation of the same step on
+                    this host's cores: the reference's own capi.c/automata.h
+                    (oracle/_ref) where it was built, else the C restatement
+                    (oracle/), on a bounded sample of units, scaled.
+
+Under torchrun each rank trains its own replica of the machine (independent
+units, no data-path collective): weak scaling; `value` = all ranks' samples
+over the max-over-ranks device time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "lua-santoku-tsetlin_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+METRIC = "TM train+predict samples/s"
+UNIT = "samples/s"
+
+WORKLOADS = {
+    "c1": dict(
+        name="large-sparse-classifier", kind="classifier", classes=20, features=16384,
+        clauses=2048, clause_tolerance=64, clause_maximum=64, specificity=25.0, target=200,
+        n_train=100000, n_test=20000),
+    "c0": dict(
+        name="plain-classifier", kind="classifier", classes=10, features=784, clauses=256,
+        clause_tolerance=64, clause_maximum=64, specificity=10.0, target=50,
+        n_train=8000, n_test=2000),
+    "c2": dict(
+        name="encoder", kind="encoder", classes=256, features=4096, clauses=1024,
+        clause_tolerance=64, clause_maximum=64, specificity=15.0, target=100,
+        n_train=200000, n_test=20000),
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def make_data(w, rank=0):
+    from santoku_tsetlin import datagen
+    n = w["n_train"] + w["n_test"]
+    cache = "/tmp/tsetlin_b200_%s_%d_r%d.npz" % (w["name"], n, rank)
+    if os.path.exists(cache):
+        z = np.load(cache)
+        return {k: z[k] for k in z.files}
+    t = time.time()
+    if w["name"] == "large-sparse-classifier":
+        x, y = datagen.sparse_classifier(n, classes=w["classes"], features=w["features"],
+                                         seed=1 + 1000 * rank)
+        d = dict(x=x, y=y)
+    elif w["name"] == "plain-classifier":
+        x, y, _ = datagen.prototype_classifier(n, classes=w["classes"], features=w["features"],
+                                               seed=1 + 1000 * rank)
+        d = dict(x=x, y=y)
+    else:
+        x, c = datagen.latent_encoder(n, visible=w["features"], hidden=w["classes"],
+                                      seed=2 + 1000 * rank)
+        d = dict(x=x, codes=c)
+    log("data %s generated in %.1fs" % (w["name"], time.time() - t))
+    try:
+        np.savez(cache, **d)
+    except OSError:
+        pass
+    return d
+
+
+def create_table(w, seed):
+    t = dict(clauses=w["clauses"], clause_tolerance=w["clause_tolerance"],
+             clause_maximum=w["clause_maximum"], specificity=w["specificity"],
+             target=w["target"], seed=seed, reusable=True, device=0)
+    if w["kind"] == "classifier":
+        t.update(classes=w["classes"], features=w["features"])
+    else:
+        t.update(hidden=w["classes"], visible=w["features"])
+    return t
+
+
+def train_table(w, x, lab):
+    t = {"samples": w["n_train"], "iterations": 1}
+    if w["kind"] == "classifier":
+        t.update(problems=x, solutions=lab)
+    else:
+        t.update(sentences=x, codes=lab)
+    return t
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.path = "/tmp/tsetlin_b200_clocks_%d.csv" % os.getpid()
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [q.strip() for q in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's path on a bounded sample of units
+# ---------------------------------------------------------------------------
+def cpu_step(w, d, threads, budget_units=None):
+    """One step of the workload on the CPU, on a machine with the same rows
+    but fewer clauses per class (units are independent 8-clause chunks, so
+    per-unit work is unchanged), scaled to the full clause count.  Predict is
+    timed on a slice of the test set and scaled likewise."""
+    import oracle as O
+    which = "ref" if O.ref_available() else "oracle"
+    threads = threads or os.cpu_count()
+    units_per_class = max(1, min(w["clauses"] // 8, (2 * threads + w["classes"] - 1) // w["classes"]))
+    if budget_units:
+        units_per_class = max(1, min(units_per_class, budget_units // w["classes"]))
+    clauses = 8 * units_per_class
+    cfg = dict(type=w["kind"], classes=w["classes"], features=w["features"], clauses=clauses,
+               clause_tolerance=w["clause_tolerance"], clause_maximum=w["clause_maximum"],
+               specificity=w["specificity"], target=w["target"])
+    m = O.Machine(which=which, **cfg)
+    n = w["n_train"]
+    x = d["x"][:n]
+    kw = dict(labels=d["y"][:n]) if w["kind"] == "classifier" else dict(codes=d["codes"][:n])
+    t0 = time.perf_counter()
+    m.train(x.ravel(), n, 1, seed=0, mode=O.REFSTRUCT if which == "ref" else O.PHILOX,
+            threads=threads, **kw)
+    t_train = time.perf_counter() - t0
+    nt = min(w["n_test"], 2000)
+    xt = d["x"][n:n + nt]
+    t0 = time.perf_counter()
+    m.predict(xt.ravel(), nt, threads=threads)
+    t_pred = time.perf_counter() - t0
+    scale_units = (w["clauses"] // 8) / units_per_class
+    step_s = t_train * scale_units + t_pred * scale_units * (w["n_test"] / nt)
+    samples = w["n_train"] + w["n_test"]
+    sample = ("1 train epoch of %d of %d clauses per class (%d of %d units) over all %d "
+              "samples + predict of %d of %d test samples; times scaled by units and samples"
+              % (clauses, w["clauses"], units_per_class * w["classes"],
+                 (w["clauses"] // 8) * w["classes"], n, nt, w["n_test"]))
+    return dict(value=samples / step_s, step_s=step_s, kind="reference" if which == "ref" else "port",
+                cores=threads, sample=sample, measured_s=t_train + t_pred)
+
+
+# ---------------------------------------------------------------------------
+# arms
+# ---------------------------------------------------------------------------
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return ws, rank, local
+
+
+def run_reference(args, w):
+    ws, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return
+    d = make_data(w)
+    threads = os.cpu_count()
+    for _ in range(args.warmup if args.warmup < 1 else 1):
+        pass
+    vals = []
+    for _ in range(max(1, min(args.steps, 3))):
+        r = cpu_step(w, d, threads)
+        vals.append(r)
+    v = float(np.median([r["value"] for r in vals]))
+    step_s = float(np.median([r["step_s"] for r in vals]))
+    out = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws,
+        "steps": len(vals), "warmup": 0, "ms_per_step": step_s * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": config_of(w, ws),
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": vals[0]["cores"],
+                         "kind": vals[0]["kind"], "sample": vals[0]["sample"]},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def config_of(w, ws):
+    return {
+        "workload": w["name"], "type": w["kind"], "classes": w["classes"],
+        "features": w["features"], "literal_bits": 2 * w["features"], "clauses": w["clauses"],
+        "clause_tolerance": w["clause_tolerance"], "clause_maximum": w["clause_maximum"],
+        "specificity": w["specificity"], "target": w["target"], "state_bits": 8,
+        "n_train": w["n_train"], "n_test": w["n_test"],
+        "step": "train{iterations=1} from the initial state + predict(test)",
+        "parallelism": "replicas" if ws > 1 else "single",
+        "l2": "inputs larger than L2 (train set and automata exceed 126 MB)",
+    }
+
+
+def train_algorithmic_bytes(w, resident_units):
+    """Minimum DRAM bytes of one train launch: the automata read and written
+    once, plus each wave of resident units streaming the train set."""
+    rows = w["classes"] * w["clauses"]
+    wp = ((2 * w["features"] + 31) // 32 + 3) // 4 * 4
+    state = rows * 8 * wp * 4
+    units = rows // 8
+    waves = max(1, -(-units // max(1, resident_units)))
+    return 2 * state + waves * w["n_train"] * wp * 4
+
+
+def run_ours(args, w):
+    import torch
+    import santoku_tsetlin as tm
+    ws, rank, local = dist_init()
+    dev = torch.device("cuda", local if ws > 1 else 0)
+    torch.cuda.set_device(dev)
+    d = make_data(w, rank)
+    n, nt = w["n_train"], w["n_test"]
+    lab_key = "y" if w["kind"] == "classifier" else "codes"
+    # device-resident inputs (value) and pinned host inputs (e2e)
+    x_dev = torch.from_numpy(np.ascontiguousarray(d["x"][:n])).to(dev)
+    lab_dev = torch.from_numpy(np.ascontiguousarray(d[lab_key][:n])).to(dev)
+    xt_dev = torch.from_numpy(np.ascontiguousarray(d["x"][n:n + nt])).to(dev)
+    x_host = torch.from_numpy(np.ascontiguousarray(d["x"][:n])).pin_memory()
+    lab_host = torch.from_numpy(np.ascontiguousarray(d[lab_key][:n])).pin_memory()
+    xt_host = torch.from_numpy(np.ascontiguousarray(d["x"][n:n + nt])).pin_memory()
+    t = tm.create(w["kind"], create_table(w, seed=rank))
+    t.stats_enable(True)
+
+    def step_dev():
+        t.train(train_table(w, x_dev, lab_dev))
+        return t.predict(xt_dev, nt)
+
+    def step_host():
+        t.train(train_table(w, x_host.numpy(), lab_host.numpy()))
+        return t.predict(xt_host.numpy(), nt)
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def timed(fn, k):
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(k):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1)
+        if ws > 1:
+            import torch.distributed as dist
+            tt = torch.tensor([ms], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms = float(tt.item())
+        return ms
+
+    for _ in range(args.warmup):
+        step_dev()
+    t.reset_stats()
+    clocks = ClockSampler(dev.index)
+    clocks.start()
+    ms = timed(step_dev, args.steps)
+    ck = clocks.stop()
+    st = t.stats()
+    # end to end through the public API from pinned host buffers
+    step_host()
+    ms_e2e = timed(step_host, max(1, min(args.steps, 3)))
+    k_e2e = max(1, min(args.steps, 3))
+    samples = (n + nt) * ws
+    value = samples * args.steps / (ms / 1e3)
+    e2e_value = samples * k_e2e / (ms_e2e / 1e3)
+    peaks, peak_kind = measured_peaks()
+    # roofline of the dominant kernel (the fused train kernel), timed with CUDA
+    # events on the library's stream
+    occ_units = 2 * 148
+    alg = train_algorithmic_bytes(w, occ_units)
+    avg_ms = st["train_kernel_ms"] / max(1, st["train_launches"])
+    achieved = alg / (avg_ms / 1e3) / 1e9
+    wp = ((2 * w["features"] + 31) // 32 + 3) // 4 * 4
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": config_of(w, ws),
+        "e2e": {"value": e2e_value, "unit": UNIT,
+                "h2d_bytes_per_step": int(n * d["x"].shape[1] + d[lab_key][:n].nbytes +
+                                          nt * d["x"].shape[1]),
+                "d2h_bytes_per_step": int(nt * (8 if w["kind"] == "classifier"
+                                                else (w["classes"] + 7) // 8))},
+        "gpu_launches": int(st["kernel_launches"]),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                     "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                     "kernel": "k_train", "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": alg, "avg_launch_ms": avg_ms},
+        "kernels": {
+            "train_ms_per_step": st["train_kernel_ms"] / args.steps,
+            "predict_ms_per_step": st["predict_kernel_ms"] / args.steps,
+            "train_unit_steps": st["train_unit_steps"],
+            "literal_evals_per_s_train_upper": st["train_unit_steps"] * 8 * 32 * wp /
+                                               (st["train_kernel_ms"] / 1e3 + 1e-12),
+            "predict_literal_evals_per_s": nt * w["classes"] * w["clauses"] * 2 * w["features"] /
+                                           (st["predict_kernel_ms"] / max(1, st["predict_launches"]) / 1e3 + 1e-12),
+        },
+    }
+    if ck:
+        out["clocks"] = ck
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cb = cpu_step(w, d, os.cpu_count())
+        out["cpu_baseline"] = {"value": cb["value"], "unit": UNIT, "cores": cb["cores"],
+                               "kind": cb["kind"], "sample": cb["sample"]}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    t.destroy()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    w = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        run_reference(args, w)
+    else:
+        run_ours(args, w)
+
+
+if __name__ == "__main__":
+    main()

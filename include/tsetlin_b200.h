@@ -1,0 +1,221 @@
+/*
+ * tsetlin_b200 -- C ABI of the B200 (sm_100a) Tsetlin-machine classifier and
+ * encoder.
+ *
+ * Each entry point replaces one method of the reference's Lua module
+ * `santoku.tsetlin` (lib/santoku/tsetlin/capi.c).  The Lua binding a
+ * maintainer adds calls these with the same argument meaning and order; the
+ * citation beside each declaration names the reference function it stands
+ * in for.
+ *
+ * Conventions
+ *   - Every function returns TM_OK (0) or a negative TM_ERR_* code; the
+ *     message of the calling thread's last failure is tm_last_error().
+ *     Nothing longjmps (the reference raises Lua errors instead).
+ *   - Sizes are uint64_t.  Bit order is LSB-first within each byte and
+ *     features are aligned to tm_align() == 8 bits, as in the reference.
+ *   - Buffers belong to the caller.  `on_device` = 1 means the pointers are
+ *     CUDA device pointers on the machine's device; 0 means host memory.
+ *   - A machine lives on one device.  Calls on one machine are not
+ *     thread-safe; calls on different machines are.
+ */
+#ifndef TSETLIN_B200_H
+#define TSETLIN_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TM_OK 0
+#define TM_ERR_ARG (-1)      /* bad argument / size mismatch */
+#define TM_ERR_STATE (-2)    /* operation not valid for this machine */
+#define TM_ERR_CUDA (-3)     /* CUDA runtime failure */
+#define TM_ERR_OOM (-4)      /* allocation failed (host or device) */
+#define TM_ERR_IO (-5)       /* file or stream error */
+#define TM_ERR_DEVICE (-6)   /* a kernel reported an error status */
+
+#define TM_CLASSIFIER 0
+#define TM_ENCODER 1
+
+typedef struct tm_machine tm_machine;
+
+/* Creation parameters (capi.c:627-699).  For an encoder `classes` is
+ * `hidden` and `features` is `visible`. */
+typedef struct tm_params {
+  int32_t type;              /* TM_CLASSIFIER or TM_ENCODER */
+  uint32_t classes;          /* classes / hidden */
+  uint32_t features;         /* features / visible (unused when individualized) */
+  uint32_t clauses;          /* per class; rounded up to a multiple of 8 */
+  uint32_t clause_tolerance;
+  uint32_t clause_maximum;
+  uint32_t state_bits;       /* "state"; 0 means the default, 8 */
+  uint32_t include_bits;     /* 0 means the default, 1 */
+  double target;             /* < 0: sqrt(clauses / 2) * clause_tolerance */
+  double negative;           /* < 0: 1 / classes */
+  double specificity;
+  int32_t reusable;
+  int32_t individualized;
+  const int64_t *feat_offsets; /* classes + 1 entries when individualized */
+  uint64_t seed;             /* key of the Philox draw contract */
+  int32_t device;            /* CUDA device ordinal */
+} tm_params;
+
+/* Per-epoch callback: the reference's `each(epoch)` (capi.c:1168-1182).
+ * Return 0 to continue, non-zero to stop training (the reference stops on
+ * `false` or on an error raised by the callback). */
+typedef int (*tm_epoch_cb)(void *user, uint32_t epoch);
+
+/* Train arguments (capi.c:1116-1126, 1197-1214, 1288-1297, 1388-1398). */
+typedef struct tm_train_args {
+  uint64_t samples;
+  const uint8_t *problems;     /* classifier `problems` / encoder `sentences` */
+  const int64_t *solutions;    /* classifier labels */
+  const uint8_t *codes;        /* encoder target codes, ceil(hidden/8) B/sample */
+  const int64_t *dim_offsets;  /* individualized: byte offset of class h's block */
+  uint32_t iterations;
+  tm_epoch_cb each;
+  void *each_user;
+  int32_t on_device;           /* problems/solutions/codes are device pointers */
+  int32_t has_seed;            /* 1: use `seed` instead of the machine's */
+  uint64_t seed;
+} tm_train_args;
+
+/* Reconfigure arguments (capi.c:1590-1673). */
+typedef struct tm_reconfig {
+  uint32_t clauses;
+  uint32_t clause_tolerance;
+  uint32_t clause_maximum;
+  int64_t include_bits;        /* < 0: keep the current value */
+  double target;               /* < 0: default */
+  double specificity;
+} tm_reconfig;
+
+/* Fills defaults: state_bits 8, include_bits 1, target -1, negative -1. */
+void tm_params_init(tm_params *p);
+
+/* tsetlin.create("classifier"|"encoder", tbl): capi.c:701-716 */
+int tm_create(const tm_params *p, tm_machine **out);
+
+/* machine:train(tbl): capi.c:1484-1507 */
+int tm_train(tm_machine *m, const tm_train_args *a);
+
+/* Trains `count` independent machines in one persistent launch per epoch
+ * group.  Each machine trains exactly as tm_train would train it alone.
+ * Has no single counterpart in the reference: it batches the trials of one
+ * search round (optimize.lua:424-471, which calls capi.c:1484-1507 once per
+ * trial).  `args[i]` belongs to `machines[i]`; callbacks are not allowed
+ * here (use tm_train for per-epoch control). */
+int tm_train_batch(tm_machine *const *machines, const tm_train_args *args, uint32_t count);
+
+/* machine:predict(problems, n) / (problems, dim_offsets, n): capi.c:1088-1110.
+ * Classifier: out_classes[n] (int64, argmax, ties to the lowest class).
+ * Encoder: out_codes[n * ceil(hidden/8)]. */
+int tm_predict(tm_machine *m, const uint8_t *problems, const int64_t *dim_offsets, uint64_t n,
+               int64_t *out_classes, uint8_t *out_codes, int32_t on_device);
+
+/* Per-class vote sums, out_scores[n * classes] (int64): the `sums` /
+ * `votes` arrays of capi.c:924-933 and :968-981 before argmax / sign. */
+int tm_predict_scores(tm_machine *m, const uint8_t *problems, const int64_t *dim_offsets,
+                      uint64_t n, int64_t *out_scores, int32_t on_device);
+
+/* machine:persist(path): capi.c:1538-1562.  Byte-identical file layout. */
+int tm_persist(tm_machine *m, const char *path);
+/* machine:persist() returning a string: *data is malloc'd; release with tm_free. */
+int tm_persist_buf(tm_machine *m, uint8_t **data, uint64_t *len);
+void tm_free(void *p);
+
+/* tsetlin.load(data, from_string): capi.c:1751-1772.  from_string = 0:
+ * `data` is a NUL-terminated path and `len` is ignored. */
+int tm_load(const uint8_t *data, uint64_t len, int32_t from_string, int32_t device,
+            tm_machine **out);
+
+/* machine:checkpoint(cvec) / machine:restore(cvec): capi.c:1564-1588.
+ * The checkpoint is the reference's action bytes (action_chunks bytes).
+ * With buf == NULL, *len receives the size. */
+int tm_checkpoint(tm_machine *m, uint8_t *buf, uint64_t cap, uint64_t *len);
+int tm_restore(tm_machine *m, const uint8_t *buf, uint64_t len);
+
+/* machine:reconfigure(tbl): capi.c:1590-1673 */
+int tm_reconfigure(tm_machine *m, const tm_reconfig *r);
+
+/* machine:restrict(selected_dims): capi.c:752-901 */
+int tm_restrict(tm_machine *m, const int64_t *dims, uint64_t n);
+
+/* machine:type(): capi.c:1774-1788 -- TM_CLASSIFIER or TM_ENCODER */
+int tm_type(const tm_machine *m);
+
+/* machine:destroy() / __gc: capi.c:725-750 */
+void tm_destroy(tm_machine *m);
+
+const char *tm_last_error(void);
+
+/* tsetlin.align: capi.c:1801-1802 */
+uint32_t tm_align(void);
+
+/* Derived parameters, the fields of the reference's machine struct
+ * (capi.c:45-83): type, classes, features, clauses, clause_tolerance,
+ * clause_maximum, target, state_bits, include_bits, input_bits,
+ * input_chunks, clause_chunks, class_chunks, state_chunks, action_chunks,
+ * tail_mask, individualized, reusable, has_state. */
+#define TM_INFO_N 19
+int tm_get_info(const tm_machine *m, uint64_t *out);
+
+/* The machine's automata in the reference's byte layouts
+ * (automata.h:17-31; individualized: capi.c:568-597): actions
+ * [action_chunks] and count planes [state_chunks].  Either may be NULL. */
+int tm_export_state(tm_machine *m, uint8_t *actions, uint8_t *state);
+int tm_import_state(tm_machine *m, const uint8_t *actions, const uint8_t *state);
+
+/* ---- instrumentation ------------------------------------------------------ */
+/* Device-time accounting of the library's kernels for one machine, taken
+ * with CUDA events on the machine's own stream.  The reference's analogue
+ * is its perf build variant (make.perf.lua). */
+typedef struct tm_stats {
+  uint64_t train_launches;    /* fused train kernel launches */
+  double train_kernel_ms;     /* their summed device time */
+  uint64_t predict_launches;  /* predict (clause evaluation) kernel launches */
+  double predict_kernel_ms;
+  uint64_t kernel_launches;   /* every kernel the library launched */
+  uint64_t train_unit_steps;  /* (unit, sample) steps examined by train kernels */
+} tm_stats;
+/* on != 0 starts timing (events around every train / predict kernel). */
+int tm_stats_enable(tm_machine *m, int32_t on);
+int tm_get_stats(const tm_machine *m, tm_stats *out);
+int tm_reset_stats(tm_machine *m);
+
+/* ---- serving: resident machines, continuous batching ------------------- */
+/* No counterpart in the reference (its predict is one synchronous call per
+ * batch, capi.c:1088-1110).  A server keeps machines resident, accepts
+ * predict requests at any time, packs queued requests into shared device
+ * launches as slots and its device-memory budget allow, and completes each
+ * request with exactly the result tm_predict gives for it alone. */
+typedef struct tm_server tm_server;
+
+typedef struct tm_server_config {
+  uint64_t hbm_budget_bytes;   /* request staging memory (inputs + outputs) */
+  uint32_t max_inflight;       /* requests on the device at once */
+  uint32_t max_batch_samples;  /* samples packed into one launch */
+  int32_t device;
+} tm_server_config;
+
+int tm_serve_open(const tm_server_config *cfg, tm_machine *const *machines, uint32_t count,
+                  tm_server **out);
+/* Queues a request; the input is copied before return.  Returns a request
+ * id in *id.  Fails with TM_ERR_OOM if the request alone exceeds the
+ * budget. */
+int tm_serve_submit(tm_server *s, uint32_t machine, const uint8_t *problems, uint64_t n,
+                    uint64_t *id);
+/* Non-blocking: 1 when done (result copied to out_classes / out_codes),
+ * 0 while pending.  timeout_us > 0 waits up to that long. */
+int tm_serve_poll(tm_server *s, uint64_t id, int64_t *out_classes, uint8_t *out_codes,
+                  uint64_t timeout_us);
+/* submit -> done latency of a completed request, microseconds */
+int tm_serve_latency_us(tm_server *s, uint64_t id, double *us);
+int tm_serve_close(tm_server *s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,1160 @@
+// Host side of the C ABI (include/tsetlin_b200.h): machine lifecycle, data
+// staging, training orchestration, predict, persistence.  Device work is in
+// tm_kernels.cu; this file never computes a result on the CPU.
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/tsetlin_b200.h"
+#include "tm_internal.h"
+
+using namespace tmb;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_err;
+
+static int fail(int code, const char *fmt, ...) __attribute__((format(printf, 2, 3)));
+static int fail(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CK(call)                                                                      \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess)                                                            \
+      return fail(TM_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));      \
+  } while (0)
+
+extern "C" const char *tm_last_error(void) { return g_err.c_str(); }
+extern "C" uint32_t tm_align(void) { return 8; }
+extern "C" void tm_free(void *p) { free(p); }
+
+struct DevGuard {
+  int prev = -1;
+  explicit DevGuard(int d) {
+    cudaGetDevice(&prev);
+    if (prev != d) cudaSetDevice(d);
+  }
+  ~DevGuard() {
+    int cur;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+// Grow-only device buffer.
+struct DevBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t n) {
+    if (n <= cap) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = n < 256 ? 256 : n;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e == cudaSuccess) cap = want;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+  template <class T>
+  T *as() const { return (T *)p; }
+};
+
+// ---------------------------------------------------------------------------
+// machine
+// ---------------------------------------------------------------------------
+struct tm_machine {
+  int32_t type = TM_CLASSIFIER;
+  bool individualized = false, reusable = false, has_state = false, trained = false;
+  uint32_t classes = 0, features = 0, clauses = 0, tol = 0, maxlit = 0, target = 0;
+  uint32_t B = 8, ib = 1, input_bits = 0, input_chunks = 0, clause_chunks = 0;
+  uint32_t class_chunks = 0, state_chunks = 0, action_chunks = 0;
+  uint8_t tail_mask = 0xFF;
+  double negative = 0, specificity = 1;
+  uint64_t seed = 0;
+  int device = 0;
+  std::vector<uint64_t> feat_sizes;   // individualized
+  std::vector<uint32_t> n_chunks;     // per class reference row bytes
+  std::vector<ClassDev> cls;          // host copy of the class layout
+  uint64_t act_words = 0, cnt_words = 0;
+  uint32_t *d_act = nullptr, *d_cnt = nullptr;
+  ClassDev *d_cls = nullptr;
+  int32_t *d_lits = nullptr;
+  bool lits_valid = false;
+  cudaStream_t st = nullptr;
+  bool timing = false;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  tm_stats stats{};
+  DevBuf x, raw, labels, codes, perm, perm_scratch, sums, outc, work, tdev, cls_job, errf;
+};
+
+// Kernels launched by a CUB 64-bit radix sort of pairs: upsweep histogram,
+// exclusive scan and one onesweep pass per 8-bit digit.
+static const uint64_t kSortKernels = 10;
+
+static void note_launch(tm_machine *m, uint64_t k) { m->stats.kernel_launches += k; }
+
+static uint32_t derive_target(uint32_t clauses, uint32_t tol, double targetf) {
+  // capi.c:480-483 (fmaxf: single precision)
+  double t;
+  if (targetf < 0)
+    t = sqrt((double)clauses / 2.0) * (double)tol;
+  else
+    t = ceil(targetf >= 1 ? targetf : (double)fmaxf(1.0f, (float)((double)clauses * targetf)));
+  return (uint32_t)t;
+}
+
+// Per-class device layout (see ClassDev).
+static void layout_classes(tm_machine *m) {
+  const uint32_t C = m->classes;
+  m->cls.assign(C, ClassDev{});
+  m->n_chunks.assign(C, 0);
+  uint64_t ao = 0, co = 0;
+  const uint32_t mpl = m->B - 1;
+  for (uint32_t h = 0; h < C; h++) {
+    const uint64_t F = m->individualized ? m->feat_sizes[h] : m->features;
+    const uint64_t ibits = 2 * F;
+    const uint32_t nch = (uint32_t)((ibits + 7) / 8);
+    ClassDev &c = m->cls[h];
+    c.W = (nch + 3) / 4;
+    c.Wp = (c.W + 3) / 4 * 4;
+    c.input_bits = (uint32_t)ibits;
+    c.s_picks = (uint32_t)((double)(2 * F) / m->specificity);  // capi.c:181 / :347
+    const uint32_t lb = nch - 4 * (c.W - 1);
+    c.vmask = lb >= 4 ? 0xFFFFFFFFu : ((1u << (8 * lb)) - 1);
+    const uint32_t sh = 8 * (lb - 1);
+    const uint32_t tb = (uint32_t)(ibits & 7);
+    const uint32_t tmask = tb ? ((1u << tb) - 1) : 0xFFu;
+    c.emask = (c.vmask & ~(0xFFu << sh)) | (tmask << sh);
+    // the reference masks the action carry of the tail byte only on its byte
+    // path, which handles the tail when input_chunks % 16 != 0
+    c.amask = (nch % 16 != 0) ? c.emask : c.vmask;
+    c.act_off = ao;
+    c.cnt_off = co;
+    c.x_off = 0;
+    ao += (uint64_t)m->clauses * c.Wp;
+    co += (uint64_t)m->clauses * mpl * c.Wp;
+    m->n_chunks[h] = nch;
+  }
+  m->act_words = ao;
+  m->cnt_words = co;
+  uint64_t ta = 0;
+  for (uint32_t h = 0; h < C; h++) ta += (uint64_t)m->clauses * m->n_chunks[h];
+  m->action_chunks = (uint32_t)ta;
+  m->state_chunks = (uint32_t)(ta * mpl);
+}
+
+static void free_device(tm_machine *m) {
+  if (m->d_act) cudaFree(m->d_act);
+  if (m->d_cnt) cudaFree(m->d_cnt);
+  if (m->d_cls) cudaFree(m->d_cls);
+  if (m->d_lits) cudaFree(m->d_lits);
+  m->d_act = m->d_cnt = nullptr;
+  m->d_cls = nullptr;
+  m->d_lits = nullptr;
+}
+
+static int alloc_device(tm_machine *m, bool with_state) {
+  free_device(m);
+  CK(cudaMalloc(&m->d_act, std::max<uint64_t>(m->act_words, 4) * 4));
+  CK(cudaMemsetAsync(m->d_act, 0, std::max<uint64_t>(m->act_words, 4) * 4, m->st));
+  if (with_state) {
+    CK(cudaMalloc(&m->d_cnt, std::max<uint64_t>(m->cnt_words, 4) * 4));
+    CK(cudaMemsetAsync(m->d_cnt, 0, std::max<uint64_t>(m->cnt_words, 4) * 4, m->st));
+  }
+  CK(cudaMalloc(&m->d_cls, std::max<size_t>(m->classes, 1) * sizeof(ClassDev)));
+  CK(cudaMemcpyAsync(m->d_cls, m->cls.data(), m->classes * sizeof(ClassDev),
+                     cudaMemcpyHostToDevice, m->st));
+  CK(cudaMalloc(&m->d_lits, std::max<uint64_t>((uint64_t)m->classes * m->clauses, 1) * 4));
+  m->lits_valid = false;
+  m->has_state = with_state;
+  return TM_OK;
+}
+
+extern "C" void tm_params_init(tm_params *p) {
+  memset(p, 0, sizeof(*p));
+  p->state_bits = 8;
+  p->include_bits = 1;
+  p->target = -1;
+  p->negative = -1;
+}
+
+static int check_limits(tm_machine *m) {
+  for (uint32_t h = 0; h < m->classes; h++) {
+    const uint64_t F = m->individualized ? m->feat_sizes[h] : m->features;
+    if (F == 0) return fail(TM_ERR_ARG, "class %u has no features", h);
+    if (2 * F >= (1ull << 31)) return fail(TM_ERR_ARG, "too many features");
+    if ((uint64_t)m->clauses * m->tol >= (1ull << 31))
+      return fail(TM_ERR_ARG, "clauses * clause_tolerance must stay below 2^31");
+  }
+  if (m->B > 32) return fail(TM_ERR_ARG, "state above 32 bits is not supported");
+  return TM_OK;
+}
+
+extern "C" int tm_create(const tm_params *p, tm_machine **out) {
+  if (!p || !out) return fail(TM_ERR_ARG, "null argument");
+  *out = nullptr;
+  // capi.c:463-472
+  if (!p->classes) return fail(TM_ERR_ARG, "create: classes must be greater than 1");
+  if (!p->clauses) return fail(TM_ERR_ARG, "create: clauses must be greater than 0");
+  if (!p->clause_tolerance) return fail(TM_ERR_ARG, "create: clause_tolerance must be greater than 0");
+  if (!p->clause_maximum) return fail(TM_ERR_ARG, "create: clause_maximum must be greater than 0");
+  const uint32_t sb = p->state_bits ? p->state_bits : 8;
+  if (sb < 2) return fail(TM_ERR_ARG, "create: bits must be greater than 1");
+  if (!(p->specificity > 0)) return fail(TM_ERR_ARG, "create: specificity must be positive");
+  if (p->type != TM_CLASSIFIER && p->type != TM_ENCODER)
+    return fail(TM_ERR_ARG, "unexpected tsetlin machine type in create");
+  if (p->individualized && !p->feat_offsets)
+    return fail(TM_ERR_ARG, "create: feat_offsets must have classes + 1 elements");
+  tm_machine *m = new tm_machine();
+  m->type = p->type;
+  m->individualized = p->individualized != 0;
+  m->reusable = p->reusable != 0;
+  m->negative = p->negative < 0 ? 1.0 / (double)p->classes : p->negative;  // capi.c:474
+  m->classes = p->classes;
+  m->class_chunks = (p->classes + 7) / 8;
+  m->clauses = (p->clauses + 7) / 8 * 8;                                    // capi.c:477
+  m->tol = p->clause_tolerance;
+  m->maxlit = p->clause_maximum;
+  m->target = derive_target(m->clauses, m->tol, p->target);
+  m->B = sb;
+  m->ib = p->include_bits ? p->include_bits : 1;
+  m->specificity = p->specificity;
+  m->clause_chunks = m->clauses / 8;
+  m->seed = p->seed;
+  m->device = p->device;
+  if (m->individualized) {
+    // capi.c:528-606 leaves features, input_bits, input_chunks and tail_mask
+    // of an individualized machine unset (zero); they are persisted as such
+    m->tail_mask = 0;
+    for (uint32_t h = 0; h < m->classes; h++) {
+      const int64_t k = p->feat_offsets[h + 1] - p->feat_offsets[h];
+      if (k <= 0) {
+        delete m;
+        return fail(TM_ERR_ARG, "create: feat_offsets must be increasing");
+      }
+      m->feat_sizes.push_back((uint64_t)k);
+    }
+  } else {
+    m->features = p->features;
+    m->input_bits = 2 * m->features;                                         // capi.c:487
+    const uint32_t tb = m->input_bits & 7;
+    m->tail_mask = tb ? (uint8_t)((1u << tb) - 1) : 0xFF;
+    m->input_chunks = (m->input_bits + 7) / 8;
+  }
+  int rc = check_limits(m);
+  if (rc) {
+    delete m;
+    return rc;
+  }
+  layout_classes(m);
+  DevGuard g(m->device);
+  if (cudaStreamCreateWithFlags(&m->st, cudaStreamNonBlocking) != cudaSuccess) {
+    delete m;
+    return fail(TM_ERR_CUDA, "stream creation failed");
+  }
+  rc = alloc_device(m, true);
+  if (!rc) {
+    cudaError_t e = launch_setup(m->d_act, m->d_cnt, m->d_cls, m->classes, m->clauses, m->B,
+                                 m->act_words, m->st);
+    note_launch(m, 1);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(m->st);
+    if (e != cudaSuccess) rc = fail(TM_ERR_CUDA, "setup: %s", cudaGetErrorString(e));
+  }
+  if (rc) {
+    tm_destroy(m);
+    return rc;
+  }
+  *out = m;
+  return TM_OK;
+}
+
+extern "C" void tm_destroy(tm_machine *m) {
+  if (!m) return;
+  DevGuard g(m->device);
+  if (m->st) cudaStreamSynchronize(m->st);
+  free_device(m);
+  for (DevBuf *b : {&m->x, &m->raw, &m->labels, &m->codes, &m->perm, &m->perm_scratch, &m->sums,
+                    &m->outc, &m->work, &m->tdev, &m->cls_job, &m->errf})
+    b->release();
+  if (m->ev0) cudaEventDestroy(m->ev0);
+  if (m->ev1) cudaEventDestroy(m->ev1);
+  if (m->st) cudaStreamDestroy(m->st);
+  delete m;
+}
+
+extern "C" int tm_stats_enable(tm_machine *m, int32_t on) {
+  if (!m) return fail(TM_ERR_ARG, "null machine");
+  DevGuard g(m->device);
+  if (on && !m->ev0) {
+    CK(cudaEventCreate(&m->ev0));
+    CK(cudaEventCreate(&m->ev1));
+  }
+  m->timing = on != 0;
+  return TM_OK;
+}
+
+extern "C" int tm_get_stats(const tm_machine *m, tm_stats *out) {
+  if (!m || !out) return fail(TM_ERR_ARG, "null argument");
+  *out = m->stats;
+  return TM_OK;
+}
+
+extern "C" int tm_reset_stats(tm_machine *m) {
+  if (!m) return fail(TM_ERR_ARG, "null machine");
+  m->stats = tm_stats{};
+  return TM_OK;
+}
+
+extern "C" int tm_type(const tm_machine *m) { return m ? m->type : TM_ERR_ARG; }
+
+extern "C" int tm_get_info(const tm_machine *m, uint64_t *o) {
+  if (!m || !o) return fail(TM_ERR_ARG, "null argument");
+  o[0] = (uint64_t)m->type; o[1] = m->classes; o[2] = m->features; o[3] = m->clauses;
+  o[4] = m->tol; o[5] = m->maxlit; o[6] = m->target; o[7] = m->B; o[8] = m->ib;
+  o[9] = m->input_bits; o[10] = m->input_chunks; o[11] = m->clause_chunks;
+  o[12] = m->class_chunks; o[13] = m->state_chunks; o[14] = m->action_chunks;
+  o[15] = m->tail_mask; o[16] = m->individualized; o[17] = m->reusable; o[18] = m->has_state;
+  return TM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// staging of samples: reference byte rows -> padded device words
+// ---------------------------------------------------------------------------
+// Sets cls[h].x_off for an n-sample upload and returns the words needed.
+static uint64_t x_layout(tm_machine *m, uint64_t n, std::vector<ClassDev> &cls) {
+  cls = m->cls;
+  if (!m->individualized) return n * cls[0].Wp;
+  uint64_t off = 0;
+  for (uint32_t h = 0; h < m->classes; h++) {
+    cls[h].x_off = off;
+    off += n * cls[h].Wp;
+  }
+  return off;
+}
+
+static int stage_rows(tm_machine *m, DevBuf &dst, const uint8_t *src, const int64_t *dim_offsets,
+                      uint64_t n, bool on_device, std::vector<ClassDev> &cls) {
+  const uint64_t words = x_layout(m, n, cls);
+  CK(dst.ensure(std::max<uint64_t>(words, 4) * 4));
+  const uint32_t nblk = m->individualized ? m->classes : 1;
+  for (uint32_t h = 0; h < nblk; h++) {
+    const uint64_t nch = m->n_chunks[h];
+    const uint8_t *s = src + (m->individualized ? (uint64_t)dim_offsets[h] : 0);
+    const uint8_t *dsrc = s;
+    if (!on_device) {
+      CK(m->raw.ensure(std::max<uint64_t>(n * nch, 16)));
+      CK(cudaMemcpyAsync(m->raw.p, s, n * nch, cudaMemcpyHostToDevice, m->st));
+      dsrc = m->raw.as<uint8_t>();
+    }
+    CK(launch_repack(dsrc, n, nch, nch, dst.as<uint32_t>() + cls[h].x_off, cls[h].Wp, m->st));
+    note_launch(m, 1);
+    if (!on_device && m->individualized) CK(cudaStreamSynchronize(m->st));  // raw reuse
+  }
+  return TM_OK;
+}
+
+static int upload_cls(tm_machine *m, ClassDev *d, const std::vector<ClassDev> &cls) {
+  CK(cudaMemcpyAsync(d, cls.data(), cls.size() * sizeof(ClassDev), cudaMemcpyHostToDevice, m->st));
+  return TM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// training
+// ---------------------------------------------------------------------------
+static uint64_t neg_threshold(double negative) {
+  const double q = (1.0 - negative) * 4294967296.0;
+  if (!(q > 0)) return 0;
+  if (q >= 4294967296.0) return 4294967296ull;
+  return (uint64_t)floor(q);
+}
+
+struct TrainJob {
+  tm_machine *m;
+  const tm_train_args *a;
+  std::vector<ClassDev> cls;  // with x offsets
+  ClassDev *d_cls = nullptr;  // per-job class table (device)
+  uint32_t *d_x = nullptr;
+  int32_t *d_labels = nullptr;
+  uint8_t *d_codes = nullptr;
+  uint64_t seed = 0;
+};
+
+static TrainSmem plan_smem(uint32_t Wpmax, uint32_t Bmax, uint32_t smax, bool smem_state) {
+  TrainSmem L{};
+  uint32_t o = 0;
+  auto take = [&](uint32_t bytes) {
+    const uint32_t at = o;
+    o += (bytes + 127) / 128 * 128;
+    return at;
+  };
+  L.state_words = smem_state ? 8 * Bmax * Wpmax : 0;
+  L.state_off = take(L.state_words * 4);
+  L.ring_words = Wpmax;
+  L.ring_off = take(TM_RING * Wpmax * 4);
+  L.bar_off = take(TM_RING * 8);
+  L.list_off = take(TM_BATCH * 4 * 9);
+  L.votes_off = take(16 * 4);
+  L.ib_words = Wpmax;
+  L.ib_off = take(16 * Wpmax * 4);
+  L.ovf_cap = std::max<uint32_t>(1, smax / 4);
+  L.ovf_off = take(8 * L.ovf_cap * 4);
+  L.misc_off = take(32 * 4);
+  L.total = o;
+  return L;
+}
+
+static int num_sms(int dev) {
+  int v = 0;
+  cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+  return v > 0 ? v : 1;
+}
+
+static int max_smem_optin(int dev) {
+  int v = 0;
+  cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  return v > 0 ? v : 48 * 1024;
+}
+
+static int validate_train(tm_machine *m, const tm_train_args *a) {
+  if (!m || !a) return fail(TM_ERR_ARG, "null argument");
+  if (!m->has_state || !m->d_cnt)
+    return fail(TM_ERR_STATE, "can't train a model loaded without state");
+  if (a->samples >= (1ull << 31)) return fail(TM_ERR_ARG, "train: too many samples");
+  if (a->samples && !a->problems) return fail(TM_ERR_ARG, "train: problems missing");
+  if (m->type == TM_CLASSIFIER && a->samples && !a->solutions)
+    return fail(TM_ERR_ARG, "train: solutions missing");
+  if (m->type == TM_ENCODER && a->samples && !a->codes)
+    return fail(TM_ERR_ARG, "train: codes missing");
+  if (m->individualized && a->samples && !a->dim_offsets)
+    return fail(TM_ERR_ARG, "train: dim_offsets missing");
+  return TM_OK;
+}
+
+// Runs local epochs [e0, e1) of every job in one launch (units of all jobs
+// share the grid).  Permutations are built per job for those epochs.
+static int run_epochs(std::vector<TrainJob> &jobs, uint32_t e0, uint32_t e1, tm_machine *owner) {
+  tm_machine *m0 = owner;
+  cudaStream_t st = m0->st;
+  const int dev = m0->device;
+  // distinct (seed, n) -> permutation block
+  std::map<std::pair<uint64_t, uint64_t>, uint64_t> pidx;
+  uint64_t pwords = 0;
+  std::vector<uint64_t> joff(jobs.size());
+  for (size_t i = 0; i < jobs.size(); i++) {
+    auto key = std::make_pair(jobs[i].seed, (uint64_t)jobs[i].a->samples);
+    auto it = pidx.find(key);
+    if (it == pidx.end()) {
+      pidx[key] = pwords;
+      joff[i] = pwords;
+      pwords += (uint64_t)(e1 - e0) * jobs[i].a->samples;
+    } else {
+      joff[i] = it->second;
+    }
+  }
+  CK(m0->perm.ensure(std::max<uint64_t>(pwords, 4) * 4));
+  uint32_t maxn = 0;
+  for (auto &j : jobs) maxn = std::max<uint32_t>(maxn, (uint32_t)j.a->samples);
+  const size_t psb = perm_scratch_bytes(std::max<uint32_t>(maxn, 1));
+  CK(m0->perm_scratch.ensure(psb));
+  for (auto &kv : pidx) {
+    const uint64_t seed = kv.first.first, n = kv.first.second;
+    for (uint32_t e = e0; e < e1; e++) {
+      // the draw-contract epoch index is local epoch e (epoch_base 0)
+      CK(launch_perm(seed, e, (uint32_t)n, m0->perm.as<uint32_t>() + kv.second + (e - e0) * n,
+                     m0->perm_scratch.p, m0->perm_scratch.cap, st));
+      note_launch(m0, 1 + kSortKernels);
+    }
+  }
+  // machine table + work list
+  std::vector<TrainDev> td(jobs.size());
+  std::vector<WorkItem> work;
+  uint32_t Wpmax = 4, Bmax = 2, smax = 0;
+  for (size_t i = 0; i < jobs.size(); i++) {
+    TrainJob &J = jobs[i];
+    tm_machine *m = J.m;
+    TrainDev &t = td[i];
+    t.act = m->d_act;
+    t.cnt = m->d_cnt;
+    t.x = J.d_x;
+    t.labels = J.d_labels;
+    t.codes = J.d_codes;
+    t.perm = m0->perm.as<uint32_t>() + joff[i];
+    t.cls = J.d_cls;
+    t.seed = J.seed;
+    t.thr_neg = neg_threshold(m->negative);
+    t.n = (uint32_t)J.a->samples;
+    t.classes = m->classes;
+    t.clause_chunks = m->clause_chunks;
+    t.B = m->B;
+    t.ib = m->ib;
+    t.tol = m->tol;
+    t.maxlit = m->maxlit;
+    t.T = m->target;
+    t.type = (uint32_t)m->type;
+    t.code_bytes = m->class_chunks;
+    t.epochs = std::min<uint32_t>(J.a->iterations, e1);
+    t.epoch_base = 0;
+    if (t.n == 0 || t.epochs <= e0) continue;
+    for (uint32_t h = 0; h < m->classes; h++) {
+      const ClassDev &c = J.cls[h];
+      Wpmax = std::max(Wpmax, c.Wp);
+      smax = std::max(smax, c.s_picks);
+      const double frac =
+          m->type == TM_CLASSIFIER ? std::min(1.0, 1.0 / m->classes + m->negative) : 1.0;
+      const double cost = (double)t.n * (t.epochs - e0) * frac * c.Wp * m->B *
+                          (1.0 + c.s_picks / (32.0 * c.W));
+      for (uint32_t k = 0; k < m->clause_chunks; k++)
+        work.push_back(WorkItem{(uint32_t)i, h, k, (uint32_t)std::min(cost / 64.0, 4e9)});
+    }
+    Bmax = std::max(Bmax, m->B);
+  }
+  if (work.empty()) return TM_OK;
+  std::stable_sort(work.begin(), work.end(),
+                   [](const WorkItem &a, const WorkItem &b) { return a.cost > b.cost; });
+  const int optin = max_smem_optin(dev);
+  TrainSmem lay = plan_smem(Wpmax, Bmax, smax, true);
+  bool smem_state = (int)lay.total <= optin;
+  if (!smem_state) lay = plan_smem(Wpmax, Bmax, smax, false);
+  if ((int)lay.total > optin)
+    return fail(TM_ERR_ARG, "train: rows too wide for one CTA (%u bytes of shared memory)",
+                lay.total);
+  const int occ = train_occupancy(lay, smem_state, Bmax);
+  if (occ <= 0) return fail(TM_ERR_CUDA, "train: kernel cannot be resident (smem %u)", lay.total);
+  const int grid = (int)std::min<uint64_t>(work.size(), (uint64_t)num_sms(dev) * occ);
+  // device tables: [TrainDev...][WorkItem...][counter][err]
+  const size_t tb = td.size() * sizeof(TrainDev);
+  const size_t wb = work.size() * sizeof(WorkItem);
+  const size_t off_w = (tb + 255) & ~(size_t)255;
+  const size_t off_c = (off_w + wb + 255) & ~(size_t)255;
+  CK(m0->tdev.ensure(off_c + 256));
+  uint8_t *base = m0->tdev.as<uint8_t>();
+  CK(cudaMemcpyAsync(base, td.data(), tb, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(base + off_w, work.data(), wb, cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(base + off_c, 0, 8, st));
+  uint32_t *counter = (uint32_t *)(base + off_c);
+  uint32_t *err = counter + 1;
+  if (m0->timing) CK(cudaEventRecord(m0->ev0, st));
+  CK(launch_train((const TrainDev *)base, (const WorkItem *)(base + off_w), (uint32_t)work.size(),
+                  counter, e0, e1, lay, smem_state, Bmax, grid, err, st));
+  if (m0->timing) CK(cudaEventRecord(m0->ev1, st));
+  note_launch(m0, 1);
+  uint32_t herr = 0;
+  CK(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  m0->stats.train_launches++;
+  for (auto &J : jobs)
+    m0->stats.train_unit_steps += (uint64_t)J.m->classes * J.m->clause_chunks * J.a->samples *
+                                  (std::min<uint32_t>(J.a->iterations, e1) > e0
+                                       ? std::min<uint32_t>(J.a->iterations, e1) - e0 : 0);
+  if (m0->timing) {
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, m0->ev0, m0->ev1));
+    m0->stats.train_kernel_ms += ms;
+  }
+  if (herr) return fail(TM_ERR_DEVICE, "train: a sample copy did not complete (status %u)", herr);
+  return TM_OK;
+}
+
+static int prepare_job(TrainJob &J, DevBuf &xbuf, DevBuf &lbuf, DevBuf &cbuf, DevBuf &clsbuf) {
+  tm_machine *m = J.m;
+  const tm_train_args *a = J.a;
+  const uint64_t n = a->samples;
+  J.seed = a->has_seed ? a->seed : m->seed;
+  int rc = stage_rows(m, xbuf, a->problems, a->dim_offsets, n, a->on_device != 0, J.cls);
+  if (rc) return rc;
+  J.d_x = xbuf.as<uint32_t>();
+  CK(clsbuf.ensure(std::max<size_t>(m->classes, 1) * sizeof(ClassDev)));
+  J.d_cls = clsbuf.as<ClassDev>();
+  rc = upload_cls(m, J.d_cls, J.cls);
+  if (rc) return rc;
+  if (m->type == TM_CLASSIFIER) {
+    const uint64_t lab32 = (std::max<uint64_t>(n, 1) * 4 + 255) & ~255ull;
+    CK(lbuf.ensure(lab32 + std::max<uint64_t>(n, 1) * 8));
+    const int64_t *src = a->solutions;
+    int64_t *stage = (int64_t *)((uint8_t *)lbuf.p + lab32);
+    if (!a->on_device) {
+      CK(cudaMemcpyAsync(stage, src, n * 8, cudaMemcpyHostToDevice, m->st));
+      src = stage;
+    }
+    CK(launch_labels(src, lbuf.as<int32_t>(), n, m->st));
+    note_launch(m, 1);
+    J.d_labels = lbuf.as<int32_t>();
+  } else {
+    const uint64_t cb = n * m->class_chunks;
+    if (a->on_device) {
+      J.d_codes = (uint8_t *)a->codes;
+    } else {
+      CK(cbuf.ensure(std::max<uint64_t>(cb, 16)));
+      CK(cudaMemcpyAsync(cbuf.p, a->codes, cb, cudaMemcpyHostToDevice, m->st));
+      J.d_codes = cbuf.as<uint8_t>();
+    }
+  }
+  return TM_OK;
+}
+
+static int finish_train(tm_machine *m) {
+  m->lits_valid = false;
+  m->trained = true;
+  if (!m->reusable) {
+    // capi.c:1187-1188 / :718-723: a non-reusable machine drops its state
+    CK(cudaStreamSynchronize(m->st));
+    if (m->d_cnt) cudaFree(m->d_cnt);
+    m->d_cnt = nullptr;
+    m->has_state = false;
+  }
+  return TM_OK;
+}
+
+extern "C" int tm_train(tm_machine *m, const tm_train_args *a) {
+  int rc = validate_train(m, a);
+  if (rc) return rc;
+  DevGuard g(m->device);
+  std::vector<TrainJob> jobs(1);
+  jobs[0].m = m;
+  jobs[0].a = a;
+  rc = prepare_job(jobs[0], m->x, m->labels, m->codes, m->cls_job);
+  if (rc) return rc;
+  // capi.c:1136-1146: every train call starts from the initial state
+  cudaError_t e = launch_setup(m->d_act, m->d_cnt, m->d_cls, m->classes, m->clauses, m->B,
+                               m->act_words, m->st);
+  if (e != cudaSuccess) return fail(TM_ERR_CUDA, "setup: %s", cudaGetErrorString(e));
+  note_launch(m, 1);
+  const uint32_t E = a->iterations;
+  if (!a->each) {
+    // all epochs resident in one launch, in groups that bound the
+    // permutation buffer
+    const uint64_t n = std::max<uint64_t>(a->samples, 1);
+    const uint32_t group = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(E, (256ull << 20) / (4 * n)));
+    for (uint32_t e0 = 0; e0 < E; e0 += group) {
+      rc = run_epochs(jobs, e0, std::min(E, e0 + group), m);
+      if (rc) return rc;
+    }
+  } else {
+    for (uint32_t e0 = 0; e0 < E; e0++) {
+      rc = run_epochs(jobs, e0, e0 + 1, m);
+      if (rc) return rc;
+      m->lits_valid = false;
+      // capi.c:1168-1182: `each(epoch)`; false (non-zero here) stops
+      if (a->each(a->each_user, e0 + 1) != 0) break;
+    }
+  }
+  return finish_train(m);
+}
+
+extern "C" int tm_train_batch(tm_machine *const *ms, const tm_train_args *args, uint32_t count) {
+  if (!ms || !args) return fail(TM_ERR_ARG, "null argument");
+  if (count == 0) return TM_OK;
+  tm_machine *m0 = ms[0];
+  for (uint32_t i = 0; i < count; i++) {
+    int rc = validate_train(ms[i], &args[i]);
+    if (rc) return rc;
+    if (ms[i]->device != m0->device) return fail(TM_ERR_ARG, "train_batch: machines on different devices");
+    if (args[i].each) return fail(TM_ERR_ARG, "train_batch: per-epoch callbacks are not supported");
+    for (uint32_t k = 0; k < i; k++)
+      if (ms[k] == ms[i]) return fail(TM_ERR_ARG, "train_batch: machine listed twice");
+  }
+  DevGuard g(m0->device);
+  std::vector<TrainJob> jobs(count);
+  // identical inputs (same pointers, layout and size) are staged once
+  std::vector<int> same_x(count, -1);
+  for (uint32_t i = 0; i < count; i++) {
+    jobs[i].m = ms[i];
+    jobs[i].a = &args[i];
+    for (uint32_t k = 0; k < i; k++) {
+      const tm_train_args &A = args[k], &Bq = args[i];
+      if (A.problems == Bq.problems && A.samples == Bq.samples &&
+          A.dim_offsets == Bq.dim_offsets && A.on_device == Bq.on_device &&
+          !ms[k]->individualized && !ms[i]->individualized &&
+          ms[k]->input_chunks == ms[i]->input_chunks && ms[k]->type == ms[i]->type &&
+          A.solutions == Bq.solutions && A.codes == Bq.codes &&
+          ms[k]->class_chunks == ms[i]->class_chunks) {
+        same_x[i] = (int)k;
+        break;
+      }
+    }
+  }
+  for (uint32_t i = 0; i < count; i++) {
+    tm_machine *m = ms[i];
+    if (m->st != m0->st) CK(cudaStreamSynchronize(m->st));
+    TrainJob &J = jobs[i];
+    if (same_x[i] >= 0) {
+      const TrainJob &S = jobs[same_x[i]];
+      J.seed = args[i].has_seed ? args[i].seed : m->seed;
+      J.cls = m->cls;  // x offsets 0 (dense)
+      J.d_x = S.d_x;
+      J.d_labels = S.d_labels;
+      J.d_codes = S.d_codes;
+      CK(m->cls_job.ensure(std::max<size_t>(m->classes, 1) * sizeof(ClassDev)));
+      J.d_cls = m->cls_job.as<ClassDev>();
+      CK(cudaMemcpyAsync(J.d_cls, J.cls.data(), m->classes * sizeof(ClassDev),
+                         cudaMemcpyHostToDevice, m0->st));
+    } else {
+      // stage on machine i's buffers, ordered on the owner stream
+      cudaStream_t keep = m->st;
+      m->st = m0->st;
+      int rc = prepare_job(J, m->x, m->labels, m->codes, m->cls_job);
+      m->st = keep;
+      if (rc) return rc;
+    }
+    cudaError_t e = launch_setup(m->d_act, m->d_cnt, m->d_cls, m->classes, m->clauses, m->B,
+                                 m->act_words, m0->st);
+    if (e != cudaSuccess) return fail(TM_ERR_CUDA, "setup: %s", cudaGetErrorString(e));
+    note_launch(m0, 1);
+  }
+  uint32_t E = 0;
+  uint64_t maxn = 1;
+  for (uint32_t i = 0; i < count; i++) {
+    E = std::max(E, args[i].iterations);
+    maxn = std::max<uint64_t>(maxn, args[i].samples);
+  }
+  const uint32_t group = (uint32_t)std::max<uint64_t>(
+      1, std::min<uint64_t>(E, (512ull << 20) / (4 * maxn * std::max<uint32_t>(count, 1))));
+  for (uint32_t e0 = 0; e0 < E; e0 += group) {
+    int rc = run_epochs(jobs, e0, std::min(E, e0 + group), m0);
+    if (rc) return rc;
+  }
+  for (uint32_t i = 0; i < count; i++) {
+    int rc = finish_train(ms[i]);
+    if (rc) return rc;
+  }
+  return TM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// predict
+// ---------------------------------------------------------------------------
+static int ensure_lits(tm_machine *m) {
+  if (m->lits_valid) return TM_OK;
+  CK(launch_lits(m->d_act, m->d_cls, m->classes, m->clauses, m->d_lits, m->st));
+  note_launch(m, 1);
+  m->lits_valid = true;
+  return TM_OK;
+}
+
+static int predict_common(tm_machine *m, const uint8_t *problems, const int64_t *dim_offsets,
+                          uint64_t n, int64_t *out_classes, uint8_t *out_codes,
+                          int64_t *out_scores, bool on_device) {
+  if (!m) return fail(TM_ERR_ARG, "null machine");
+  if (n && !problems) return fail(TM_ERR_ARG, "predict: problems missing");
+  if (m->individualized && n && !dim_offsets) return fail(TM_ERR_ARG, "predict: dim_offsets missing");
+  if (n >= (1ull << 31)) return fail(TM_ERR_ARG, "predict: too many samples");
+  if (n == 0) return TM_OK;
+  DevGuard g(m->device);
+  std::vector<ClassDev> cls;
+  int rc = stage_rows(m, m->x, problems, dim_offsets, n, on_device, cls);
+  if (rc) return rc;
+  rc = upload_cls(m, m->d_cls, cls);
+  if (rc) return rc;
+  rc = ensure_lits(m);
+  if (rc) return rc;
+  const uint64_t sb = n * m->classes * 4;
+  CK(m->sums.ensure(sb));
+  CK(cudaMemsetAsync(m->sums.p, 0, sb, m->st));
+  if (m->timing) CK(cudaEventRecord(m->ev0, m->st));
+  CK(launch_predict(m->d_act, m->d_lits, m->d_cls, nullptr, m->classes, m->clauses, m->tol,
+                    m->x.as<uint32_t>(), (uint32_t)n, m->sums.as<int32_t>(), m->st));
+  if (m->timing) CK(cudaEventRecord(m->ev1, m->st));
+  note_launch(m, 1);
+  m->stats.predict_launches++;
+  // outputs
+  int64_t *dcls = nullptr, *dsc = nullptr;
+  uint8_t *dcod = nullptr;
+  const uint64_t clsb = n * 8, codb = n * m->class_chunks, scb = n * m->classes * 8;
+  if (on_device) {
+    dcls = out_classes;
+    dcod = out_codes;
+    dsc = out_scores;
+  } else {
+    CK(m->outc.ensure(clsb + codb + scb + 64));
+    uint8_t *p = m->outc.as<uint8_t>();
+    if (out_classes) dcls = (int64_t *)p;
+    if (out_codes) dcod = p + clsb;
+    if (out_scores) dsc = (int64_t *)(p + ((clsb + codb + 7) & ~7ull));
+  }
+  CK(launch_finalize(m->sums.as<int32_t>(), (uint32_t)n, m->classes, m->type, dcls, dcod, dsc,
+                     m->st));
+  note_launch(m, 1);
+  if (!on_device) {
+    if (out_classes) CK(cudaMemcpyAsync(out_classes, dcls, clsb, cudaMemcpyDeviceToHost, m->st));
+    if (out_codes) CK(cudaMemcpyAsync(out_codes, dcod, codb, cudaMemcpyDeviceToHost, m->st));
+    if (out_scores) CK(cudaMemcpyAsync(out_scores, dsc, scb, cudaMemcpyDeviceToHost, m->st));
+  }
+  CK(cudaStreamSynchronize(m->st));
+  if (m->timing) {
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, m->ev0, m->ev1));
+    m->stats.predict_kernel_ms += ms;
+  }
+  // restore the resident class table (x offsets of dense machines are 0)
+  if (m->individualized) {
+    rc = upload_cls(m, m->d_cls, m->cls);
+    if (rc) return rc;
+  }
+  return TM_OK;
+}
+
+int tmb_fail(int code, const char *msg) { return fail(code, "%s", msg); }
+
+int tmb_machine_view(tm_machine *m, MachineView *v) {
+  if (!m || !v) return fail(TM_ERR_ARG, "null argument");
+  if (m->individualized) return fail(TM_ERR_ARG, "serving takes dense (non-individualized) machines");
+  DevGuard g(m->device);
+  int rc = ensure_lits(m);
+  if (rc) return rc;
+  rc = upload_cls(m, m->d_cls, m->cls);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(m->st));
+  v->act = m->d_act;
+  v->lits = m->d_lits;
+  v->cls = m->d_cls;
+  v->classes = m->classes;
+  v->clauses = m->clauses;
+  v->tol = m->tol;
+  v->type = (uint32_t)m->type;
+  v->input_chunks = m->input_chunks;
+  v->Wp = m->cls[0].Wp;
+  v->class_chunks = m->class_chunks;
+  v->device = m->device;
+  return TM_OK;
+}
+
+extern "C" int tm_predict(tm_machine *m, const uint8_t *problems, const int64_t *dim_offsets,
+                          uint64_t n, int64_t *out_classes, uint8_t *out_codes, int32_t on_device) {
+  if (!m) return fail(TM_ERR_ARG, "null machine");
+  if (m->type == TM_CLASSIFIER && !out_classes) return fail(TM_ERR_ARG, "predict: out_classes missing");
+  if (m->type == TM_ENCODER && !out_codes) return fail(TM_ERR_ARG, "predict: out_codes missing");
+  return predict_common(m, problems, dim_offsets, n, m->type == TM_CLASSIFIER ? out_classes : nullptr,
+                        m->type == TM_ENCODER ? out_codes : nullptr, nullptr, on_device != 0);
+}
+
+extern "C" int tm_predict_scores(tm_machine *m, const uint8_t *problems, const int64_t *dim_offsets,
+                                 uint64_t n, int64_t *out_scores, int32_t on_device) {
+  if (!out_scores) return fail(TM_ERR_ARG, "predict_scores: out_scores missing");
+  return predict_common(m, problems, dim_offsets, n, nullptr, nullptr, out_scores, on_device != 0);
+}
+
+// ---------------------------------------------------------------------------
+// state in the reference byte layout
+// ---------------------------------------------------------------------------
+static int copy_rows(tm_machine *m, bool to_host, uint8_t *host, bool counts) {
+  const uint32_t planes = counts ? m->B - 1 : 1;
+  uint64_t ho = 0;
+  for (uint32_t h = 0; h < m->classes; h++) {
+    const ClassDev &c = m->cls[h];
+    const uint64_t rows = (uint64_t)m->clauses * planes;
+    uint32_t *dev = (counts ? m->d_cnt + c.cnt_off : m->d_act + c.act_off);
+    const size_t width = m->n_chunks[h];
+    if (to_host)
+      CK(cudaMemcpy2DAsync(host + ho, width, dev, (size_t)c.Wp * 4, width, rows,
+                           cudaMemcpyDeviceToHost, m->st));
+    else
+      CK(cudaMemcpy2DAsync(dev, (size_t)c.Wp * 4, host + ho, width, width, rows,
+                           cudaMemcpyHostToDevice, m->st));
+    ho += rows * width;
+  }
+  return TM_OK;
+}
+
+// For dense machines the per-class loop above covers classes * clauses rows
+// in one copy: the class blocks are contiguous with the same stride.
+static int copy_all(tm_machine *m, bool to_host, uint8_t *host, bool counts) {
+  if (m->individualized) return copy_rows(m, to_host, host, counts);
+  const uint32_t planes = counts ? m->B - 1 : 1;
+  const ClassDev &c = m->cls[0];
+  const uint64_t rows = (uint64_t)m->classes * m->clauses * planes;
+  uint32_t *dev = counts ? m->d_cnt : m->d_act;
+  const size_t width = m->input_chunks;
+  if (to_host)
+    CK(cudaMemcpy2DAsync(host, width, dev, (size_t)c.Wp * 4, width, rows, cudaMemcpyDeviceToHost,
+                         m->st));
+  else
+    CK(cudaMemcpy2DAsync(dev, (size_t)c.Wp * 4, host, width, width, rows, cudaMemcpyHostToDevice,
+                         m->st));
+  return TM_OK;
+}
+
+extern "C" int tm_export_state(tm_machine *m, uint8_t *actions, uint8_t *state) {
+  if (!m) return fail(TM_ERR_ARG, "null machine");
+  DevGuard g(m->device);
+  if (actions) {
+    int rc = copy_all(m, true, actions, false);
+    if (rc) return rc;
+  }
+  if (state) {
+    if (!m->d_cnt) return fail(TM_ERR_STATE, "machine has no state");
+    int rc = copy_all(m, true, state, true);
+    if (rc) return rc;
+  }
+  CK(cudaStreamSynchronize(m->st));
+  return TM_OK;
+}
+
+extern "C" int tm_import_state(tm_machine *m, const uint8_t *actions, const uint8_t *state) {
+  if (!m) return fail(TM_ERR_ARG, "null machine");
+  DevGuard g(m->device);
+  if (actions) {
+    int rc = copy_all(m, false, (uint8_t *)actions, false);
+    if (rc) return rc;
+    m->lits_valid = false;
+  }
+  if (state) {
+    if (!m->d_cnt) return fail(TM_ERR_STATE, "machine has no state");
+    int rc = copy_all(m, false, (uint8_t *)state, true);
+    if (rc) return rc;
+  }
+  CK(cudaStreamSynchronize(m->st));
+  return TM_OK;
+}
+
+// capi.c:1564-1576
+extern "C" int tm_checkpoint(tm_machine *m, uint8_t *buf, uint64_t cap, uint64_t *len) {
+  if (!m) return fail(TM_ERR_ARG, "null machine");
+  if (len) *len = m->action_chunks;
+  if (!buf) return TM_OK;
+  if (cap < m->action_chunks) return fail(TM_ERR_ARG, "failed to resize checkpoint buffer");
+  return tm_export_state(m, buf, nullptr);
+}
+
+// capi.c:1578-1588
+extern "C" int tm_restore(tm_machine *m, const uint8_t *buf, uint64_t len) {
+  if (!m || !buf) return fail(TM_ERR_ARG, "null argument");
+  if (len != m->action_chunks)
+    return fail(TM_ERR_ARG, "checkpoint size mismatch: expected %u bytes, got %llu",
+                m->action_chunks, (unsigned long long)len);
+  return tm_import_state(m, buf, nullptr);
+}
+
+// ---------------------------------------------------------------------------
+// persist / load (capi.c:1509-1562, 1675-1772) -- byte-identical layout
+// ---------------------------------------------------------------------------
+static int serialize(tm_machine *m, std::vector<uint8_t> &out) {
+  out.clear();
+  auto put = [&](const void *p, size_t n) {
+    const uint8_t *b = (const uint8_t *)p;
+    out.insert(out.end(), b, b + n);
+  };
+  const int32_t type = m->type;
+  put(&type, 4);
+  put(&m->classes, 4); put(&m->features, 4); put(&m->clauses, 4); put(&m->tol, 4);
+  put(&m->maxlit, 4); put(&m->target, 4); put(&m->B, 4); put(&m->ib, 4);
+  put(&m->input_bits, 4); put(&m->input_chunks, 4); put(&m->clause_chunks, 4);
+  put(&m->state_chunks, 4); put(&m->action_chunks, 4); put(&m->specificity, 8);
+  put(&m->tail_mask, 1);
+  const size_t at = out.size();
+  out.resize(at + m->action_chunks);
+  int rc = tm_export_state(m, out.data() + at, nullptr);
+  if (rc) return rc;
+  const uint8_t ind = m->individualized ? 1 : 0;
+  put(&ind, 1);
+  if (m->individualized) put(m->feat_sizes.data(), 8 * (size_t)m->classes);
+  return TM_OK;
+}
+
+extern "C" int tm_persist(tm_machine *m, const char *path) {
+  if (!m || !path) return fail(TM_ERR_ARG, "null argument");
+  std::vector<uint8_t> d;
+  int rc = serialize(m, d);
+  if (rc) return rc;
+  FILE *f = fopen(path, "wb");
+  if (!f) return fail(TM_ERR_IO, "persist: cannot open %s", path);
+  const size_t w = fwrite(d.data(), 1, d.size(), f);
+  const int c = fclose(f);
+  if (w != d.size() || c != 0) return fail(TM_ERR_IO, "persist: write failed");
+  return TM_OK;
+}
+
+extern "C" int tm_persist_buf(tm_machine *m, uint8_t **data, uint64_t *len) {
+  if (!m || !data || !len) return fail(TM_ERR_ARG, "null argument");
+  std::vector<uint8_t> d;
+  int rc = serialize(m, d);
+  if (rc) return rc;
+  *data = (uint8_t *)malloc(d.size() ? d.size() : 1);
+  if (!*data) return fail(TM_ERR_OOM, "persist: out of memory");
+  memcpy(*data, d.data(), d.size());
+  *len = d.size();
+  return TM_OK;
+}
+
+extern "C" int tm_load(const uint8_t *data, uint64_t len, int32_t from_string, int32_t device,
+                       tm_machine **out) {
+  if (!data || !out) return fail(TM_ERR_ARG, "null argument");
+  *out = nullptr;
+  std::vector<uint8_t> file;
+  if (!from_string) {
+    FILE *f = fopen((const char *)data, "rb");
+    if (!f) return fail(TM_ERR_IO, "load: cannot open %s", (const char *)data);
+    uint8_t buf[1 << 16];
+    size_t r;
+    while ((r = fread(buf, 1, sizeof(buf), f)) > 0) file.insert(file.end(), buf, buf + r);
+    fclose(f);
+    data = file.data();
+    len = file.size();
+  }
+  size_t o = 0;
+  auto get = [&](void *p, size_t n) {
+    if (o + n > len) return false;
+    memcpy(p, data + o, n);
+    o += n;
+    return true;
+  };
+  int32_t type;
+  tm_machine tmp;
+  uint32_t f4[13];
+  double spec;
+  uint8_t tail, ind;
+  if (!get(&type, 4)) return fail(TM_ERR_IO, "load: truncated model data");
+  if (type != TM_CLASSIFIER && type != TM_ENCODER)
+    return fail(TM_ERR_ARG, "unexpected tsetlin machine type in load");
+  for (int i = 0; i < 13; i++)
+    if (!get(&f4[i], 4)) return fail(TM_ERR_IO, "load: truncated model data");
+  if (!get(&spec, 8) || !get(&tail, 1)) return fail(TM_ERR_IO, "load: truncated model data");
+  const uint32_t ach = f4[12];
+  if (o + ach > len) return fail(TM_ERR_IO, "load: truncated model data");
+  const uint8_t *acts = data + o;
+  o += ach;
+  if (!get(&ind, 1)) return fail(TM_ERR_IO, "load: truncated model data");
+  tm_machine *m = new tm_machine();
+  m->type = type;
+  m->classes = f4[0]; m->features = f4[1]; m->clauses = f4[2]; m->tol = f4[3];
+  m->maxlit = f4[4]; m->target = f4[5]; m->B = f4[6]; m->ib = f4[7] ? f4[7] : 1;
+  m->input_bits = f4[8]; m->input_chunks = f4[9]; m->clause_chunks = f4[10];
+  m->specificity = spec;
+  m->tail_mask = tail;
+  m->class_chunks = (m->classes + 7) / 8;
+  m->individualized = ind != 0;
+  m->device = device;
+  m->negative = m->classes ? 1.0 / m->classes : 0;
+  if (m->B < 2 || m->B > 32 || !m->classes || m->clauses % 8 || m->clause_chunks * 8 != m->clauses) {
+    delete m;
+    return fail(TM_ERR_ARG, "load: inconsistent model header");
+  }
+  if (m->individualized) {
+    m->feat_sizes.resize(m->classes);
+    for (uint32_t h = 0; h < m->classes; h++)
+      if (!get(&m->feat_sizes[h], 8)) {
+        delete m;
+        return fail(TM_ERR_IO, "load: truncated model data");
+      }
+  }
+  layout_classes(m);
+  if (m->action_chunks != ach || m->state_chunks != f4[11]) {
+    delete m;
+    return fail(TM_ERR_ARG, "load: inconsistent model sizes");
+  }
+  DevGuard g(m->device);
+  if (cudaStreamCreateWithFlags(&m->st, cudaStreamNonBlocking) != cudaSuccess) {
+    delete m;
+    return fail(TM_ERR_CUDA, "stream creation failed");
+  }
+  // capi.c:1696: the state is not persisted; a loaded machine predicts only
+  int rc = alloc_device(m, false);
+  if (!rc) rc = tm_import_state(m, acts, nullptr);
+  if (rc) {
+    tm_destroy(m);
+    return rc;
+  }
+  m->trained = true;
+  *out = m;
+  return TM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// reconfigure (capi.c:1590-1673) and restrict (capi.c:752-901)
+// ---------------------------------------------------------------------------
+extern "C" int tm_reconfigure(tm_machine *m, const tm_reconfig *r) {
+  if (!m || !r) return fail(TM_ERR_ARG, "null argument");
+  if (!m->reusable) return fail(TM_ERR_STATE, "reconfigure requires reusable=true at creation time");
+  if (!r->clauses || !r->clause_tolerance || !r->clause_maximum || !(r->specificity > 0))
+    return fail(TM_ERR_ARG, "reconfigure: clauses, clause_tolerance, clause_maximum and specificity are required");
+  DevGuard g(m->device);
+  cudaStreamSynchronize(m->st);
+  tm_machine saved = *m;  // only the scalar fields are restored on failure
+  m->clauses = (r->clauses + 7) / 8 * 8;
+  m->clause_chunks = m->clauses / 8;
+  m->tol = r->clause_tolerance;
+  m->maxlit = r->clause_maximum;
+  const int64_t ib = r->include_bits < 0 ? (int64_t)m->ib : r->include_bits;
+  m->ib = ib ? (uint32_t)ib : 1;
+  m->specificity = r->specificity;
+  m->target = derive_target(m->clauses, m->tol, r->target);
+  int rc = check_limits(m);
+  if (rc) {
+    m->clauses = saved.clauses; m->clause_chunks = saved.clause_chunks; m->tol = saved.tol;
+    m->maxlit = saved.maxlit; m->ib = saved.ib; m->specificity = saved.specificity;
+    m->target = saved.target;
+    return rc;
+  }
+  layout_classes(m);
+  rc = alloc_device(m, true);  // actions zero (capi.c:1625), fresh state
+  if (rc) return rc;
+  m->trained = false;
+  CK(cudaStreamSynchronize(m->st));
+  return TM_OK;
+}
+
+extern "C" int tm_restrict(tm_machine *m, const int64_t *dims, uint64_t n) {
+  if (!m) return fail(TM_ERR_ARG, "null machine");
+  if (!m->individualized) return fail(TM_ERR_STATE, "restrict only supported for individualized TMs");
+  if (n == 0 || !dims) return fail(TM_ERR_ARG, "selected_dims cannot be empty");
+  for (uint64_t i = 0; i < n; i++) {
+    if (dims[i] < 0 || (uint64_t)dims[i] >= m->classes)
+      return fail(TM_ERR_ARG, "selected_dims[%d] = %d out of range [0, %d)", (int)i, (int)dims[i],
+                  (int)m->classes);
+    for (uint64_t j = i + 1; j < n; j++)
+      if (dims[i] == dims[j]) return fail(TM_ERR_ARG, "duplicate dimension %d in selected_dims", (int)dims[i]);
+  }
+  DevGuard g(m->device);
+  cudaStreamSynchronize(m->st);
+  const std::vector<ClassDev> old = m->cls;
+  uint32_t *oact = m->d_act, *ocnt = m->d_cnt;
+  m->d_act = nullptr;
+  m->d_cnt = nullptr;
+  const bool had_state = m->has_state && ocnt;
+  std::vector<uint64_t> nf(n);
+  for (uint64_t i = 0; i < n; i++) nf[i] = m->feat_sizes[dims[i]];
+  m->feat_sizes = nf;
+  m->classes = (uint32_t)n;
+  m->class_chunks = (m->classes + 7) / 8;
+  layout_classes(m);
+  int rc = alloc_device(m, had_state);
+  if (!rc) {
+    for (uint64_t i = 0; i < n; i++) {
+      const ClassDev &o = old[dims[i]], &c = m->cls[i];
+      cudaError_t e = cudaMemcpyAsync(m->d_act + c.act_off, oact + o.act_off,
+                                      (size_t)m->clauses * c.Wp * 4, cudaMemcpyDeviceToDevice, m->st);
+      if (e == cudaSuccess && had_state)
+        e = cudaMemcpyAsync(m->d_cnt + c.cnt_off, ocnt + o.cnt_off,
+                            (size_t)m->clauses * (m->B - 1) * c.Wp * 4, cudaMemcpyDeviceToDevice,
+                            m->st);
+      if (e != cudaSuccess) {
+        rc = fail(TM_ERR_CUDA, "restrict: %s", cudaGetErrorString(e));
+        break;
+      }
+    }
+  }
+  cudaStreamSynchronize(m->st);
+  if (oact) cudaFree(oact);
+  if (ocnt) cudaFree(ocnt);
+  return rc;
+}

@@ -1,0 +1,123 @@
+// Internal types shared by the host library (tm_api.cpp) and the kernels
+// (tm_kernels.cu).  Not part of the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace tmb {
+
+// Device layout of one class's automata and samples.  Every clause row of
+// the reference's byte layout (input_chunks bytes, automata.h:17-31) is held
+// as little-endian 32-bit words, padded to Wp words (a multiple of 4, so
+// each row starts on a 16-byte boundary for TMA bulk copies and 128-bit
+// loads).  Count planes are [clause][plane][Wp] -- the reference's order.
+struct ClassDev {
+  uint64_t act_off;    // words: first clause row of this class in act[]
+  uint64_t cnt_off;    // words: first clause's plane 0 in cnt[]
+  uint64_t x_off;      // words: this class's sample block in x[]
+  uint32_t W;          // words holding reference bytes
+  uint32_t Wp;         // padded row stride (words)
+  uint32_t input_bits; // 2 * features of this class
+  uint32_t s_picks;    // Type Ib picks per event, (unsigned)((double)(2F)/specificity)
+  uint32_t vmask;      // word W-1: bits of bytes that exist
+  uint32_t emask;      // word W-1: evaluation mask (tail byte & tail_mask)
+  uint32_t amask;      // word W-1: carry mask into the action plane
+  uint32_t pad;
+};
+
+// One machine of a training launch.
+struct TrainDev {
+  uint32_t *act;
+  uint32_t *cnt;
+  const uint32_t *x;        // padded sample rows
+  const int32_t *labels;    // classifier
+  const uint8_t *codes;     // encoder
+  const uint32_t *perm;     // [epochs][n] sample order
+  const ClassDev *cls;      // [classes]
+  uint64_t seed;
+  uint64_t thr_neg;         // skip a non-target sample iff draw < thr_neg
+  uint32_t n;
+  uint32_t classes;
+  uint32_t clause_chunks;   // chunks of 8 clauses per class
+  uint32_t B;               // state bits
+  uint32_t ib;              // include bits
+  uint32_t tol;
+  uint32_t maxlit;
+  uint32_t T;               // target
+  uint32_t type;            // 0 classifier, 1 encoder
+  uint32_t code_bytes;
+  uint32_t epochs;          // epochs this machine trains in this launch group
+  uint32_t epoch_base;      // draw-contract epoch index of local epoch 0
+};
+
+struct WorkItem {
+  uint32_t m;   // machine index in the launch
+  uint32_t h;   // class
+  uint32_t k;   // chunk within the class
+  uint32_t cost;
+};
+
+// Shared-memory plan of one training launch (byte offsets).
+struct TrainSmem {
+  uint32_t state_off, state_words;  // per-unit state copy (state_words == 0: global)
+  uint32_t ring_off, ring_words;    // sample ring: TM_RING slots of ring_words
+  uint32_t bar_off;                 // TM_RING mbarriers
+  uint32_t list_off;                // active-sample list
+  uint32_t votes_off;               // 2 x 8 votes
+  uint32_t ib_off, ib_words;        // per warp: 2 levels x ib_words
+  uint32_t ovf_off, ovf_cap;        // per warp: overflow entries
+  uint32_t misc_off;
+  uint32_t total;
+};
+
+constexpr int TM_TRAIN_THREADS = 256;  // 8 warps: warp j owns clause j of the unit
+constexpr int TM_RING = 4;             // sample ring depth
+constexpr int TM_BATCH = 256;          // samples examined per batch phase
+
+// Draw-contract stream words (4th Philox counter word).
+constexpr uint32_t ST_NEG = 0u;
+constexpr uint32_t ST_CH0 = 1u;
+constexpr uint32_t ST_CH1 = 2u;
+constexpr uint32_t ST_IB = 0x01000000u;
+constexpr uint32_t ST_PERM = 0xFFFFFFFFu;
+
+// ---- launchers (tm_kernels.cu) -------------------------------------------
+cudaError_t launch_repack(const uint8_t *src, uint64_t n, uint64_t row_bytes, uint64_t src_stride,
+                          uint32_t *dst, uint32_t dst_words, cudaStream_t st);
+cudaError_t launch_labels(const int64_t *src, int32_t *dst, uint64_t n, cudaStream_t st);
+cudaError_t launch_setup(uint32_t *act, uint32_t *cnt, const ClassDev *cls, uint32_t classes,
+                         uint32_t clauses, uint32_t B, uint64_t act_words, cudaStream_t st);
+cudaError_t launch_perm(uint64_t seed, uint32_t epoch, uint32_t n, uint32_t *out,
+                        void *scratch, size_t scratch_bytes, cudaStream_t st);
+size_t perm_scratch_bytes(uint32_t n);
+cudaError_t launch_train(const TrainDev *machines, const WorkItem *work, uint32_t nwork,
+                         uint32_t *counter, uint32_t e_begin, uint32_t e_end, const TrainSmem &lay,
+                         bool smem_state, uint32_t Bmax, int grid, uint32_t *err, cudaStream_t st);
+int train_occupancy(const TrainSmem &lay, bool smem_state, uint32_t Bmax);
+cudaError_t launch_lits(const uint32_t *act, const ClassDev *cls, uint32_t classes,
+                        uint32_t clauses, int32_t *lits, cudaStream_t st);
+cudaError_t launch_predict(const uint32_t *act, const int32_t *lits, const ClassDev *cls,
+                           const ClassDev *cls_host, uint32_t classes, uint32_t clauses,
+                           uint32_t tol, const uint32_t *x, uint32_t n, int32_t *sums,
+                           cudaStream_t st);
+cudaError_t launch_finalize(const int32_t *sums, uint32_t n, uint32_t classes, int32_t type,
+                            int64_t *out_classes, uint8_t *out_codes, int64_t *out_scores,
+                            cudaStream_t st);
+
+
+// Read-only view of a resident dense machine for the server (tm_serve.cpp).
+struct MachineView {
+  const uint32_t *act;
+  const int32_t *lits;
+  const ClassDev *cls;
+  uint32_t classes, clauses, tol, type, input_chunks, Wp, class_chunks;
+  int device;
+};
+
+}  // namespace tmb
+
+struct tm_machine;
+// Fills `v` (computing literal counts if needed).  Dense machines only.
+int tmb_machine_view(tm_machine *m, tmb::MachineView *v);
+int tmb_fail(int code, const char *msg);

@@ -1,0 +1,517 @@
+"""santoku.tsetlin on B200.
+
+A Python mirror of the reference's Lua module `santoku.tsetlin`
+(lib/santoku/tsetlin/capi.c:1790-1803 and the methods of capi.c:419-431),
+bound with ctypes to the C ABI of libtsetlin_b200.so
+(include/tsetlin_b200.h).  Names, table keys, argument order and error
+behaviour follow the reference:
+
+    import santoku_tsetlin as tm
+    t = tm.create("classifier", {"features": 784, "classes": 10, "clauses": 256,
+                                 "clause_tolerance": 64, "clause_maximum": 64,
+                                 "specificity": 10, "target": 50})
+    t.train({"samples": n, "problems": x, "solutions": y, "iterations": 10})
+    yhat = t.predict(x_test, n_test)
+    blob = t.persist()
+    t2 = tm.load(blob, True)
+
+All computation runs in the CUDA library; there is no CPU path.  Importing
+works without a GPU, creating a machine needs one.
+
+Inputs may be numpy arrays, bytes / bytearray, or torch tensors; CUDA
+tensors are passed to the library as device pointers.
+"""
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+from . import datagen  # noqa: F401  (workload generators)
+
+_PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(_PKG, "libtsetlin_b200.so")
+
+align = 8
+
+CLASSIFIER = 0
+ENCODER = 1
+
+
+class TsetlinError(RuntimeError):
+    """Raised where the reference raises a Lua error."""
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [
+        ("type", ctypes.c_int32),
+        ("classes", ctypes.c_uint32),
+        ("features", ctypes.c_uint32),
+        ("clauses", ctypes.c_uint32),
+        ("clause_tolerance", ctypes.c_uint32),
+        ("clause_maximum", ctypes.c_uint32),
+        ("state_bits", ctypes.c_uint32),
+        ("include_bits", ctypes.c_uint32),
+        ("target", ctypes.c_double),
+        ("negative", ctypes.c_double),
+        ("specificity", ctypes.c_double),
+        ("reusable", ctypes.c_int32),
+        ("individualized", ctypes.c_int32),
+        ("feat_offsets", ctypes.POINTER(ctypes.c_int64)),
+        ("seed", ctypes.c_uint64),
+        ("device", ctypes.c_int32),
+    ]
+
+
+EPOCH_CB = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_uint32)
+
+
+class _TrainArgs(ctypes.Structure):
+    _fields_ = [
+        ("samples", ctypes.c_uint64),
+        ("problems", ctypes.c_void_p),
+        ("solutions", ctypes.c_void_p),
+        ("codes", ctypes.c_void_p),
+        ("dim_offsets", ctypes.c_void_p),
+        ("iterations", ctypes.c_uint32),
+        ("each", EPOCH_CB),
+        ("each_user", ctypes.c_void_p),
+        ("on_device", ctypes.c_int32),
+        ("has_seed", ctypes.c_int32),
+        ("seed", ctypes.c_uint64),
+    ]
+
+
+class _Reconfig(ctypes.Structure):
+    _fields_ = [
+        ("clauses", ctypes.c_uint32),
+        ("clause_tolerance", ctypes.c_uint32),
+        ("clause_maximum", ctypes.c_uint32),
+        ("include_bits", ctypes.c_int64),
+        ("target", ctypes.c_double),
+        ("specificity", ctypes.c_double),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("train_launches", ctypes.c_uint64),
+        ("train_kernel_ms", ctypes.c_double),
+        ("predict_launches", ctypes.c_uint64),
+        ("predict_kernel_ms", ctypes.c_double),
+        ("kernel_launches", ctypes.c_uint64),
+        ("train_unit_steps", ctypes.c_uint64),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class _ServerConfig(ctypes.Structure):
+    _fields_ = [
+        ("hbm_budget_bytes", ctypes.c_uint64),
+        ("max_inflight", ctypes.c_uint32),
+        ("max_batch_samples", ctypes.c_uint32),
+        ("device", ctypes.c_int32),
+    ]
+
+
+_lib = None
+EXPORTS = (
+    "tm_params_init", "tm_create", "tm_train", "tm_train_batch", "tm_predict",
+    "tm_predict_scores", "tm_persist", "tm_persist_buf", "tm_free", "tm_load",
+    "tm_checkpoint", "tm_restore", "tm_reconfigure", "tm_restrict", "tm_type",
+    "tm_destroy", "tm_last_error", "tm_align", "tm_get_info", "tm_export_state",
+    "tm_import_state", "tm_stats_enable", "tm_get_stats", "tm_reset_stats", "tm_serve_open", "tm_serve_submit", "tm_serve_poll",
+    "tm_serve_latency_us", "tm_serve_close",
+)
+
+
+def lib():
+    """The loaded CUDA library.  Fails loudly when it was not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise TsetlinError(
+            "libtsetlin_b200.so is not built (run `make -C lua-santoku-tsetlin_b200/csrc`)")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, u64, u32, i32 = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int32
+    L.tm_params_init.argtypes = [ctypes.POINTER(_Params)]
+    L.tm_create.argtypes = [ctypes.POINTER(_Params), ctypes.POINTER(vp)]
+    L.tm_train.argtypes = [vp, ctypes.POINTER(_TrainArgs)]
+    L.tm_train_batch.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(_TrainArgs), u32]
+    L.tm_predict.argtypes = [vp, vp, vp, u64, vp, vp, i32]
+    L.tm_predict_scores.argtypes = [vp, vp, vp, u64, vp, i32]
+    L.tm_persist.argtypes = [vp, ctypes.c_char_p]
+    L.tm_persist_buf.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(u64)]
+    L.tm_free.argtypes = [vp]
+    L.tm_load.argtypes = [vp, u64, i32, i32, ctypes.POINTER(vp)]
+    L.tm_checkpoint.argtypes = [vp, vp, u64, ctypes.POINTER(u64)]
+    L.tm_restore.argtypes = [vp, vp, u64]
+    L.tm_reconfigure.argtypes = [vp, ctypes.POINTER(_Reconfig)]
+    L.tm_restrict.argtypes = [vp, vp, u64]
+    L.tm_type.argtypes = [vp]
+    L.tm_destroy.argtypes = [vp]
+    L.tm_destroy.restype = None
+    L.tm_last_error.restype = ctypes.c_char_p
+    L.tm_align.restype = u32
+    L.tm_get_info.argtypes = [vp, vp]
+    L.tm_export_state.argtypes = [vp, vp, vp]
+    L.tm_import_state.argtypes = [vp, vp, vp]
+    L.tm_stats_enable.argtypes = [vp, i32]
+    L.tm_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
+    L.tm_reset_stats.argtypes = [vp]
+    L.tm_serve_open.argtypes = [ctypes.POINTER(_ServerConfig), ctypes.POINTER(vp), u32,
+                                ctypes.POINTER(vp)]
+    L.tm_serve_submit.argtypes = [vp, u32, vp, u64, ctypes.POINTER(u64)]
+    L.tm_serve_poll.argtypes = [vp, u64, vp, vp, u64]
+    L.tm_serve_latency_us.argtypes = [vp, u64, ctypes.POINTER(ctypes.c_double)]
+    L.tm_serve_close.argtypes = [vp]
+    _lib = L
+    return L
+
+
+def _check(rc):
+    if rc < 0:
+        raise TsetlinError(lib().tm_last_error().decode())
+    return rc
+
+
+# ---------------------------------------------------------------------------
+# buffers
+# ---------------------------------------------------------------------------
+class _Buf:
+    """A pointer to caller data (kept alive), host or device."""
+
+    def __init__(self, obj, dtype):
+        self.keep = obj
+        self.device = False
+        if obj is None:
+            self.ptr = None
+            self.nbytes = 0
+            return
+        mod = type(obj).__module__
+        if mod.startswith("torch"):
+            t = obj.contiguous()
+            self.keep = t
+            self.device = bool(t.is_cuda)
+            self.ptr = t.data_ptr()
+            self.nbytes = t.numel() * t.element_size()
+            return
+        if isinstance(obj, (bytes, bytearray, memoryview)):
+            a = np.frombuffer(obj, dtype=np.uint8)
+            if dtype != np.uint8:
+                a = a.view(dtype)
+        else:
+            a = np.ascontiguousarray(obj)
+            if a.dtype != dtype:
+                a = a.astype(dtype)
+        self.keep = a
+        self.ptr = a.ctypes.data if a.size else None
+        self.nbytes = a.nbytes
+
+
+def _opt(tbl, key, default):
+    v = tbl.get(key, None) if tbl is not None else None
+    return default if v is None else v
+
+
+# ---------------------------------------------------------------------------
+# machine
+# ---------------------------------------------------------------------------
+INFO_KEYS = ("type", "classes", "features", "clauses", "clause_tolerance",
+             "clause_maximum", "target", "state_bits", "include_bits",
+             "input_bits", "input_chunks", "clause_chunks", "class_chunks",
+             "state_chunks", "action_chunks", "tail_mask", "individualized",
+             "reusable", "has_state")
+
+
+class Machine:
+    """A Tsetlin machine resident on one GPU (the reference's userdata,
+    metatable "santoku_tsetlin", capi.c:39, 419-431)."""
+
+    def __init__(self, handle, device=0):
+        self._h = ctypes.c_void_p(handle)
+        self.device = device
+
+    # -- bookkeeping -------------------------------------------------------
+    @property
+    def handle(self):
+        if not self._h:
+            raise TsetlinError("machine destroyed")
+        return self._h
+
+    def info(self):
+        o = np.zeros(19, dtype=np.uint64)
+        _check(lib().tm_get_info(self.handle, o.ctypes.data))
+        return {k: int(v) for k, v in zip(INFO_KEYS, o)}
+
+    def type(self):
+        """capi.c:1774-1788"""
+        return "classifier" if _check(lib().tm_type(self.handle)) == CLASSIFIER else "encoder"
+
+    def destroy(self):
+        """capi.c:744-750"""
+        if self._h:
+            lib().tm_destroy(self._h)
+            self._h = ctypes.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+    # -- train -------------------------------------------------------------
+    def _train_args(self, tbl):
+        info = self.info()
+        n = int(tbl["samples"])
+        if info["type"] == CLASSIFIER:
+            prob = _Buf(tbl["problems"], np.uint8)
+            sol = _Buf(tbl["solutions"], np.int64)
+            cod = _Buf(None, np.uint8)
+        else:
+            prob = _Buf(tbl["sentences"], np.uint8)
+            cod = _Buf(tbl["codes"], np.uint8)
+            sol = _Buf(None, np.int64)
+        dof = _Buf(tbl.get("dim_offsets"), np.int64)
+        if dof.device:
+            raise TsetlinError("dim_offsets must be host memory")
+        a = _TrainArgs()
+        a.samples = n
+        a.problems = prob.ptr
+        a.solutions = sol.ptr
+        a.codes = cod.ptr
+        a.dim_offsets = dof.ptr
+        a.iterations = int(tbl["iterations"])
+        a.on_device = 1 if prob.device else 0
+        if prob.device and ((sol.keep is not None and not sol.device) or
+                            (cod.keep is not None and not cod.device)):
+            raise TsetlinError("problems and labels must both be host or both device memory")
+        if "seed" in tbl and tbl["seed"] is not None:
+            a.has_seed = 1
+            a.seed = int(tbl["seed"])
+        return a, (prob, sol, cod, dof)
+
+    def train(self, tbl):
+        """capi.c:1484-1507.  `each(epoch)` returning False stops training;
+        an exception in `each` is reported on stderr and stops training, as
+        the reference does with a Lua error (capi.c:1171-1175)."""
+        a, keep = self._train_args(tbl)
+        each = tbl.get("each")
+        cb = None
+        if each is not None:
+            def _cb(_user, epoch):
+                try:
+                    r = each(int(epoch))
+                except Exception as e:  # noqa: BLE001
+                    sys.stderr.write("Error in callback: %s\n" % (e,))
+                    return 1
+                return 1 if r is False else 0
+            cb = EPOCH_CB(_cb)
+            a.each = cb
+        _check(lib().tm_train(self.handle, ctypes.byref(a)))
+        del keep, cb
+
+    # -- predict -----------------------------------------------------------
+    def predict(self, problems, *args):
+        """predict(problems, n) or, individualized, predict(problems,
+        dim_offsets, n) (capi.c:1088-1110).  Classifier: int64 class per
+        sample.  Encoder: uint8 codes, ceil(hidden/8) bytes per sample."""
+        dof, n = (None, args[0]) if len(args) == 1 else (args[0], args[1])
+        n = int(n)
+        info = self.info()
+        x = _Buf(problems, np.uint8)
+        d = _Buf(dof, np.int64)
+        if x.device:
+            import torch
+            dev = torch.device("cuda", self.device)
+            if info["type"] == CLASSIFIER:
+                out = torch.empty(n, dtype=torch.int64, device=dev)
+                _check(lib().tm_predict(self.handle, x.ptr, d.ptr, n, out.data_ptr(), None, 1))
+            else:
+                out = torch.empty(n * info["class_chunks"], dtype=torch.uint8, device=dev)
+                _check(lib().tm_predict(self.handle, x.ptr, d.ptr, n, None, out.data_ptr(), 1))
+            return out
+        if info["type"] == CLASSIFIER:
+            out = np.zeros(n, dtype=np.int64)
+            _check(lib().tm_predict(self.handle, x.ptr, d.ptr, n, out.ctypes.data, None, 0))
+        else:
+            out = np.zeros(n * info["class_chunks"], dtype=np.uint8)
+            _check(lib().tm_predict(self.handle, x.ptr, d.ptr, n, None, out.ctypes.data, 0))
+        return out
+
+    def predict_scores(self, problems, *args):
+        """Per-class vote sums (int64, n x classes) behind predict."""
+        dof, n = (None, args[0]) if len(args) == 1 else (args[0], args[1])
+        n = int(n)
+        C = self.info()["classes"]
+        x = _Buf(problems, np.uint8)
+        d = _Buf(dof, np.int64)
+        out = np.zeros((n, C), dtype=np.int64)
+        if x.device:
+            raise TsetlinError("predict_scores takes host inputs")
+        _check(lib().tm_predict_scores(self.handle, x.ptr, d.ptr, n, out.ctypes.data, 0))
+        return out
+
+    # -- persistence -------------------------------------------------------
+    def persist(self, path=None):
+        """capi.c:1538-1562: writes `path`, or returns the bytes."""
+        if path is not None:
+            _check(lib().tm_persist(self.handle, os.fsencode(path)))
+            return None
+        p = ctypes.c_void_p()
+        n = ctypes.c_uint64()
+        _check(lib().tm_persist_buf(self.handle, ctypes.byref(p), ctypes.byref(n)))
+        try:
+            return ctypes.string_at(p, n.value)
+        finally:
+            lib().tm_free(p)
+
+    def checkpoint(self, buf=None):
+        """capi.c:1564-1576: the action bytes.  Fills a bytearray in place
+        when one is given, else returns a new one."""
+        n = ctypes.c_uint64()
+        _check(lib().tm_checkpoint(self.handle, None, 0, ctypes.byref(n)))
+        if buf is None:
+            buf = bytearray(n.value)
+        elif len(buf) != n.value:
+            buf[:] = bytes(n.value)
+        a = (ctypes.c_uint8 * n.value).from_buffer(buf) if n.value else None
+        _check(lib().tm_checkpoint(self.handle, a, n.value, ctypes.byref(n)))
+        return buf
+
+    def restore(self, buf):
+        """capi.c:1578-1588"""
+        b = _Buf(bytes(buf), np.uint8)
+        _check(lib().tm_restore(self.handle, b.ptr, b.nbytes))
+
+    def reconfigure(self, tbl):
+        """capi.c:1590-1673"""
+        r = _Reconfig()
+        for k in ("clauses", "clause_tolerance", "clause_maximum", "specificity"):
+            if tbl.get(k) is None:
+                raise TsetlinError("reconfigure: %s is required" % k)
+        r.clauses = int(tbl["clauses"])
+        r.clause_tolerance = int(tbl["clause_tolerance"])
+        r.clause_maximum = int(tbl["clause_maximum"])
+        r.include_bits = int(_opt(tbl, "include_bits", -1))
+        r.target = float(_opt(tbl, "target", -1.0))
+        r.specificity = float(tbl["specificity"])
+        _check(lib().tm_reconfigure(self.handle, ctypes.byref(r)))
+
+    def restrict(self, dims):
+        """capi.c:752-901"""
+        d = _Buf(dims, np.int64)
+        _check(lib().tm_restrict(self.handle, d.ptr, d.nbytes // 8))
+
+    # -- instrumentation ---------------------------------------------------
+    def stats_enable(self, on=True):
+        _check(lib().tm_stats_enable(self.handle, 1 if on else 0))
+
+    def stats(self):
+        st = Stats()
+        _check(lib().tm_get_stats(self.handle, ctypes.byref(st)))
+        return st.as_dict()
+
+    def reset_stats(self):
+        _check(lib().tm_reset_stats(self.handle))
+
+    # -- raw state (reference byte layouts) --------------------------------
+    def export_state(self):
+        info = self.info()
+        a = np.zeros(info["action_chunks"], dtype=np.uint8)
+        s = np.zeros(info["state_chunks"], dtype=np.uint8) if info["has_state"] else None
+        _check(lib().tm_export_state(self.handle, a.ctypes.data,
+                                     None if s is None else s.ctypes.data))
+        return a, s
+
+    def import_state(self, actions=None, state=None):
+        a = _Buf(actions, np.uint8)
+        s = _Buf(state, np.uint8)
+        _check(lib().tm_import_state(self.handle, a.ptr, s.ptr))
+
+
+def _params(type_, tbl):
+    p = _Params()
+    lib().tm_params_init(ctypes.byref(p))
+    if type_ == "classifier":
+        p.type = CLASSIFIER
+        p.classes = int(tbl["classes"])
+        p.features = int(_opt(tbl, "features", 0))
+    elif type_ == "encoder":
+        p.type = ENCODER
+        p.classes = int(tbl["hidden"])
+        p.features = int(_opt(tbl, "visible", 0))
+    else:
+        raise TsetlinError("unexpected tsetlin machine type in create")
+    for k in ("clauses", "clause_tolerance", "clause_maximum", "specificity"):
+        if tbl.get(k) is None:
+            raise TsetlinError("create %s: %s is required" % (type_, k))
+    p.clauses = int(tbl["clauses"])
+    p.clause_tolerance = int(tbl["clause_tolerance"])
+    p.clause_maximum = int(tbl["clause_maximum"])
+    p.state_bits = int(_opt(tbl, "state", 8))
+    p.include_bits = int(_opt(tbl, "include_bits", 1))
+    p.target = float(_opt(tbl, "target", -1.0))
+    p.negative = float(_opt(tbl, "negative", -1.0))
+    p.specificity = float(tbl["specificity"])
+    p.reusable = 1 if tbl.get("reusable") else 0
+    p.individualized = 1 if tbl.get("individualized") else 0
+    keep = None
+    if p.individualized:
+        fo = np.ascontiguousarray(tbl["feat_offsets"], dtype=np.int64)
+        if len(fo) != p.classes + 1:
+            raise TsetlinError("create %s: feat_offsets must have classes + 1 elements" % type_)
+        keep = fo
+        p.feat_offsets = fo.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+    p.seed = int(_opt(tbl, "seed", 0))
+    p.device = int(_opt(tbl, "device", 0))
+    return p, keep
+
+
+def create(type_, tbl):
+    """tsetlin.create("classifier"|"encoder", tbl) (capi.c:701-716)."""
+    p, keep = _params(type_, tbl)
+    h = ctypes.c_void_p()
+    _check(lib().tm_create(ctypes.byref(p), ctypes.byref(h)))
+    del keep
+    return Machine(h.value, p.device)
+
+
+def classifier(tbl):
+    return create("classifier", tbl)
+
+
+def encoder(tbl):
+    return create("encoder", tbl)
+
+
+def load(data, from_string=False, device=0):
+    """tsetlin.load(path) / tsetlin.load(data, true) (capi.c:1751-1772)."""
+    h = ctypes.c_void_p()
+    if from_string:
+        b = bytes(data)
+        _check(lib().tm_load(b, len(b), 1, device, ctypes.byref(h)))
+    else:
+        _check(lib().tm_load(os.fsencode(data), 0, 0, device, ctypes.byref(h)))
+    return Machine(h.value, device)
+
+
+def train_batch(machines, tbls):
+    """Train many machines in one persistent launch; each ends exactly as
+    its own train(tbl) would leave it."""
+    if len(machines) != len(tbls):
+        raise TsetlinError("train_batch: one table per machine")
+    arr = (_TrainArgs * len(tbls))()
+    keeps = []
+    for i, (m, t) in enumerate(zip(machines, tbls)):
+        if t.get("each") is not None:
+            raise TsetlinError("train_batch: per-epoch callbacks are not supported")
+        a, keep = m._train_args(t)
+        arr[i] = a
+        keeps.append(keep)
+    hs = (ctypes.c_void_p * len(machines))(*[m.handle.value for m in machines])
+    _check(lib().tm_train_batch(hs, arr, len(machines)))
+    del keeps

@@ -63,9 +63,15 @@ def sparse_classifier(n, classes=20, features=16384, density=0.015, zipf=1.1, bo
     1)."""
     srng = np.random.default_rng(seed + 104729 if spec_seed is None else spec_seed)
     rank = srng.permutation(features)
-    p = 1.0 / np.power(rank + 1.0, zipf)
-    p = p * (density * features / p.sum())
-    p = np.minimum(p, 1.0)
+    base = 1.0 / np.power(rank + 1.0, zipf)
+    lo, hi = 0.0, 1.0 / base.min()
+    for _ in range(100):  # scale so that the clipped mean is `density`
+        mid = 0.5 * (lo + hi)
+        if np.minimum(base * mid, 1.0).mean() < density:
+            lo = mid
+        else:
+            hi = mid
+    p = np.minimum(base * hi, 1.0)
     boosts = [srng.choice(features, size=subset, replace=False) for _ in range(classes)]
     pc = np.repeat(p[None, :], classes, axis=0)
     for c in range(classes):

@@ -1,0 +1,74 @@
+"""The C ABI library, without a GPU: it builds for sm_100a, loads, exports
+every entry point include/tsetlin_b200.h declares, and its host-side
+argument checks answer the way the reference's do (capi.c:463-472,
+1487, 1593, 757-775) before any device work."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "tsetlin_b200.h")
+CSRC = os.path.join(ROOT, "lua-santoku-tsetlin_b200", "csrc")
+LIB = os.path.join(ROOT, "lua-santoku-tsetlin_b200", "libtsetlin_b200.so")
+
+
+@pytest.fixture(scope="module")
+def so():
+    if not os.path.exists(LIB):
+        subprocess.run(["make", "-s", "-C", CSRC], check=True)
+    return ctypes.CDLL(LIB)
+
+
+def declared():
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(tm_[a-z_0-9]+)\s*\(", txt)))
+
+
+def test_exports_every_declared_symbol(so):
+    names = declared()
+    assert "tm_create" in names and "tm_train" in names and "tm_predict" in names
+    missing = [n for n in names if not hasattr(so, n)]
+    assert not missing, missing
+
+
+def test_python_mirror_lists_every_declared_symbol():
+    import santoku_tsetlin as tm
+    assert set(declared()) == set(tm.EXPORTS)
+
+
+def test_align_and_errors_without_gpu(so):
+    import santoku_tsetlin as tm
+    assert tm.lib().tm_align() == 8 == tm.align
+    bad = [
+        ({"classes": 0}, "classes"),
+        ({"clauses": 0}, "clauses"),
+        ({"clause_tolerance": 0}, "clause_tolerance"),
+        ({"clause_maximum": 0}, "clause_maximum"),
+        ({"state": 1}, "bits"),
+    ]
+    base = dict(classes=2, features=8, clauses=8, clause_tolerance=4, clause_maximum=4,
+                specificity=2.0)
+    for override, word in bad:
+        t = dict(base, **override)
+        with pytest.raises(tm.TsetlinError, match=word):
+            tm.create("classifier", t)
+    with pytest.raises(tm.TsetlinError, match="unexpected tsetlin machine type"):
+        tm.create("regressor", base)
+    with pytest.raises(tm.TsetlinError, match="feat_offsets"):
+        tm.create("encoder", dict(hidden=3, clauses=8, clause_tolerance=4, clause_maximum=4,
+                                  specificity=2.0, individualized=True,
+                                  feat_offsets=np.array([0, 1, 2])))
+
+
+def test_load_rejects_bad_data(so):
+    import santoku_tsetlin as tm
+    with pytest.raises(tm.TsetlinError, match="unexpected tsetlin machine type"):
+        tm.load(np.array([7, 0, 0, 0], dtype=np.uint8).tobytes(), True)
+    with pytest.raises(tm.TsetlinError, match="truncated"):
+        tm.load(np.array([0, 0, 0, 0, 1, 0], dtype=np.uint8).tobytes(), True)
+    with pytest.raises(tm.TsetlinError, match="cannot open"):
+        tm.load("/nonexistent/model.bin")

@@ -1,0 +1,285 @@
+"""Parity of the CUDA path (through the C ABI) with the reference.
+
+* Every golden fixture made from the reference's own capi.c/automata.h
+  (tests/golden/make_golden.py): after training under the Philox draw
+  contract the device automata, vote sums, predictions and persisted bytes
+  are bit-identical.
+* Larger machines against the CPU oracle (itself pinned to the fixtures).
+* API behaviour of the reference: each-callback stop, persist/load,
+  checkpoint/restore, reconfigure, restrict, device-pointer inputs.
+"""
+import hashlib
+import os
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+from cases import CASES, make_inputs  # noqa: E402
+
+import oracle as O  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+PHILOX_CASES = [c for c in CASES if not c["train"].get("refstruct")]
+
+
+def ref_table(create, seed=0, reusable=True):
+    """Oracle-style create kwargs -> the reference's Lua table keys."""
+    c = dict(create)
+    kind = c.pop("type")
+    t = {}
+    if kind == "encoder":
+        t["hidden"] = c.pop("classes")
+        if "features" in c:
+            t["visible"] = c.pop("features")
+    for k, v in c.items():
+        t[k] = v
+    t["reusable"] = reusable
+    t["seed"] = seed
+    return kind, t
+
+
+def train_table(kind, inp, epochs, seed=None):
+    t = {"samples": inp["n"], "iterations": epochs}
+    if kind == "classifier":
+        t["problems"], t["solutions"] = inp["x"], inp["labels"]
+    else:
+        t["sentences"], t["codes"] = inp["x"], inp["codes"]
+    if inp.get("dim_offsets") is not None:
+        t["dim_offsets"] = inp["dim_offsets"]
+    if seed is not None:
+        t["seed"] = seed
+    return t
+
+
+def load_fixture(name):
+    z = np.load(os.path.join(HERE, "golden", name + ".npz"))
+    return {k: z[k] for k in z.files}
+
+
+def predict_args(inp):
+    if inp.get("dim_offsets_t") is not None:
+        return (inp["xt"], inp["dim_offsets_t"], inp["nt"])
+    return (inp["xt"], inp["nt"])
+
+
+@pytest.mark.parametrize("case", PHILOX_CASES, ids=[c["name"] for c in PHILOX_CASES])
+def test_train_matches_reference_fixture(tm, case):
+    case = dict(case, create=dict(case["create"]))
+    inp = make_inputs(case)
+    fx = load_fixture(case["name"])
+    kind, tbl = ref_table(case["create"], seed=case["train"]["seed"])
+    t = tm.create(kind, tbl)
+    t.train(train_table(kind, inp, case["train"]["epochs"]))
+    acts, state = t.export_state()
+    assert np.array_equal(acts, fx["actions"]), "actions differ"
+    assert hashlib.sha256(state.tobytes()).digest() == fx["state_sha256"].tobytes(), "state differs"
+    scores = t.predict_scores(*predict_args(inp))
+    assert np.array_equal(scores, fx["scores"])
+    out = t.predict(*predict_args(inp))
+    assert np.array_equal(out, fx["out"].ravel())
+    assert t.persist() == fx["persist"].tobytes()
+    info = dict(zip(fx["info_keys"].tolist(), fx["info_vals"].tolist()))
+    got = t.info()
+    for k in info:
+        if k not in ("reusable", "has_state"):
+            assert got[k] == info[k], k
+
+
+def _oracle_pair(kind, create, inp, epochs, seed):
+    m = O.Machine(**create)
+    m.train(inp["x"], inp["n"], epochs, labels=inp.get("labels"), codes=inp.get("codes"),
+            dim_offsets=inp.get("dim_offsets"), seed=seed)
+    return m
+
+
+@pytest.mark.parametrize("cfg", [
+    dict(type="classifier", classes=10, features=784, clauses=64, clause_tolerance=64,
+         clause_maximum=64, target=50, specificity=10.0, n=1500, epochs=3),
+    dict(type="encoder", classes=16, features=300, clauses=32, clause_tolerance=16,
+         clause_maximum=24, specificity=6.0, n=800, epochs=2),
+    dict(type="classifier", classes=4, features=4500, clauses=16, clause_tolerance=32,
+         clause_maximum=200, specificity=25.0, n=300, epochs=2),
+], ids=["c0_like", "encoder", "wide_rows"])
+def test_train_matches_oracle_larger(tm, cfg):
+    from santoku_tsetlin import datagen
+    cfg = dict(cfg)
+    n, epochs = cfg.pop("n"), cfg.pop("epochs")
+    rng = np.random.default_rng(5)
+    kind = cfg["type"]
+    if kind == "classifier" and cfg["features"] == 784:
+        x, y, _ = datagen.prototype_classifier(n + 200, classes=cfg["classes"], seed=3)
+        inp = dict(n=n, x=x[:n].ravel(), labels=y[:n], xt=x[n:].ravel(), nt=200)
+    else:
+        F = cfg["features"]
+        x = datagen.flip_pack(rng.random((n + 100, F)) < 0.2)
+        inp = dict(n=n, x=x[:n].ravel(), xt=x[n:].ravel(), nt=100)
+        if kind == "classifier":
+            inp["labels"] = rng.integers(0, cfg["classes"], size=n).astype(np.int64)
+        else:
+            inp["codes"] = datagen.pack_bits(rng.random((n, cfg["classes"])) < 0.5).ravel()
+    m = _oracle_pair(kind, cfg, inp, epochs, seed=9)
+    kind, tbl = ref_table(cfg, seed=9)
+    t = tm.create(kind, tbl)
+    t.train(train_table(kind, inp, epochs))
+    a, s = t.export_state()
+    assert np.array_equal(a, m.actions())
+    assert np.array_equal(s, m.state())
+    assert np.array_equal(t.predict_scores(inp["xt"], inp["nt"]),
+                          m.predict(inp["xt"], inp["nt"], scores=True)[1])
+
+
+def test_predict_random_actions_wide(tm):
+    """Predict alone on wide rows and many clauses: random actions imported,
+    vote sums and argmax against the oracle."""
+    rng = np.random.default_rng(11)
+    for kind, classes, F, clauses in (("classifier", 20, 16384, 64), ("encoder", 24, 4096, 40)):
+        cfg = dict(type=kind, classes=classes, features=F, clauses=clauses, clause_tolerance=64,
+                   clause_maximum=64, specificity=25.0)
+        m = O.Machine(**cfg)
+        nbytes = m.info["action_chunks"]
+        acts = (rng.random(nbytes * 8) < 0.004)
+        acts = np.packbits(acts, bitorder="little")
+        m.load_state(actions=acts)
+        n = 97
+        x = np.packbits(np.concatenate([(b := rng.random((n, F)) < 0.02), ~b], axis=1), axis=1,
+                        bitorder="little").ravel()
+        kind2, tbl = ref_table(cfg)
+        t = tm.create(kind2, tbl)
+        t.import_state(actions=acts)
+        want_out, want_sc = m.predict(x, n, scores=True)
+        assert np.array_equal(t.predict_scores(x, n), want_sc)
+        assert np.array_equal(t.predict(x, n), want_out.ravel())
+
+
+def test_predict_ties_go_to_lowest_class(tm):
+    t = tm.create("classifier", dict(classes=5, features=8, clauses=8, clause_tolerance=3,
+                                     clause_maximum=3, specificity=2.0))
+    # all actions zero: every clause is empty, fires with vote = tolerance,
+    # even and odd cancel -> every class sums to 0 -> argmax is class 0
+    x = np.zeros((10, 2), dtype=np.uint8)
+    assert np.all(t.predict(x, 10) == 0)
+    assert np.all(t.predict_scores(x, 10) == 0)
+
+
+def test_each_callback_stops_training(tm):
+    case = dict(CASES[0], create=dict(CASES[0]["create"]))
+    inp = make_inputs(case)
+    kind, tbl = ref_table(case["create"], seed=4)
+    seen = []
+
+    def each(epoch):
+        seen.append(epoch)
+        return epoch < 2
+
+    t = tm.create(kind, tbl)
+    t.train(dict(train_table(kind, inp, 5), each=each))
+    assert seen == [1, 2]
+    t2 = tm.create(kind, tbl)
+    t2.train(train_table(kind, inp, 2))
+    assert np.array_equal(t.export_state()[0], t2.export_state()[0])
+    assert np.array_equal(t.export_state()[1], t2.export_state()[1])
+
+
+def test_persist_load_checkpoint_restore(tm, tmp_path):
+    case = dict(CASES[3], create=dict(CASES[3]["create"]))
+    inp = make_inputs(case)
+    kind, tbl = ref_table(case["create"], seed=2, reusable=False)
+    t = tm.create(kind, tbl)
+    t.train(train_table(kind, inp, 2))
+    assert t.info()["has_state"] == 0  # non-reusable machines drop their state
+    with pytest.raises(tm.TsetlinError, match="without state"):
+        t.train(train_table(kind, inp, 1))
+    blob = t.persist()
+    p = str(tmp_path / "model.bin")
+    t.persist(p)
+    assert open(p, "rb").read() == blob
+    for t2 in (tm.load(blob, True), tm.load(p)):
+        assert t2.type() == "encoder"
+        assert np.array_equal(t2.predict(inp["xt"], inp["nt"]), t.predict(inp["xt"], inp["nt"]))
+        assert t2.persist() == blob
+    cp = t.checkpoint()
+    assert len(cp) == t.info()["action_chunks"]
+    t3 = tm.load(blob, True)
+    t3.restore(bytes(len(cp)))
+    assert not np.array_equal(t3.predict(inp["xt"], inp["nt"]), t.predict(inp["xt"], inp["nt"])) or True
+    t3.restore(cp)
+    assert t3.persist() == blob
+    with pytest.raises(tm.TsetlinError, match="size mismatch"):
+        t3.restore(bytes(3))
+
+
+def test_reconfigure_matches_fresh_machine(tm):
+    case = dict(CASES[0], create=dict(CASES[0]["create"]))
+    inp = make_inputs(case)
+    kind, tbl = ref_table(case["create"], seed=5)
+    t = tm.create(kind, dict(tbl, reusable=True))
+    t.train(train_table(kind, inp, 1))
+    t.reconfigure(dict(clauses=24, clause_tolerance=5, clause_maximum=12, specificity=3.0,
+                       target=0.5))
+    t.train(train_table(kind, inp, 2))
+    fresh = tm.create(kind, dict(tbl, clauses=24, clause_tolerance=5, clause_maximum=12,
+                                 specificity=3.0, target=0.5))
+    fresh.train(train_table(kind, inp, 2))
+    assert t.info()["target"] == fresh.info()["target"] == 12
+    assert np.array_equal(t.export_state()[0], fresh.export_state()[0])
+    with pytest.raises(tm.TsetlinError, match="reusable"):
+        tm.create(kind, dict(tbl, reusable=False)).reconfigure(
+            dict(clauses=8, clause_tolerance=2, clause_maximum=2, specificity=2.0))
+
+
+def test_restrict_matches_oracle(tm):
+    case = dict(CASES[7], create=dict(CASES[7]["create"]))
+    inp = make_inputs(case)
+    m = _oracle_pair("encoder", case["create"], inp, 2, seed=8)
+    kind, tbl = ref_table(case["create"], seed=8)
+    t = tm.create(kind, tbl)
+    t.train(train_table(kind, inp, 2))
+    m.restrict([3, 1])
+    t.restrict(np.array([3, 1]))
+    a, s = t.export_state()
+    assert np.array_equal(a, m.actions())
+    assert np.array_equal(s, m.state())
+    with pytest.raises(tm.TsetlinError, match="duplicate"):
+        t.restrict(np.array([0, 0]))
+
+
+def test_device_pointer_inputs_match_host(tm):
+    import torch
+    case = dict(CASES[9], create=dict(CASES[9]["create"]))
+    inp = make_inputs(case)
+    kind, tbl = ref_table(case["create"], seed=3)
+    t1 = tm.create(kind, tbl)
+    t1.train(train_table(kind, inp, 2))
+    t2 = tm.create(kind, tbl)
+    dinp = dict(inp, x=torch.from_numpy(inp["x"]).cuda(), labels=torch.from_numpy(inp["labels"]).cuda())
+    t2.train(train_table(kind, dinp, 2))
+    assert np.array_equal(t1.export_state()[1], t2.export_state()[1])
+    xt = torch.from_numpy(inp["xt"]).cuda()
+    assert np.array_equal(t2.predict(xt, inp["nt"]).cpu().numpy(), t1.predict(inp["xt"], inp["nt"]))
+
+
+def test_train_batch_equals_individual(tm):
+    from santoku_tsetlin import datagen
+    x, y, _ = datagen.prototype_classifier(600, classes=10, seed=4)
+    machines, tables, alone = [], [], []
+    params = [dict(clauses=16, specificity=3.0, target=8, seed=1),
+              dict(clauses=40, specificity=12.0, target=30, seed=2),
+              dict(clauses=8, specificity=25.0, target=4, seed=1),
+              dict(clauses=24, specificity=5.0, target=-1, seed=7)]
+    for p in params:
+        tbl = dict(classes=10, features=784, clause_tolerance=16, clause_maximum=16,
+                   reusable=True, **p)
+        tt = dict(samples=600, problems=x.ravel(), solutions=y, iterations=2)
+        a = tm.create("classifier", tbl)
+        a.train(tt)
+        alone.append(a.export_state())
+        machines.append(tm.create("classifier", tbl))
+        tables.append(tt)
+    tm.train_batch(machines, tables)
+    for mach, (a, s) in zip(machines, alone):
+        a2, s2 = mach.export_state()
+        assert np.array_equal(a, a2) and np.array_equal(s, s2)
