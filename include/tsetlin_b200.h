@@ -168,6 +168,21 @@ int tm_get_info(const tm_machine *m, uint64_t *out);
 int tm_export_state(tm_machine *m, uint8_t *actions, uint8_t *state);
 int tm_import_state(tm_machine *m, const uint8_t *actions, const uint8_t *state);
 
+/* Predict without allocating.  No counterpart in the reference.  For
+ * callers that must not call cudaMalloc / cudaFree while they run -- a
+ * serving loop that cannot absorb the device-wide synchronisation those
+ * calls cause, or an application whose own allocator already holds the GPU's
+ * memory.  Works in one fixed 8 MiB scratch array compiled into the library
+ * (held on every GPU that loads it until the process exits) instead of
+ * buffers grown on demand.  Dense machines only; `problems` and the output
+ * are device pointers; n * (row words * 4 + classes * 4) plus 256 bytes of
+ * alignment must fit in 8 MiB, larger requests fail with TM_ERR_ARG.  The
+ * first call on a device looks up the scratch array's device address (call
+ * it once before any stream capture).  Calls share the array: calls whose
+ * work overlaps on the GPU race.  Results equal tm_predict's. */
+int tm_predict_noalloc(tm_machine *m, const uint8_t *problems, uint64_t n, int64_t *out_classes,
+                       uint8_t *out_codes);
+
 /* ---- instrumentation ------------------------------------------------------ */
 /* Device-time accounting of the library's kernels for one machine, taken
  * with CUDA events on the machine's own stream.  The reference's analogue

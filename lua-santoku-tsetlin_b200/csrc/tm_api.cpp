@@ -836,6 +836,7 @@ int tmb_machine_view(tm_machine *m, MachineView *v) {
   v->Wp = m->cls[0].Wp;
   v->class_chunks = m->class_chunks;
   v->device = m->device;
+  v->st = m->st;
   return TM_OK;
 }
 

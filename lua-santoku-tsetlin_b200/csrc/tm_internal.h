@@ -113,6 +113,7 @@ struct MachineView {
   const ClassDev *cls;
   uint32_t classes, clauses, tol, type, input_chunks, Wp, class_chunks;
   int device;
+  cudaStream_t st;  // the machine's own stream
 };
 
 }  // namespace tmb

@@ -122,7 +122,7 @@ EXPORTS = (
     "tm_predict_scores", "tm_persist", "tm_persist_buf", "tm_free", "tm_load",
     "tm_checkpoint", "tm_restore", "tm_reconfigure", "tm_restrict", "tm_type",
     "tm_destroy", "tm_last_error", "tm_align", "tm_get_info", "tm_export_state",
-    "tm_import_state", "tm_stats_enable", "tm_get_stats", "tm_reset_stats", "tm_serve_open", "tm_serve_submit", "tm_serve_poll",
+    "tm_import_state", "tm_predict_noalloc", "tm_stats_enable", "tm_get_stats", "tm_reset_stats", "tm_serve_open", "tm_serve_submit", "tm_serve_poll",
     "tm_serve_latency_us", "tm_serve_close",
 )
 
@@ -159,6 +159,7 @@ def lib():
     L.tm_get_info.argtypes = [vp, vp]
     L.tm_export_state.argtypes = [vp, vp, vp]
     L.tm_import_state.argtypes = [vp, vp, vp]
+    L.tm_predict_noalloc.argtypes = [vp, vp, u64, vp, vp]
     L.tm_stats_enable.argtypes = [vp, i32]
     L.tm_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
     L.tm_reset_stats.argtypes = [vp]
