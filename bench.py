@@ -393,15 +393,218 @@ def run_ours(args, w):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+# batched hyper-parameter search: 64 machines, batched vs one per launch
+# ---------------------------------------------------------------------------
+def run_search(args):
+    import torch
+    import santoku_tsetlin as tm
+    from santoku_tsetlin import datagen
+    count, n_train, n_test = args.machines, 60000, 6000
+    epochs = args.epochs or 2
+    params = datagen.search_machines(count)
+    protos = np.random.default_rng(7919 + 1).random((10, 784)) < 0.2
+    xs = {}
+    for negated in (True, False):
+        x, y, _ = datagen.prototype_classifier(n_train + n_test, classes=10, features=784,
+                                               seed=1, negated=negated, prototypes=protos)
+        xs[negated] = (np.ascontiguousarray(x[:n_train]), np.ascontiguousarray(x[n_train:]))
+    yv = y
+    y_tr, y_te = np.ascontiguousarray(yv[:n_train]), yv[n_train:]
+    dev = torch.device("cuda", 0)
+    xd = {k: (torch.from_numpy(v[0]).to(dev), torch.from_numpy(v[1]).to(dev)) for k, v in xs.items()}
+    yd = torch.from_numpy(y_tr).to(dev)
+
+    def make():
+        out = []
+        for p in params:
+            out.append(tm.create("classifier", dict(
+                classes=10, features=p["features"], clauses=p["clauses"],
+                clause_tolerance=p["clause_tolerance"], clause_maximum=p["clause_maximum"],
+                specificity=p["specificity"], target=p["target"], seed=p["seed"],
+                reusable=True)))
+        return out
+
+    def tables():
+        return [{"samples": n_train, "problems": xd[p["negated"]][0], "solutions": yd,
+                 "iterations": epochs} for p in params]
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    warm = make()
+    tm.train_batch(warm[:4], tables()[:4])
+    for m in warm:
+        m.destroy()
+    batched = make()
+    clocks = ClockSampler(0)
+    clocks.start()
+    ms_b = timed(lambda: tm.train_batch(batched, tables()))
+    ck = clocks.stop()
+    plain = make()
+    tabs = tables()
+    ms_p = timed(lambda: [m.train(t) for m, t in zip(plain, tabs)])
+    same = all(np.array_equal(a.export_state()[0], b.export_state()[0])
+               for a, b in zip(batched[:8], plain[:8]))
+    acc_b = [float((m.predict(xd[p["negated"]][1], n_test).cpu().numpy() == y_te).mean())
+             for m, p in zip(batched, params)]
+    acc_p = [float((m.predict(xd[p["negated"]][1], n_test).cpu().numpy() == y_te).mean())
+             for m, p in zip(plain, params)]
+    samples = count * n_train * epochs
+    units = sum(10 * p["clauses"] // 8 for p in params)
+    out = {
+        "metric": "TM batched search train samples/s", "value": samples / (ms_b / 1e3),
+        "unit": "samples/s", "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": ms_b,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic",
+        "config": {"workload": "batched-search", "machines": count, "units": units,
+                   "n_train": n_train, "epochs": epochs,
+                   "clauses_per_class": [p["clauses"] for p in params],
+                   "step": "%d machines x %d epochs in one tm_train_batch" % (count, epochs)},
+        "plain": {"value": samples / (ms_p / 1e3), "ms": ms_p,
+                  "form": "one tm_train call (one launch group) per machine, in sequence"},
+        "batched_over_plain": ms_p / ms_b,
+        "bit_identical_first_8": bool(same),
+        "accuracy": {"batched_mean": float(np.mean(acc_b)), "plain_mean": float(np.mean(acc_p))},
+    }
+    if ck:
+        out["clocks"] = ck
+    print(json.dumps(out), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# predict serving: 16 resident machines, Poisson arrivals
+# ---------------------------------------------------------------------------
+def run_serve(args):
+    import ctypes
+    import threading
+    import santoku_tsetlin as tm
+    L = tm.lib()
+    rng = np.random.default_rng(11)
+    shapes = ([("classifier", 10, 784, 256)] * 6 + [("classifier", 20, 16384, 2048)] * 5 +
+              [("encoder", 256, 4096, 1024)] * 5)
+    machines, pools = [], []
+    for i, (kind, classes, feats, clauses) in enumerate(shapes):
+        tbl = dict(clauses=clauses, clause_tolerance=64, clause_maximum=64, specificity=10.0,
+                   seed=i)
+        tbl.update(dict(classes=classes, features=feats) if kind == "classifier"
+                   else dict(hidden=classes, visible=feats))
+        t = tm.create(kind, tbl)
+        info = t.info()
+        acts = np.packbits(rng.random(info["action_chunks"] * 8) < 0.01, bitorder="little")
+        t.import_state(actions=acts)
+        blob = t.persist()
+        t.destroy()
+        machines.append(tm.load(blob, True))
+        dens = 0.015 if feats == 16384 else 0.2
+        pools.append(np.packbits(np.concatenate([(b := rng.random((4096, feats)) < dens), ~b],
+                                                axis=1), axis=1, bitorder="little"))
+    out = serve_at(args, L, tm, machines, pools, rng, args.rate)
+    out["at_sustainable_rate"] = serve_at(args, L, tm, machines, pools, rng, args.sustainable_rate,
+                                          requests=max(200, args.requests // 4))
+    print(json.dumps(out), flush=True)
+
+
+def serve_at(args, L, tm, machines, pools, rng, rate, requests=None):
+    import ctypes
+    import threading
+    nreq = requests or args.requests
+    gaps = rng.exponential(1.0 / rate, size=nreq)
+    arrive = np.cumsum(gaps)
+    sizes = np.exp(rng.uniform(0, np.log(4096), size=nreq)).astype(np.int64)
+    which = rng.integers(0, len(machines), size=nreq)
+    starts = [int(rng.integers(0, 4096 - s + 1)) for s in sizes]
+    inputs = [np.ascontiguousarray(pools[w][st:st + s]).ravel()
+              for w, st, s in zip(which, starts, sizes)]
+    cfg = tm._ServerConfig(args.hbm_budget << 20, 8, 4096, 0)
+    hs = (ctypes.c_void_p * len(machines))(*[m.handle.value for m in machines])
+    srv = ctypes.c_void_p()
+    assert L.tm_serve_open(ctypes.byref(cfg), hs, len(machines), ctypes.byref(srv)) == 0, \
+        L.tm_last_error()
+    ids = [0] * nreq
+    t0 = time.perf_counter()
+
+    def submit():
+        for i in range(nreq):
+            d = t0 + arrive[i] - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            rid = ctypes.c_uint64()
+            L.tm_serve_submit(srv, int(which[i]), inputs[i].ctypes.data, int(sizes[i]),
+                              ctypes.byref(rid))
+            ids[i] = rid.value
+
+    th = threading.Thread(target=submit)
+    th.start()
+    th.join()
+    lat = []
+    for i in range(nreq):
+        info_t = machines[which[i]]
+        out = np.zeros(int(sizes[i]) * 32, dtype=np.int64)
+        assert L.tm_serve_poll(srv, ids[i], out.ctypes.data, out.ctypes.data, 60_000_000) == 1
+        us = ctypes.c_double()
+        L.tm_serve_latency_us(srv, ids[i], ctypes.byref(us))
+        lat.append(us.value / 1e3)
+    makespan = float(np.max(arrive + np.array(lat) / 1e3))
+    L.tm_serve_close(srv)
+    # serial per-request predict under the same arrivals
+    lat_s = []
+    t0 = time.perf_counter()
+    for i in range(nreq):
+        d = t0 + arrive[i] - time.perf_counter()
+        if d > 0:
+            time.sleep(d)
+        machines[which[i]].predict(inputs[i], int(sizes[i]))
+        lat_s.append((time.perf_counter() - (t0 + arrive[i])) * 1e3)
+    t_end_s = time.perf_counter()
+    total = int(sizes.sum())
+    out = {
+        "metric": "serve p99 ms", "value": float(np.percentile(lat, 99)), "unit": "ms",
+        "n_gpus": 1, "steps": nreq, "warmup": 0, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": "predict-serving", "machines": len(machines),
+                   "shapes": "6 plain classifiers, 5 large sparse classifiers, 5 encoders",
+                   "requests": nreq, "rate_per_s": rate, "batch": "log-uniform [1, 4096]",
+                   "hbm_budget_mb": args.hbm_budget},
+        "p50_ms": float(np.percentile(lat, 50)),
+        "offered_samples_per_s": float(sizes.sum() / arrive[-1]),
+        "samples_per_s": total / makespan,
+        "serial": {"p50_ms": float(np.percentile(lat_s, 50)),
+                   "p99_ms": float(np.percentile(lat_s, 99)),
+                   "samples_per_s": total / (t_end_s - t0),
+                   "form": "one tm_predict call per request, in arrival order"},
+    }
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS) + ["search", "serve"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--machines", type=int, default=64, help="search: machines")
+    ap.add_argument("--epochs", type=int, default=0, help="search: epochs (default 2)")
+    ap.add_argument("--requests", type=int, default=2000, help="serve: requests")
+    ap.add_argument("--rate", type=float, default=5000.0, help="serve: arrivals per second")
+    ap.add_argument("--hbm-budget", type=int, default=2048, help="serve: staging MB")
+    ap.add_argument("--sustainable-rate", type=float, default=150.0,
+                    help="serve: second, sustainable arrival rate")
     args = ap.parse_args()
+    if args.workload == "search":
+        run_search(args)
+        return
+    if args.workload == "serve":
+        run_serve(args)
+        return
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
         run_reference(args, w)

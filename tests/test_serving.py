@@ -1,0 +1,113 @@
+"""Continuous-batching predict server (tm_serve_*).
+
+Requests of many sizes for several resident machines are submitted from
+several threads while earlier ones are on the GPU; each result must equal
+what tm_predict returns for that request alone (predict is integer
+arithmetic: zero tolerance).  Also: the HBM budget decides how many launch
+slots exist and refuses a budget that covers none; a request larger than a
+slot is refused.
+"""
+import ctypes
+import threading
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _machine(tm, kind, features, classes, clauses, seed):
+    from santoku_tsetlin import datagen
+    rng = np.random.default_rng(seed)
+    n = 300
+    x = datagen.flip_pack(rng.random((n, features)) < 0.2)
+    if kind == "classifier":
+        t = tm.create("classifier", dict(classes=classes, features=features, clauses=clauses,
+                                         clause_tolerance=16, clause_maximum=32,
+                                         specificity=6.0, seed=seed))
+        t.train({"samples": n, "problems": x.ravel(),
+                 "solutions": rng.integers(0, classes, size=n).astype(np.int64),
+                 "iterations": 2})
+    else:
+        t = tm.create("encoder", dict(hidden=classes, visible=features, clauses=clauses,
+                                      clause_tolerance=16, clause_maximum=32, specificity=6.0,
+                                      seed=seed))
+        t.train({"samples": n, "sentences": x.ravel(),
+                 "codes": datagen.pack_bits(rng.random((n, classes)) < 0.5).ravel(),
+                 "iterations": 2})
+    return t
+
+
+def _open(tm, machines, budget, inflight=4, batch=4096):
+    L = tm.lib()
+    cfg = tm._ServerConfig(budget, inflight, batch, 0)
+    hs = (ctypes.c_void_p * len(machines))(*[m.handle.value for m in machines])
+    srv = ctypes.c_void_p()
+    rc = L.tm_serve_open(ctypes.byref(cfg), hs, len(machines), ctypes.byref(srv))
+    return rc, srv
+
+
+def test_alone_equals_mixed(tm):
+    L = tm.lib()
+    ms = [_machine(tm, "classifier", 784, 10, 64, 1),
+          _machine(tm, "encoder", 500, 20, 32, 2),
+          _machine(tm, "classifier", 4096, 6, 24, 3)]
+    infos = [m.info() for m in ms]
+    rc, srv = _open(tm, ms, budget=1 << 30)
+    assert rc == 0, L.tm_last_error()
+    rng = np.random.default_rng(5)
+    reqs = []
+    for i in range(120):
+        k = int(rng.integers(0, len(ms)))
+        n = int(np.exp(rng.uniform(0, np.log(2048))))
+        feats = infos[k]["features"]
+        x = np.packbits(np.concatenate([(b := rng.random((n, feats)) < 0.2), ~b], axis=1),
+                        axis=1, bitorder="little").ravel()
+        reqs.append((k, n, x))
+    ids = [None] * len(reqs)
+
+    def submit(lo, hi):
+        for i in range(lo, hi):
+            k, n, x = reqs[i]
+            rid = ctypes.c_uint64()
+            assert L.tm_serve_submit(srv, k, x.ctypes.data, n, ctypes.byref(rid)) == 0
+            ids[i] = rid.value
+
+    th = [threading.Thread(target=submit, args=(j * 30, (j + 1) * 30)) for j in range(4)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    lat = []
+    for i, (k, n, x) in enumerate(reqs):
+        info = infos[k]
+        if info["type"] == 0:
+            out = np.zeros(n, dtype=np.int64)
+            done = L.tm_serve_poll(srv, ids[i], out.ctypes.data, None, 30_000_000)
+        else:
+            out = np.zeros(n * info["class_chunks"], dtype=np.uint8)
+            done = L.tm_serve_poll(srv, ids[i], None, out.ctypes.data, 30_000_000)
+        assert done == 1, L.tm_last_error()
+        assert np.array_equal(out, ms[k].predict(x, n)), "request %d differs from predict alone" % i
+        us = ctypes.c_double()
+        assert L.tm_serve_latency_us(srv, ids[i], ctypes.byref(us)) == 0
+        lat.append(us.value)
+    assert all(v > 0 for v in lat)
+    assert L.tm_serve_close(srv) == 0
+
+
+def test_budget_and_oversized_requests(tm):
+    L = tm.lib()
+    m = _machine(tm, "classifier", 784, 10, 16, 4)
+    rc, _ = _open(tm, [m], budget=1024)
+    assert rc < 0 and b"budget" in L.tm_last_error()
+    rc, srv = _open(tm, [m], budget=1 << 28, inflight=2, batch=64)
+    assert rc == 0
+    x = np.zeros(65 * 196, dtype=np.uint8)
+    rid = ctypes.c_uint64()
+    assert L.tm_serve_submit(srv, 0, x.ctypes.data, 65, ctypes.byref(rid)) < 0
+    assert L.tm_serve_submit(srv, 0, x.ctypes.data, 64, ctypes.byref(rid)) == 0
+    out = np.zeros(64, dtype=np.int64)
+    assert L.tm_serve_poll(srv, rid.value, out.ctypes.data, None, 10_000_000) == 1
+    assert np.array_equal(out, m.predict(x, 64))
+    assert L.tm_serve_close(srv) == 0
