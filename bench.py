@@ -45,11 +45,11 @@ WORKLOADS = {
         name="large-sparse-classifier", kind="classifier", classes=20, features=16384,
         clauses=2048, clause_tolerance=64, clause_maximum=64, specificity=25.0, target=200,
         n_train=100000, n_test=20000),
-    # the large sparse classifier's rows and data with 64 clauses per class:
-    # one wave of units, for profiler captures
+    # the large sparse classifier's rows and data with 112 clauses per class
+    # (280 units: one wave at two CTAs per SM), for profiler captures
     "c1_small": dict(
         name="large-sparse-classifier", kind="classifier", classes=20, features=16384,
-        clauses=64, clause_tolerance=64, clause_maximum=64, specificity=25.0, target=200,
+        clauses=112, clause_tolerance=64, clause_maximum=64, specificity=25.0, target=200,
         n_train=40000, n_test=4000),
     "c0": dict(
         name="plain-classifier", kind="classifier", classes=10, features=784, clauses=256,

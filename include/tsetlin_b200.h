@@ -194,6 +194,9 @@ typedef struct tm_stats {
   double predict_kernel_ms;
   uint64_t kernel_launches;   /* every kernel the library launched */
   uint64_t train_unit_steps;  /* (unit, sample) steps examined by train kernels */
+  int32_t train_mode;         /* last train kernel variant: 0 automata in shared memory,
+                                 1 in global memory, 2 split over a 2-CTA cluster,
+                                 3 one warp per unit (rows of at most 64 words) */
 } tm_stats;
 /* on != 0 starts timing (events around every train / predict kernel). */
 int tm_stats_enable(tm_machine *m, int32_t on);

@@ -103,6 +103,10 @@ struct tm_machine {
   bool lits_valid = false;
   cudaStream_t st = nullptr;
   bool timing = false;
+  bool pair = false;      // TSETLIN_B200_PAIR=1: split units too large for one SM over a
+                          // 2-CTA cluster instead of keeping their automata in global memory
+  bool no_warp = false;   // TSETLIN_B200_NO_WARP=1: never train a unit with one warp
+  int last_mode = -1;     // k_train variant of the last launch
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   tm_stats stats{};
   DevBuf x, raw, labels, codes, perm, perm_scratch, sums, outc, work, tdev, cls_job, errf;
@@ -243,6 +247,12 @@ extern "C" int tm_create(const tm_params *p, tm_machine **out) {
   m->clause_chunks = m->clauses / 8;
   m->seed = p->seed;
   m->device = p->device;
+  {
+    const char *e = getenv("TSETLIN_B200_PAIR");
+    m->pair = e && e[0] == '1';
+    const char *w = getenv("TSETLIN_B200_NO_WARP");
+    m->no_warp = w && w[0] == '1';
+  }
   if (m->individualized) {
     // capi.c:528-606 leaves features, input_bits, input_chunks and tail_mask
     // of an individualized machine unset (zero); they are persisted as such
@@ -400,7 +410,7 @@ struct TrainJob {
   uint64_t seed = 0;
 };
 
-static TrainSmem plan_smem(uint32_t Wpmax, uint32_t Bmax, uint32_t smax, bool smem_state) {
+static TrainSmem plan_smem(uint32_t Wpmax, uint32_t Bmax, uint32_t smax, int mode) {
   TrainSmem L{};
   uint32_t o = 0;
   auto take = [&](uint32_t bytes) {
@@ -408,17 +418,18 @@ static TrainSmem plan_smem(uint32_t Wpmax, uint32_t Bmax, uint32_t smax, bool sm
     o += (bytes + 127) / 128 * 128;
     return at;
   };
-  L.state_words = smem_state ? 8 * Bmax * Wpmax : 0;
+  const uint32_t cpc = mode == TM_MODE_PAIR ? 4 : 8;  // clauses held by one CTA
+  L.state_words = mode == TM_MODE_GLOBAL ? 0 : cpc * Bmax * Wpmax;
   L.state_off = take(L.state_words * 4);
   L.ring_words = Wpmax;
   L.ring_off = take(TM_RING * Wpmax * 4);
   L.bar_off = take(TM_RING * 8);
-  L.list_off = take(TM_BATCH * 4 * 9);
-  L.votes_off = take(16 * 4);
+  L.list_off = take(2 * TM_BATCH * 4 * 9);  // one entry per thread (pair CTAs: 512)
+  L.votes_off = take(128 * 4);
   L.ib_words = Wpmax;
-  L.ib_off = take(16 * Wpmax * 4);
+  L.ib_off = take(2 * cpc * Wpmax * 4);
   L.ovf_cap = std::max<uint32_t>(1, smax / 4);
-  L.ovf_off = take(8 * L.ovf_cap * 4);
+  L.ovf_off = take(cpc * L.ovf_cap * 4);
   L.misc_off = take(32 * 4);
   L.total = o;
   return L;
@@ -532,16 +543,69 @@ static int run_epochs(std::vector<TrainJob> &jobs, uint32_t e0, uint32_t e1, tm_
   if (work.empty()) return TM_OK;
   std::stable_sort(work.begin(), work.end(),
                    [](const WorkItem &a, const WorkItem &b) { return a.cost > b.cost; });
+  // automata in shared memory when a unit fits one SM, else in global
+  // memory (L2-resident working set) or, on request, split over a 2-CTA
+  // cluster
   const int optin = max_smem_optin(dev);
-  TrainSmem lay = plan_smem(Wpmax, Bmax, smax, true);
-  bool smem_state = (int)lay.total <= optin;
-  if (!smem_state) lay = plan_smem(Wpmax, Bmax, smax, false);
+  if (Wpmax <= 64 && Bmax <= 8 && !m0->no_warp) {
+    // short rows: one warp per unit
+    size_t wsm = 0;
+    const int occ = train_warp_occupancy(Wpmax, Bmax, smax, &wsm);
+    if (occ > 0 && (int)wsm <= optin) {
+      const int grid = (int)std::min<uint64_t>((work.size() + 3) / 4, (uint64_t)num_sms(dev) * occ);
+      m0->last_mode = TM_MODE_WARP;
+      m0->stats.train_mode = TM_MODE_WARP;
+      const size_t tb = td.size() * sizeof(TrainDev);
+      const size_t wb = work.size() * sizeof(WorkItem);
+      const size_t off_w = (tb + 255) & ~(size_t)255;
+      const size_t off_c = (off_w + wb + 255) & ~(size_t)255;
+      CK(m0->tdev.ensure(off_c + 256));
+      uint8_t *base = m0->tdev.as<uint8_t>();
+      CK(cudaMemcpyAsync(base, td.data(), tb, cudaMemcpyHostToDevice, st));
+      CK(cudaMemcpyAsync(base + off_w, work.data(), wb, cudaMemcpyHostToDevice, st));
+      CK(cudaMemsetAsync(base + off_c, 0, 8, st));
+      uint32_t *counter = (uint32_t *)(base + off_c);
+      if (m0->timing) CK(cudaEventRecord(m0->ev0, st));
+      CK(launch_train_warp((const TrainDev *)base, (const WorkItem *)(base + off_w),
+                           (uint32_t)work.size(), counter, e0, e1, Wpmax, Bmax, smax, grid, st));
+      if (m0->timing) CK(cudaEventRecord(m0->ev1, st));
+      note_launch(m0, 1);
+      CK(cudaStreamSynchronize(st));
+      m0->stats.train_launches++;
+      for (auto &J : jobs)
+        m0->stats.train_unit_steps += (uint64_t)J.m->classes * J.m->clause_chunks * J.a->samples *
+                                      (std::min<uint32_t>(J.a->iterations, e1) > e0
+                                           ? std::min<uint32_t>(J.a->iterations, e1) - e0 : 0);
+      if (m0->timing) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, m0->ev0, m0->ev1));
+        m0->stats.train_kernel_ms += ms;
+      }
+      return TM_OK;
+    }
+  }
+  int mode = TM_MODE_SMEM;
+  TrainSmem lay = plan_smem(Wpmax, Bmax, smax, mode);
+  // (measured on B200: the pair's per-sample cluster barrier costs more than
+  // the L2 round trips it saves, so global memory is the default)
+  if ((int)lay.total > optin && Bmax <= 8 && m0->pair) {
+    mode = TM_MODE_PAIR;
+    lay = plan_smem(Wpmax, Bmax, smax, mode);
+  }
+  if ((int)lay.total > optin) {
+    mode = TM_MODE_GLOBAL;
+    lay = plan_smem(Wpmax, Bmax, smax, mode);
+  }
   if ((int)lay.total > optin)
     return fail(TM_ERR_ARG, "train: rows too wide for one CTA (%u bytes of shared memory)",
                 lay.total);
-  const int occ = train_occupancy(lay, smem_state, Bmax);
+  const int occ = train_occupancy(lay, mode, Bmax);
   if (occ <= 0) return fail(TM_ERR_CUDA, "train: kernel cannot be resident (smem %u)", lay.total);
-  const int grid = (int)std::min<uint64_t>(work.size(), (uint64_t)num_sms(dev) * occ);
+  const int grid = mode == TM_MODE_PAIR
+                       ? 2 * (int)std::min<uint64_t>(work.size(), (uint64_t)occ)
+                       : (int)std::min<uint64_t>(work.size(), (uint64_t)num_sms(dev) * occ);
+  m0->last_mode = mode;
+  m0->stats.train_mode = mode;
   // device tables: [TrainDev...][WorkItem...][counter][err]
   const size_t tb = td.size() * sizeof(TrainDev);
   const size_t wb = work.size() * sizeof(WorkItem);
@@ -556,7 +620,7 @@ static int run_epochs(std::vector<TrainJob> &jobs, uint32_t e0, uint32_t e1, tm_
   uint32_t *err = counter + 1;
   if (m0->timing) CK(cudaEventRecord(m0->ev0, st));
   CK(launch_train((const TrainDev *)base, (const WorkItem *)(base + off_w), (uint32_t)work.size(),
-                  counter, e0, e1, lay, smem_state, Bmax, grid, err, st));
+                  counter, e0, e1, lay, mode, Bmax, grid, err, st));
   if (m0->timing) CK(cudaEventRecord(m0->ev1, st));
   note_launch(m0, 1);
   uint32_t herr = 0;

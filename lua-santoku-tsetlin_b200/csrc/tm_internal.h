@@ -64,9 +64,9 @@ struct TrainSmem {
   uint32_t ring_off, ring_words;    // sample ring: TM_RING slots of ring_words
   uint32_t bar_off;                 // TM_RING mbarriers
   uint32_t list_off;                // active-sample list
-  uint32_t votes_off;               // 2 x 8 votes
-  uint32_t ib_off, ib_words;        // per warp: 2 levels x ib_words
-  uint32_t ovf_off, ovf_cap;        // per warp: overflow entries
+  uint32_t votes_off;               // 2 x 8 x 2 clause partial sums
+  uint32_t ib_off, ib_words;        // per CTA clause: 2 levels x ib_words
+  uint32_t ovf_off, ovf_cap;        // per CTA clause: overflow entries
   uint32_t misc_off;
   uint32_t total;
 };
@@ -91,10 +91,21 @@ cudaError_t launch_setup(uint32_t *act, uint32_t *cnt, const ClassDev *cls, uint
 cudaError_t launch_perm(uint64_t seed, uint32_t epoch, uint32_t n, uint32_t *out,
                         void *scratch, size_t scratch_bytes, cudaStream_t st);
 size_t perm_scratch_bytes(uint32_t n);
+// k_train variants: automata in shared memory (one CTA per unit), in global
+// memory (one CTA per unit), or split over a 2-CTA cluster in shared memory.
+constexpr int TM_MODE_SMEM = 0;
+constexpr int TM_MODE_GLOBAL = 1;
+constexpr int TM_MODE_PAIR = 2;
 cudaError_t launch_train(const TrainDev *machines, const WorkItem *work, uint32_t nwork,
                          uint32_t *counter, uint32_t e_begin, uint32_t e_end, const TrainSmem &lay,
-                         bool smem_state, uint32_t Bmax, int grid, uint32_t *err, cudaStream_t st);
-int train_occupancy(const TrainSmem &lay, bool smem_state, uint32_t Bmax);
+                         int mode, uint32_t Bmax, int grid, uint32_t *err, cudaStream_t st);
+int train_occupancy(const TrainSmem &lay, int mode, uint32_t Bmax);
+// k_train_warp: one warp per unit for rows of at most 64 words and B <= 8
+constexpr int TM_MODE_WARP = 3;
+int train_warp_occupancy(uint32_t Wpmax, uint32_t Bmax, uint32_t smax, size_t *smem_bytes);
+cudaError_t launch_train_warp(const TrainDev *machines, const WorkItem *work, uint32_t nwork,
+                              uint32_t *counter, uint32_t e_begin, uint32_t e_end, uint32_t Wpmax,
+                              uint32_t Bmax, uint32_t smax, int grid, cudaStream_t st);
 cudaError_t launch_lits(const uint32_t *act, const ClassDev *cls, uint32_t classes,
                         uint32_t clauses, int32_t *lits, cudaStream_t st);
 cudaError_t launch_predict(const uint32_t *act, const int32_t *lits, const ClassDev *cls,

@@ -9,6 +9,7 @@
 //   k_predict   tiled clause evaluation + per-class vote sums
 //               (capi.c:903-1086)
 //   k_finalize  argmax (ties to the lowest class) / code bits / scores
+#include <cooperative_groups.h>
 #include <cub/cub.cuh>
 
 #include "tm_internal.h"
@@ -352,59 +353,167 @@ __device__ __forceinline__ void rg_sub_pow2(uint32_t (&p)[BM], uint32_t &a, uint
   a = na;
 }
 
+// Four consecutive words at once: the B-1 planes and the action of words
+// w0..w0+3 (w0 a multiple of 4) are moved with 128-bit accesses and updated
+// word by word in registers.
+template <int BM>
+__device__ __forceinline__ void ld_quad(const uint32_t *__restrict__ act_c,
+                                        const uint32_t *__restrict__ cnt_c, uint32_t Wp,
+                                        uint32_t m, uint32_t w0, uint32_t (&p)[4][BM],
+                                        uint32_t (&a)[4]) {
+#pragma unroll
+  for (int b = 0; b < BM; b++)
+    if (b < (int)m) {
+      const uint4 t = *(const uint4 *)(cnt_c + b * Wp + w0);
+      p[0][b] = t.x;
+      p[1][b] = t.y;
+      p[2][b] = t.z;
+      p[3][b] = t.w;
+    }
+  const uint4 t = *(const uint4 *)(act_c + w0);
+  a[0] = t.x;
+  a[1] = t.y;
+  a[2] = t.z;
+  a[3] = t.w;
+}
+
+template <int BM>
+__device__ __forceinline__ void st_quad(uint32_t *__restrict__ act_c, uint32_t *__restrict__ cnt_c,
+                                        uint32_t Wp, uint32_t m, uint32_t w0,
+                                        const uint32_t (&p)[4][BM], const uint32_t (&a)[4]) {
+#pragma unroll
+  for (int b = 0; b < BM; b++)
+    if (b < (int)m) *(uint4 *)(cnt_c + b * Wp + w0) = make_uint4(p[0][b], p[1][b], p[2][b], p[3][b]);
+  *(uint4 *)(act_c + w0) = make_uint4(a[0], a[1], a[2], a[3]);
+}
+
+// rg_add with no decrements (Type II): plain carry ripple.
+template <int BM>
+__device__ __forceinline__ void rg_inc(uint32_t (&p)[BM], uint32_t &a, uint32_t m, uint32_t I,
+                                       uint32_t am) {
+  uint32_t c = I;
+#pragma unroll
+  for (int b = 0; b < BM; b++)
+    if (b < (int)m) {
+      const uint32_t q = p[b];
+      p[b] = q ^ c;
+      c &= q;
+    }
+  const uint32_t ca = c & am;
+  uint32_t na = a ^ ca;
+  c = a & ca;
+  if (c) {
+#pragma unroll
+    for (int b = 0; b < BM; b++)
+      if (b < (int)m) p[b] |= c;
+    na |= c;
+  }
+  a = na;
+}
+
+__device__ __forceinline__ uint32_t quad_get(const uint4 &v, int k) {
+  return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w));
+}
+
+// Mask of word w0 + k given the last-word mask `last` and W words.
+__device__ __forceinline__ uint32_t word_mask(uint32_t w, uint32_t W, uint32_t last) {
+  return w + 1 < W ? 0xFFFFFFFFu : (w + 1 == W ? last : 0u);
+}
+
 // ---------------------------------------------------------------------------
-// k_train: one CTA trains one unit (8 clauses of one class of one machine)
-// at a time, pulling units from a work list.  Warp j owns clause j.
+// k_train: trains units (8 clauses of one class of one machine), pulling
+// them from a work list.
+//
+// Two shapes:
+//   single  one CTA of 8 warps per unit; warp j owns clause j.  The unit's
+//           automata live in shared memory (SMEM_STATE, copied in and out
+//           once per unit) or stay in global memory.
+//   PAIR    a cluster of 2 CTAs per unit, for units too large for one SM
+//           (the large sparse classifier: 256 KB): CTA r holds clauses
+//           4r..4r+3 with all their bit planes in shared memory; two warps
+//           own each clause.  Clause partial sums are written to both CTAs'
+//           shared memory (DSMEM) and one cluster barrier per sample makes
+//           all eight visible to both.
 //
 // Per batch of TM_BATCH sample positions of the epoch order, every thread
 // examines one position: negative-sampling skip (capi.c:215) and the eight
 // chance draws (capi.c:232-239) are independent of the automata, so they
-// are drawn up front and the surviving samples are compacted into a list.
-// Per surviving sample:
+// are drawn up front and the surviving samples are compacted into a list
+// (both CTAs of a pair compute the same list).  Per surviving sample:
 //   1. its padded row arrives in a 4-slot shared-memory ring by TMA bulk
-//      copy (issued 3 samples ahead, completion on an mbarrier);
-//   2. warp j evaluates clause j (popcounts reduced with __reduce_add_sync)
-//      and publishes its vote;
-//   3. one CTA barrier; every warp forms the clamped chunk vote and decides
-//      its own clause's feedback from the pre-drawn chance values;
-//   4. warp j applies Type Ia / Ib / II feedback to clause j alone, so no
-//      further barrier is needed before the next sample.
+//      copy (issued 3 samples ahead, completion on an mbarrier; no
+//      multicast -- each CTA of a pair fetches its own copy);
+//   2. the warps of clause j reduce its literal and failed counts
+//      (__reduce_add_sync) and publish them;
+//   3. one barrier (CTA, or cluster for a pair); every warp forms all eight
+//      votes and the clamped chunk vote and decides its clause's feedback
+//      from the pre-drawn chance values;
+//   4. the Type Ia / Ib / II feedback of all fed-back clauses is spread over
+//      every thread of the CTA as (clause, word) items, so that no warp waits
+//      for another's clause; a barrier ends the sample.
 // ---------------------------------------------------------------------------
-template <bool SMEM_STATE, int BM>
-__global__ void __launch_bounds__(TM_TRAIN_THREADS)
+namespace cg = cooperative_groups;
+
+template <bool PAIR>
+__device__ __forceinline__ void unit_sync() {
+  if constexpr (PAIR)
+    cg::this_cluster().sync();
+  else
+    __syncthreads();
+}
+
+// Single-CTA variants (256 threads) are capped at 128 registers, two CTAs
+// per SM; a pair CTA (512 threads, its shared memory fills the SM) too.
+template <bool SMEM_STATE, bool PAIR, int BM>
+__global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS, PAIR ? 1 : 2)
     k_train(const TrainDev *__restrict__ machines, const WorkItem *__restrict__ work,
             uint32_t nwork, uint32_t *__restrict__ counter, uint32_t e_begin, uint32_t e_end,
             TrainSmem lay, uint32_t *__restrict__ err) {
+  constexpr uint32_t NW = PAIR ? 4 : 1;   // warps per clause
+  constexpr uint32_t CPC = PAIR ? 4 : 8;  // clauses per CTA
+  constexpr uint32_t GS = 32 * NW;        // lanes per clause group
   extern __shared__ __align__(128) uint8_t smem[];
-  const uint32_t tid = threadIdx.x, lane = tid & 31, j = tid >> 5;
+  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t rank = PAIR ? cg::this_cluster().block_rank() : 0;
+  const uint32_t lc = warp / NW;            // local clause
+  const uint32_t gl = (warp % NW) * 32 + lane;  // lane within the clause group
+  const uint32_t j = rank * CPC + lc;       // clause of the unit (0..7)
   uint32_t *ring = (uint32_t *)(smem + lay.ring_off);
   uint64_t *bars = (uint64_t *)(smem + lay.bar_off);
   uint32_t *list_s = (uint32_t *)(smem + lay.list_off);
-  uint32_t *list_d = list_s + TM_BATCH;
-  int32_t *votes = (int32_t *)(smem + lay.votes_off);
-  uint32_t *lev0 = (uint32_t *)(smem + lay.ib_off) + (size_t)j * 2 * lay.ib_words;
-  uint32_t *lev1 = lev0 + lay.ib_words;
-  uint32_t *ovf = (uint32_t *)(smem + lay.ovf_off) + (size_t)j * lay.ovf_cap;
+  uint32_t *list_d = list_s + blockDim.x;
+  // parts[buf][clause][warp of the clause][literal count, failed count]
+  uint32_t *parts = (uint32_t *)(smem + lay.votes_off);
   uint32_t *misc = (uint32_t *)(smem + lay.misc_off);
-  // misc: [0] unit, [1..8] warp active counts, [9] abort, [16..23] overflow counts
+  // misc: [0] unit, [1..16] warp active counts, [20] abort, [24..31] overflow counts
+  uint32_t *peer_parts = parts, *peer_misc = misc;
+  if constexpr (PAIR) {
+    cg::cluster_group cl = cg::this_cluster();
+    peer_parts = cl.map_shared_rank(parts, rank ^ 1u);
+    peer_misc = cl.map_shared_rank(misc, rank ^ 1u);
+  }
 
   if (tid == 0) {
     for (int r = 0; r < TM_RING; r++) mbar_init(&bars[r], 1);
     mbar_fence_init();
-    misc[9] = 0;
+    misc[20] = 0;
   }
-  for (uint32_t i = tid; i < 16 * lay.ib_words; i += blockDim.x)
+  for (uint32_t i = tid; i < 2 * CPC * lay.ib_words; i += blockDim.x)
     ((uint32_t *)(smem + lay.ib_off))[i] = 0;
-  if (tid < 8) misc[16 + tid] = 0;
-  __syncthreads();
+  if (tid < 8) misc[24 + tid] = 0;
+  unit_sync<PAIR>();
 
   uint32_t gs = 0;  // rows issued to the ring so far (slot/phase of row k: k % R, k / R)
   uint32_t issued = 0;
   bool aborted = false;
 
   while (true) {
-    if (tid == 0) misc[0] = atomicAdd(counter, 1u);
-    __syncthreads();
+    if (tid == 0 && rank == 0) {
+      const uint32_t u = atomicAdd(counter, 1u);
+      misc[0] = u;
+      if constexpr (PAIR) peer_misc[0] = u;
+    }
+    unit_sync<PAIR>();
     const uint32_t u = misc[0];
     if (u >= nwork) break;
     const WorkItem wi = work[u];
@@ -413,13 +522,14 @@ __global__ void __launch_bounds__(TM_TRAIN_THREADS)
     const uint32_t m = M.B - 1;
     const uint32_t Wp = C.Wp, W = C.W;
     const uint32_t g = wi.h * M.clause_chunks + wi.k;
-    uint32_t *gact = M.act + C.act_off + (uint64_t)wi.k * 8 * Wp;
-    uint32_t *gcnt = M.cnt + C.cnt_off + (uint64_t)wi.k * 8 * m * Wp;
+    // this CTA's clauses: rows rank*CPC .. rank*CPC+CPC-1 of the unit
+    uint32_t *gact = M.act + C.act_off + ((uint64_t)wi.k * 8 + rank * CPC) * Wp;
+    uint32_t *gcnt = M.cnt + C.cnt_off + ((uint64_t)wi.k * 8 + rank * CPC) * m * Wp;
     uint32_t *act, *cnt;
     if (SMEM_STATE) {
       act = (uint32_t *)(smem + lay.state_off);
-      cnt = act + 8 * Wp;
-      const uint32_t na4 = 2 * Wp, nc4 = 2 * m * Wp;  // uint4 counts
+      cnt = act + CPC * Wp;
+      const uint32_t na4 = CPC * Wp / 4, nc4 = CPC * m * Wp / 4;  // uint4 counts
       for (uint32_t i = tid; i < na4; i += blockDim.x)
         ((uint4 *)act)[i] = ((const uint4 *)gact)[i];
       for (uint32_t i = tid; i < nc4; i += blockDim.x)
@@ -429,8 +539,10 @@ __global__ void __launch_bounds__(TM_TRAIN_THREADS)
       act = gact;
       cnt = gcnt;
     }
-    uint32_t *act_j = act + j * Wp;
-    uint32_t *cnt_j = cnt + (size_t)j * m * Wp;
+    uint32_t *act_j = act + lc * Wp;
+    uint32_t *cnt_j = cnt + (size_t)lc * m * Wp;
+    bool dirty = true;       // this warp's clause changed since its literal count was taken
+    uint32_t lit_cache = 0;  // its literal count when clean
     const uint32_t T = M.T;
     const uint64_t T2 = 2ull * T;
     const uint32_t ep_end = e_end < M.epochs ? e_end : M.epochs;
@@ -440,7 +552,7 @@ __global__ void __launch_bounds__(TM_TRAIN_THREADS)
     for (uint32_t e = e_begin; e < ep_end && !aborted; e++) {
       const uint32_t ee = M.epoch_base + e;
       const uint32_t *perm = M.perm + (uint64_t)(e - e_begin) * M.n;
-      for (uint32_t base = 0; base < M.n && !aborted; base += TM_BATCH) {
+      for (uint32_t base = 0; base < M.n && !aborted; base += blockDim.x) {
         // ---- batch phase: skip decisions and chance draws ----------------
         const uint32_t i = base + tid;
         bool live = false;
@@ -461,13 +573,12 @@ __global__ void __launch_bounds__(TM_TRAIN_THREADS)
           }
         }
         const uint32_t bal = __ballot_sync(0xFFFFFFFFu, live);
-        if (lane == 0) misc[1 + j] = __popc(bal);
+        if (lane == 0) misc[1 + warp] = __popc(bal);
         __syncthreads();
         uint32_t off = 0, nact = 0;
-#pragma unroll
-        for (uint32_t w = 0; w < 8; w++) {
+        for (uint32_t w = 0; w < (blockDim.x >> 5); w++) {
           const uint32_t c = misc[1 + w];
-          off += w < j ? c : 0;
+          off += w < warp ? c : 0;
           nact += c;
         }
         if (live) {
@@ -494,33 +605,52 @@ __global__ void __launch_bounds__(TM_TRAIN_THREADS)
         for (uint32_t a = 0; a < nact; a++) {
           const uint32_t k = gs + a, sl = k % TM_RING;
           if (!mbar_wait(&bars[sl], (k / TM_RING) & 1u)) {
-            misc[9] = 1;
+            misc[20] = 1;
+            if constexpr (PAIR) peer_misc[20] = 1;
             atomicOr(err, 1u);
           }
           const uint32_t *xr = ring + sl * lay.ring_words;
           const uint32_t ent = list_s[a];
           const uint32_t pa = ent >> 31;
 
-          // clause j: literal count L and failed count F (capi.c:97-122)
+          // clause j: literal count L and failed count F (capi.c:97-122).
+          // L only changes when the clause is updated, so it is recounted
+          // only after feedback to the clause (`dirty`).
           uint32_t l = 0, f = 0;
-          for (uint32_t w = lane; w < W; w += 32) {
-            uint32_t av = act_j[w];
-            if (w + 1 == W) av &= C.emask;
-            l += __popc(av);
-            f += __popc(av & ~xr[w]);
+          const uint32_t Q = Wp >> 2, qlast = (W - 1) >> 2;
+#pragma unroll 4
+          for (uint32_t qi = gl; qi < Q; qi += GS) {
+            uint4 a4 = *(const uint4 *)(act_j + 4 * qi);
+            const uint4 x4 = *(const uint4 *)(xr + 4 * qi);
+            if (qi == qlast) {  // evaluation mask on word W-1 (capi.c:104-106)
+              const uint32_t k = (W - 1) & 3;
+              if (k == 0) a4.x &= C.emask;
+              if (k == 1) a4.y &= C.emask;
+              if (k == 2) a4.z &= C.emask;
+              if (k == 3) a4.w &= C.emask;
+            }
+            f += __popc(a4.x & ~x4.x) + __popc(a4.y & ~x4.y) + __popc(a4.z & ~x4.z) +
+                 __popc(a4.w & ~x4.w);
+            if (dirty) l += __popc(a4.x) + __popc(a4.y) + __popc(a4.z) + __popc(a4.w);
           }
-          const uint32_t L = __reduce_add_sync(0xFFFFFFFFu, l);
-          const uint32_t F = __reduce_add_sync(0xFFFFFFFFu, f);
-          int32_t vote;
-          if (L == 0)
-            vote = (int32_t)M.tol;
-          else {
-            vote = (int32_t)(L < M.tol ? L : M.tol) - (int32_t)F;
-            vote = vote < 0 ? 0 : vote;
+          if (dirty) {
+            l = __reduce_add_sync(0xFFFFFFFFu, l);
+          } else {
+            l = (warp % NW == 0) ? lit_cache : 0u;
           }
-          if (lane == 0) votes[(a & 1) * 8 + j] = vote;
-          __syncthreads();
-          if (misc[9]) {
+          f = __reduce_add_sync(0xFFFFFFFFu, f);
+          uint32_t *slot_parts = parts + (a & 1) * 64;
+          if (lane == 0) {
+            const uint32_t at = j * 8 + (warp % NW) * 2;
+            slot_parts[at] = l;
+            slot_parts[at + 1] = f;
+            if constexpr (PAIR) {
+              peer_parts[(a & 1) * 64 + at] = l;
+              peer_parts[(a & 1) * 64 + at + 1] = f;
+            }
+          }
+          unit_sync<PAIR>();
+          if (misc[20]) {
             aborted = true;
             break;
           }
@@ -530,29 +660,377 @@ __global__ void __launch_bounds__(TM_TRAIN_THREADS)
                     xbase + (uint64_t)(list_s[a + TM_RING - 1] & 0x7FFFFFFFu) * Wp, row_bytes);
             issued = k2 + 1;
           }
-          // chunk vote, clamp, feedback probability (capi.c:217-225)
-          const int32_t *vv = votes + (a & 1) * 8;
-          int32_t v = vv[0] - vv[1] + vv[2] - vv[3] + vv[4] - vv[5] + vv[6] - vv[7];
+          // votes of all eight clauses (capi.c:110-118), lane q computing
+          // clause q's; chunk vote, clamp, feedback probability
+          // (capi.c:217-225) by warp reduction
+          uint32_t Lq = 0;
+          int32_t vq = 0;
+          if (lane < 8) {
+            Lq = 0;
+            uint32_t Fq = 0;
+#pragma unroll
+            for (uint32_t h = 0; h < NW; h++) {
+              Lq += slot_parts[lane * 8 + 2 * h];
+              Fq += slot_parts[lane * 8 + 2 * h + 1];
+            }
+            if (Lq == 0)
+              vq = (int32_t)M.tol;
+            else {
+              vq = (int32_t)(Lq < M.tol ? Lq : M.tol) - (int32_t)Fq;
+              vq = vq < 0 ? 0 : vq;
+            }
+          }
+          int32_t v = __reduce_add_sync(0xFFFFFFFFu, (lane & 1) ? -vq : vq);
           v = v > (int32_t)T ? (int32_t)T : v;
           v = v < -(int32_t)T ? -(int32_t)T : v;
           const uint64_t av = (uint64_t)(pa ? (int64_t)T - v : (int64_t)T + v);
-          // clause j's pair and role (capi.c:226-242)
-          const uint32_t pr = j >> 1, odd = j & 1u;
+          lit_cache = __shfl_sync(0xFFFFFFFFu, Lq, j);
+          dirty = false;
+          // feedback of this CTA's clauses (capi.c:226-242), lane c deciding
+          // local clause c: draw 2p decides Type I of pair p, draw 2p+1 Type
+          // II; the positive case gives Type I to the even clause.  Masks over
+          // local clauses: Ia/II, Ib, Type I, Ia increments where x = 1.
+          const uint32_t cl = lane % CPC, jj = rank * CPC + cl;
+          const int32_t vj = __shfl_sync(0xFFFFFFFFu, vq, jj);
+          const uint32_t lj = __shfl_sync(0xFFFFFFFFu, Lq, jj);
+          const uint32_t odd = jj & 1u;
           const bool type1 = pa ? !odd : odd;
-          const uint32_t dr = list_d[a * 8 + 2 * pr + (type1 ? 0 : 1)];
-          if (bounded64(dr, T2) >= av) continue;
-          if (type1 && vote == 0) {
+          const uint32_t dr = list_d[a * 8 + 2 * (jj >> 1) + (type1 ? 0 : 1)];
+          const bool fire = lane < CPC && bounded64(dr, T2) < av;
+          const uint32_t ibm = __ballot_sync(0xFFFFFFFFu, fire && type1 && vj == 0);
+          const uint32_t fbm = __ballot_sync(0xFFFFFFFFu, fire && vj > 0);
+          const uint32_t t1m = __ballot_sync(0xFFFFFFFFu, fire && type1 && vj > 0);
+          const uint32_t incm = __ballot_sync(0xFFFFFFFFu, fire && type1 && vj > 0 && lj <= M.maxlit);
+          const uint32_t all = fbm | ibm;
+          if (!all) continue;
+          // Feedback work is shared by the whole CTA: Type Ib picks of every
+          // Ib clause are drawn by all threads, then (clause, word) items of
+          // every fed-back clause are spread over all threads.
+          uint32_t *ibase = (uint32_t *)(smem + lay.ib_off);
+          const uint32_t sp = ent & 0x7FFFFFFFu;
+          if (ibm) {
             // Type Ib (capi.c:181-190): s single-automaton decrements with
             // replacement, counted per bit in binary (two levels in shared
             // memory, larger counts as overflow entries of 4 each), then
             // applied as saturating subtractions -- order-free, so equal to
             // the reference's sequential decrements.
-            const uint32_t sp = ent & 0x7FFFFFFFu;
             const uint32_t npk = C.s_picks;
             const uint32_t nq = (npk + 3) >> 2;
+            for (uint32_t cm = ibm; cm; cm &= cm - 1) {
+              const uint32_t c = __ffs(cm) - 1, jj = rank * CPC + c;
+              uint32_t *l0 = ibase + (size_t)c * 2 * lay.ib_words, *l1 = l0 + lay.ib_words;
+              uint32_t *ov = (uint32_t *)(smem + lay.ovf_off) + (size_t)c * lay.ovf_cap;
+              for (uint32_t q = tid; q < nq; q += blockDim.x) {
+                uint32_t o[4];
+                philox(sp, ee, g, ST_IB | (jj << 20) | q, M.seed, o);
+#pragma unroll
+                for (uint32_t r = 0; r < 4; r++) {
+                  if (4 * q + r < npk) {
+                    const uint32_t bit = __umulhi(o[r], C.input_bits);
+                    const uint32_t w = bit >> 5, mk = 1u << (bit & 31);
+                    if (atomicXor(&l0[w], mk) & mk) {
+                      if (atomicXor(&l1[w], mk) & mk) {
+                        const uint32_t at = atomicAdd(&misc[24 + c], 1u);
+                        if (at < lay.ovf_cap) ov[at] = bit;
+                      }
+                    }
+                  }
+                }
+              }
+            }
+            __syncthreads();
+          }
+          // (clause, quad) items: item i -> the (i / Q)-th fed-back clause,
+          // words 4(i % Q) .. 4(i % Q) + 3
+          {
+            const uint32_t Q4 = Wp >> 2;
+            const uint32_t total = __popc(all) * Q4;
+            const uint32_t NT = blockDim.x;
+            uint32_t kk = tid / Q4, qi = tid - kk * Q4;
+            for (uint32_t it = tid; it < total; it += NT) {
+              const uint32_t c = __fns(all, 0, kk + 1);
+              const uint32_t w0 = 4 * qi;
+              uint32_t *act_c = act + c * Wp, *cnt_c = cnt + (size_t)c * m * Wp;
+              if ((ibm >> c) & 1u) {
+                uint32_t *l0 = ibase + (size_t)c * 2 * lay.ib_words;
+                const uint4 m0 = *(const uint4 *)(l0 + w0);
+                const uint4 m1 = *(const uint4 *)(l0 + lay.ib_words + w0);
+                if ((m0.x | m0.y | m0.z | m0.w | m1.x | m1.y | m1.z | m1.w) != 0) {
+                  *(uint4 *)(l0 + w0) = make_uint4(0, 0, 0, 0);
+                  *(uint4 *)(l0 + lay.ib_words + w0) = make_uint4(0, 0, 0, 0);
+                  uint32_t pq[4][BM], aq[4];
+                  ld_quad<BM>(act_c, cnt_c, Wp, m, w0, pq, aq);
+#pragma unroll
+                  for (int k = 0; k < 4; k++) {
+                    const uint32_t am = word_mask(w0 + k, W, C.amask);
+                    rg_sub_pow2<BM>(pq[k], aq[k], m, 0, quad_get(m0, k), am);
+                    rg_sub_pow2<BM>(pq[k], aq[k], m, 1, quad_get(m1, k), am);
+                  }
+                  st_quad<BM>(act_c, cnt_c, Wp, m, w0, pq, aq);
+                }
+              } else {
+                const uint4 x4 = *(const uint4 *)(xr + w0);
+                const bool t1 = (t1m >> c) & 1u;
+                uint32_t vm[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++) vm[k] = word_mask(w0 + k, W, C.vmask);
+                // Type II changes nothing where every literal is 1
+                const bool need = t1 || ((~x4.x & vm[0]) | (~x4.y & vm[1]) | (~x4.z & vm[2]) |
+                                         (~x4.w & vm[3])) != 0;
+                if (need) {
+                  uint32_t pq[4][BM], aq[4];
+                  ld_quad<BM>(act_c, cnt_c, Wp, m, w0, pq, aq);
+                  const bool incx = (incm >> c) & 1u;
+#pragma unroll
+                  for (int k = 0; k < 4; k++) {
+                    const uint32_t x = quad_get(x4, k);
+                    const uint32_t am = word_mask(w0 + k, W, C.amask);
+                    const uint32_t nx = ~x & ~rg_included<BM>(pq[k], aq[k], m, M.ib) & vm[k];
+                    // Type Ia (capi.c:177-180): inc where x=1 (if L <= maximum),
+                    // dec where x=0 and not included.  Type II (capi.c:192-196):
+                    // inc where x=0 and not included.
+                    if (t1)
+                      rg_add<BM>(pq[k], aq[k], m, incx ? (x & vm[k]) : 0u, nx, am);
+                    else
+                      rg_inc<BM>(pq[k], aq[k], m, nx, am);
+                  }
+                  st_quad<BM>(act_c, cnt_c, Wp, m, w0, pq, aq);
+                }
+              }
+              qi += NT;
+              while (qi >= Q4) {
+                qi -= Q4;
+                kk++;
+              }
+            }
+          }
+          if (all & (1u << lc)) dirty = true;
+          if (ibm) {
+            uint32_t novf = 0;
+            for (uint32_t cm = ibm; cm; cm &= cm - 1) novf += misc[24 + __ffs(cm) - 1];
+            if (novf) {
+              // bits picked 4 or more times: rare, applied by one thread
+              __syncthreads();
+              if (tid == 0) {
+                for (uint32_t cm = ibm; cm; cm &= cm - 1) {
+                  const uint32_t c = __ffs(cm) - 1;
+                  const uint32_t *ov = (uint32_t *)(smem + lay.ovf_off) + (size_t)c * lay.ovf_cap;
+                  const uint32_t no = misc[24 + c];
+                  for (uint32_t t = 0; t < no && t < lay.ovf_cap; t++) {
+                    const uint32_t bit = ov[t], w = bit >> 5;
+                    const uint32_t am = w + 1 == W ? C.amask : 0xFFFFFFFFu;
+                    uint32_t pp[BM], aq;
+                    ld_word<BM>(act + c * Wp, cnt + (size_t)c * m * Wp, Wp, m, w, pp, aq);
+                    rg_sub_pow2<BM>(pp, aq, m, 2, 1u << (bit & 31), am);
+                    st_word<BM>(act + c * Wp, cnt + (size_t)c * m * Wp, Wp, m, w, pp, aq);
+                  }
+                  misc[24 + c] = 0;
+                }
+              }
+            }
+          }
+          // the next sample's evaluation reads clauses this step updated
+          __syncthreads();
+        }
+        gs += nact;
+        unit_sync<PAIR>();
+      }
+    }
+    if (aborted) break;
+    if (SMEM_STATE) {
+      __syncthreads();
+      const uint32_t na4 = CPC * Wp / 4, nc4 = CPC * m * Wp / 4;
+      for (uint32_t i = tid; i < na4; i += blockDim.x)
+        ((uint4 *)gact)[i] = ((const uint4 *)act)[i];
+      for (uint32_t i = tid; i < nc4; i += blockDim.x)
+        ((uint4 *)gcnt)[i] = ((const uint4 *)cnt)[i];
+    }
+    unit_sync<PAIR>();
+  }
+  if (aborted && tid == 0) {
+    // wait (bounded) for this CTA's copies still in flight before exiting
+    for (uint32_t k = gs; k < issued; k++) mbar_wait(&bars[k % TM_RING], (k / TM_RING) & 1u);
+  }
+  // no CTA of a pair leaves while its peer may still write to its shared memory
+  unit_sync<PAIR>();
+}
+
+// ---------------------------------------------------------------------------
+// k_train_warp: short rows (Wp <= 64 words, B <= 8 state bits) -- one warp
+// per unit, warp-synchronous, no CTA barriers.  Lane l owns words l and
+// l + 32 of all 8 clauses; the unit's planes live in the warp's slice of
+// shared memory.  Per 32 positions of the epoch order each lane draws one
+// position's skip decision and chance draws into registers; surviving
+// positions are visited in order through the ballot mask, their draws
+// broadcast by shuffles.  The next surviving sample's row is loaded while
+// the current one is processed.  Same rules and draws as k_train.
+// ---------------------------------------------------------------------------
+constexpr int TM_WARP_THREADS = 128;
+
+template <int BM>
+__global__ void __launch_bounds__(TM_WARP_THREADS)
+    k_train_warp(const TrainDev *__restrict__ machines, const WorkItem *__restrict__ work,
+                 uint32_t nwork, uint32_t *__restrict__ counter, uint32_t e_begin, uint32_t e_end,
+                 uint32_t slice_words, uint32_t ib_words, uint32_t ovf_cap, uint32_t stride) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  // stride: words per warp, a multiple of 32 (16-byte alignment of every slice)
+  uint32_t *slice = (uint32_t *)smem + (size_t)wid * stride;
+  uint32_t *lev0 = slice + slice_words, *lev1 = lev0 + ib_words, *ovf = lev1 + ib_words;
+  uint32_t *cnt_ovf = ovf + ovf_cap;  // [0]: overflow entries
+  for (uint32_t i = lane; i < 2 * ib_words; i += 32) lev0[i] = 0;
+  if (lane == 0) cnt_ovf[0] = 0;
+  __syncwarp();
+  while (true) {
+    uint32_t u = 0;
+    if (lane == 0) u = atomicAdd(counter, 1u);
+    u = __shfl_sync(0xFFFFFFFFu, u, 0);
+    if (u >= nwork) break;
+    const WorkItem wi = work[u];
+    const TrainDev &M = machines[wi.m];
+    const ClassDev C = M.cls[wi.h];
+    const uint32_t m = M.B - 1;
+    const uint32_t Wp = C.Wp, W = C.W;
+    const uint32_t g = wi.h * M.clause_chunks + wi.k;
+    uint32_t *gact = M.act + C.act_off + (uint64_t)wi.k * 8 * Wp;
+    uint32_t *gcnt = M.cnt + C.cnt_off + (uint64_t)wi.k * 8 * m * Wp;
+    uint32_t *act = slice, *cnt = slice + 8 * Wp;
+    for (uint32_t i = lane; i < 2 * Wp; i += 32) ((uint4 *)act)[i] = ((const uint4 *)gact)[i];
+    for (uint32_t i = lane; i < 2 * m * Wp; i += 32) ((uint4 *)cnt)[i] = ((const uint4 *)gcnt)[i];
+    __syncwarp();
+    const uint32_t T = M.T;
+    const uint64_t T2 = 2ull * T;
+    const uint32_t ep_end = e_end < M.epochs ? e_end : M.epochs;
+    const uint32_t *xbase = M.x + C.x_off;
+    const uint32_t w0 = lane, w1 = lane + 32;
+    const uint32_t vm0 = word_mask(w0, W, C.vmask), vm1 = word_mask(w1, W, C.vmask);
+    const uint32_t em0 = word_mask(w0, W, C.emask), em1 = word_mask(w1, W, C.emask);
+    const uint32_t am0 = word_mask(w0, W, C.amask), am1 = word_mask(w1, W, C.amask);
+    uint32_t lits = 0;  // lane q < 8: literal count of clause q (valid when !dirty)
+    uint32_t dirty = 0xFFu;
+
+    for (uint32_t e = e_begin; e < ep_end; e++) {
+      const uint32_t ee = M.epoch_base + e;
+      const uint32_t *perm = M.perm + (uint64_t)(e - e_begin) * M.n;
+      for (uint32_t base = 0; base < M.n; base += 32) {
+        const uint32_t i = base + lane;
+        bool live = false;
+        uint32_t s = 0, pos = 0;
+        uint32_t d[8];
+        if (i < M.n) {
+          s = perm[i];
+          if (M.type == 0) {
+            pos = (uint32_t)M.labels[s] == wi.h;
+            live = pos;
+            if (!pos) {
+              uint32_t o[4];
+              philox(s, ee, g, ST_NEG, M.seed, o);
+              live = (uint64_t)o[0] >= M.thr_neg;
+            }
+          } else {
+            pos = (M.codes[(uint64_t)s * M.code_bytes + (wi.h >> 3)] >> (wi.h & 7)) & 1u;
+            live = true;
+          }
+          if (live) {
+            philox(s, ee, g, ST_CH0, M.seed, d);
+            philox(s, ee, g, ST_CH1, M.seed, d + 4);
+          }
+        }
+        uint32_t bal = __ballot_sync(0xFFFFFFFFu, live);
+        if (!bal) continue;
+        // row of the first surviving sample
+        uint32_t src = __ffs(bal) - 1;
+        uint32_t sc = __shfl_sync(0xFFFFFFFFu, s, src);
+        uint32_t x0 = xbase[(uint64_t)sc * Wp + (w0 < Wp ? w0 : 0)];
+        uint32_t x1 = w1 < Wp ? xbase[(uint64_t)sc * Wp + w1] : 0u;
+        while (bal) {
+          src = __ffs(bal) - 1;
+          bal &= bal - 1;
+          const uint32_t sp = __shfl_sync(0xFFFFFFFFu, s, src);
+          const uint32_t pa = __shfl_sync(0xFFFFFFFFu, pos, src);
+          uint32_t dd[8];
+#pragma unroll
+          for (int k = 0; k < 8; k++) dd[k] = __shfl_sync(0xFFFFFFFFu, d[k], src);
+          const uint32_t xa = w0 < W ? x0 : 0u, xb = w1 < W ? x1 : 0u;
+          // prefetch the next surviving sample's row
+          if (bal) {
+            const uint32_t sn = __shfl_sync(0xFFFFFFFFu, s, __ffs(bal) - 1);
+            x0 = xbase[(uint64_t)sn * Wp + (w0 < Wp ? w0 : 0)];
+            x1 = w1 < Wp ? xbase[(uint64_t)sn * Wp + w1] : 0u;
+          }
+          // evaluation of the 8 clauses (capi.c:97-122)
+          uint32_t Lq = 0, Fq = 0;
+#pragma unroll
+          for (uint32_t c = 0; c < 8; c++) {
+            const uint32_t a0 = (w0 < Wp ? act[c * Wp + w0] : 0u) & em0;
+            const uint32_t a1 = (w1 < Wp ? act[c * Wp + w1] : 0u) & em1;
+            const uint32_t fc = __reduce_add_sync(0xFFFFFFFFu, __popc(a0 & ~xa) + __popc(a1 & ~xb));
+            if (lane == c) Fq = fc;
+            if ((dirty >> c) & 1u) {
+              const uint32_t lc = __reduce_add_sync(0xFFFFFFFFu, __popc(a0) + __popc(a1));
+              if (lane == c) Lq = lc;
+            } else if (lane == c) {
+              Lq = lits;
+            }
+          }
+          lits = Lq;
+          dirty = 0;
+          int32_t vq = 0;
+          if (lane < 8) {
+            if (Lq == 0)
+              vq = (int32_t)M.tol;
+            else {
+              vq = (int32_t)(Lq < M.tol ? Lq : M.tol) - (int32_t)Fq;
+              vq = vq < 0 ? 0 : vq;
+            }
+          }
+          int32_t v = __reduce_add_sync(0xFFFFFFFFu, (lane & 1) ? -vq : vq);
+          v = v > (int32_t)T ? (int32_t)T : v;
+          v = v < -(int32_t)T ? -(int32_t)T : v;
+          const uint64_t av = (uint64_t)(pa ? (int64_t)T - v : (int64_t)T + v);
+          // lane c < 8 decides clause c (capi.c:226-242)
+          const uint32_t odd = lane & 1u;
+          const bool type1 = pa ? !odd : odd;
+          uint32_t dsel = 0;
+#pragma unroll
+          for (int k = 0; k < 8; k++)
+            if ((uint32_t)k == ((lane & 7) & ~1u) + (type1 ? 0u : 1u)) dsel = dd[k];
+          const bool fire = lane < 8 && bounded64(dsel, T2) < av;
+          const uint32_t ibm = __ballot_sync(0xFFFFFFFFu, fire && type1 && vq == 0);
+          const uint32_t fbm = __ballot_sync(0xFFFFFFFFu, fire && vq > 0);
+          const uint32_t t1m = __ballot_sync(0xFFFFFFFFu, fire && type1 && vq > 0);
+          const uint32_t incm =
+              __ballot_sync(0xFFFFFFFFu, fire && type1 && vq > 0 && Lq <= M.maxlit);
+          dirty = fbm | ibm;
+          // Type Ia / II (capi.c:177-180, 192-196) on the lane's two words
+          for (uint32_t cm = fbm; cm; cm &= cm - 1) {
+            const uint32_t c = __ffs(cm) - 1;
+            uint32_t *act_c = act + c * Wp, *cnt_c = cnt + (size_t)c * m * Wp;
+            const bool t1 = (t1m >> c) & 1u, incx = (incm >> c) & 1u;
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+              const uint32_t w = h ? w1 : w0, x = h ? xb : xa, vm = h ? vm1 : vm0;
+              const uint32_t am = h ? am1 : am0;
+              if (w >= W) continue;
+              if (!t1 && (~x & vm) == 0) continue;
+              uint32_t pp[BM], aq;
+              ld_word<BM>(act_c, cnt_c, Wp, m, w, pp, aq);
+              const uint32_t nx = ~x & ~rg_included<BM>(pp, aq, m, M.ib) & vm;
+              if (t1)
+                rg_add<BM>(pp, aq, m, incx ? (x & vm) : 0u, nx, am);
+              else
+                rg_inc<BM>(pp, aq, m, nx, am);
+              st_word<BM>(act_c, cnt_c, Wp, m, w, pp, aq);
+            }
+          }
+          // Type Ib (capi.c:181-190), counted per bit then applied
+          for (uint32_t cm = ibm; cm; cm &= cm - 1) {
+            const uint32_t c = __ffs(cm) - 1;
+            uint32_t *act_c = act + c * Wp, *cnt_c = cnt + (size_t)c * m * Wp;
+            const uint32_t npk = C.s_picks, nq = (npk + 3) >> 2;
             for (uint32_t q = lane; q < nq; q += 32) {
               uint32_t o[4];
-              philox(sp, ee, g, ST_IB | (j << 20) | q, M.seed, o);
+              philox(sp, ee, g, ST_IB | (c << 20) | q, M.seed, o);
 #pragma unroll
               for (uint32_t r = 0; r < 4; r++) {
                 if (4 * q + r < npk) {
@@ -560,138 +1038,141 @@ __global__ void __launch_bounds__(TM_TRAIN_THREADS)
                   const uint32_t w = bit >> 5, mk = 1u << (bit & 31);
                   if (atomicXor(&lev0[w], mk) & mk) {
                     if (atomicXor(&lev1[w], mk) & mk) {
-                      const uint32_t at = atomicAdd(&misc[16 + j], 1u);
-                      if (at < lay.ovf_cap) ovf[at] = bit;
+                      const uint32_t at = atomicAdd(&cnt_ovf[0], 1u);
+                      if (at < ovf_cap) ovf[at] = bit;
                     }
                   }
                 }
               }
             }
             __syncwarp();
-            for (uint32_t w0 = lane; w0 < W; w0 += 64) {
-              const uint32_t w1 = w0 + 32;
-              const uint32_t a0m = lev0[w0], a1m = lev1[w0];
-              const uint32_t b0m = w1 < W ? lev0[w1] : 0u, b1m = w1 < W ? lev1[w1] : 0u;
-              uint32_t pa[BM], pb[BM], aa = 0, ab = 0;
-              const bool ua = (a0m | a1m) != 0, ub = (b0m | b1m) != 0;
-              if (ua) {
-                lev0[w0] = 0;
-                lev1[w0] = 0;
-                ld_word<BM>(act_j, cnt_j, Wp, m, w0, pa, aa);
-              }
-              if (ub) {
-                lev0[w1] = 0;
-                lev1[w1] = 0;
-                ld_word<BM>(act_j, cnt_j, Wp, m, w1, pb, ab);
-              }
-              if (ua) {
-                const uint32_t am = w0 + 1 == W ? C.amask : 0xFFFFFFFFu;
-                rg_sub_pow2<BM>(pa, aa, m, 0, a0m, am);
-                rg_sub_pow2<BM>(pa, aa, m, 1, a1m, am);
-                st_word<BM>(act_j, cnt_j, Wp, m, w0, pa, aa);
-              }
-              if (ub) {
-                const uint32_t am = w1 + 1 == W ? C.amask : 0xFFFFFFFFu;
-                rg_sub_pow2<BM>(pb, ab, m, 0, b0m, am);
-                rg_sub_pow2<BM>(pb, ab, m, 1, b1m, am);
-                st_word<BM>(act_j, cnt_j, Wp, m, w1, pb, ab);
-              }
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+              const uint32_t w = h ? w1 : w0, am = h ? am1 : am0;
+              if (w >= W) continue;
+              const uint32_t m0 = lev0[w], m1 = lev1[w];
+              if (!(m0 | m1)) continue;
+              lev0[w] = 0;
+              lev1[w] = 0;
+              uint32_t pp[BM], aq;
+              ld_word<BM>(act_c, cnt_c, Wp, m, w, pp, aq);
+              rg_sub_pow2<BM>(pp, aq, m, 0, m0, am);
+              rg_sub_pow2<BM>(pp, aq, m, 1, m1, am);
+              st_word<BM>(act_c, cnt_c, Wp, m, w, pp, aq);
             }
             __syncwarp();
-            const uint32_t no = misc[16 + j];
-            for (uint32_t t = 0; t < no && t < lay.ovf_cap; t++) {
-              const uint32_t bit = ovf[t], w = bit >> 5;
-              if ((w & 31) == lane) {
-                const uint32_t am = w + 1 == W ? C.amask : 0xFFFFFFFFu;
-                uint32_t pp[BM], aq;
-                ld_word<BM>(act_j, cnt_j, Wp, m, w, pp, aq);
-                rg_sub_pow2<BM>(pp, aq, m, 2, 1u << (bit & 31), am);
-                st_word<BM>(act_j, cnt_j, Wp, m, w, pp, aq);
+            const uint32_t no = cnt_ovf[0];
+            if (no) {
+              if (lane == 0) {
+                for (uint32_t t = 0; t < no && t < ovf_cap; t++) {
+                  const uint32_t bit = ovf[t], w = bit >> 5;
+                  const uint32_t am = word_mask(w, W, C.amask);
+                  uint32_t pp[BM], aq;
+                  ld_word<BM>(act_c, cnt_c, Wp, m, w, pp, aq);
+                  rg_sub_pow2<BM>(pp, aq, m, 2, 1u << (bit & 31), am);
+                  st_word<BM>(act_c, cnt_c, Wp, m, w, pp, aq);
+                }
+                cnt_ovf[0] = 0;
               }
-            }
-            __syncwarp();
-            if (lane == 0) misc[16 + j] = 0;
-            __syncwarp();
-          } else if (vote > 0) {
-            // Type Ia (capi.c:177-180): inc where x=1 (if L <= maximum),
-            // dec where x=0 and not included.  Type II (capi.c:192-196): inc
-            // where x=0 and not included.
-            const bool inc_x = type1 && L <= M.maxlit;
-            for (uint32_t w0 = lane; w0 < W; w0 += 64) {
-              const uint32_t w1 = w0 + 32;
-              const uint32_t vma = w0 + 1 == W ? C.vmask : 0xFFFFFFFFu;
-              const uint32_t vmb = w1 + 1 == W ? C.vmask : (w1 < W ? 0xFFFFFFFFu : 0u);
-              const uint32_t xa = xr[w0], xb = w1 < W ? xr[w1] : 0xFFFFFFFFu;
-              // Type II changes nothing where every literal is 1
-              const bool ua = type1 || (~xa & vma) != 0;
-              const bool ub = w1 < W && (type1 || (~xb & vmb) != 0);
-              uint32_t pa[BM], pb[BM], aa = 0, ab = 0;
-              if (ua) ld_word<BM>(act_j, cnt_j, Wp, m, w0, pa, aa);
-              if (ub) ld_word<BM>(act_j, cnt_j, Wp, m, w1, pb, ab);
-              if (ua) {
-                const uint32_t am = w0 + 1 == W ? C.amask : 0xFFFFFFFFu;
-                const uint32_t nx = ~xa & ~rg_included<BM>(pa, aa, m, M.ib) & vma;
-                if (type1)
-                  rg_add<BM>(pa, aa, m, inc_x ? (xa & vma) : 0u, nx, am);
-                else
-                  rg_add<BM>(pa, aa, m, nx, 0u, am);
-                st_word<BM>(act_j, cnt_j, Wp, m, w0, pa, aa);
-              }
-              if (ub) {
-                const uint32_t am = w1 + 1 == W ? C.amask : 0xFFFFFFFFu;
-                const uint32_t nx = ~xb & ~rg_included<BM>(pb, ab, m, M.ib) & vmb;
-                if (type1)
-                  rg_add<BM>(pb, ab, m, inc_x ? (xb & vmb) : 0u, nx, am);
-                else
-                  rg_add<BM>(pb, ab, m, nx, 0u, am);
-                st_word<BM>(act_j, cnt_j, Wp, m, w1, pb, ab);
-              }
+              __syncwarp();
             }
           }
+          __syncwarp();
         }
-        gs += nact;
-        __syncthreads();
       }
     }
-    if (aborted) break;
-    if (SMEM_STATE) {
-      __syncthreads();
-      const uint32_t na4 = 2 * Wp, nc4 = 2 * m * Wp;
-      for (uint32_t i = tid; i < na4; i += blockDim.x)
-        ((uint4 *)gact)[i] = ((const uint4 *)act)[i];
-      for (uint32_t i = tid; i < nc4; i += blockDim.x)
-        ((uint4 *)gcnt)[i] = ((const uint4 *)cnt)[i];
-    }
-    __syncthreads();
-  }
-  if (aborted && tid == 0) {
-    // wait (bounded) for this CTA's copies still in flight before exiting
-    for (uint32_t k = gs; k < issued; k++) mbar_wait(&bars[k % TM_RING], (k / TM_RING) & 1u);
+    __syncwarp();
+    for (uint32_t i = lane; i < 2 * Wp; i += 32) ((uint4 *)gact)[i] = ((const uint4 *)act)[i];
+    for (uint32_t i = lane; i < 2 * m * Wp; i += 32) ((uint4 *)gcnt)[i] = ((const uint4 *)cnt)[i];
+    __syncwarp();
   }
 }
 
-template <bool S, int BM>
-static int occ_of(const TrainSmem &lay) {
+// shared memory per warp of k_train_warp, in words (a multiple of 32)
+static uint32_t warp_slice_words(uint32_t Wpmax, uint32_t Bmax, uint32_t ib_words,
+                                 uint32_t ovf_cap) {
+  return (8 * Bmax * Wpmax + 2 * ib_words + ovf_cap + 32 + 31) / 32 * 32;
+}
+
+int train_warp_occupancy(uint32_t Wpmax, uint32_t Bmax, uint32_t smax, size_t *smem_bytes) {
+  const uint32_t ovf_cap = smax / 4 > 0 ? smax / 4 : 1;
+  const size_t bytes = (size_t)(TM_WARP_THREADS / 32) * warp_slice_words(Wpmax, Bmax, Wpmax, ovf_cap) * 4;
+  *smem_bytes = bytes;
+  cudaFuncSetAttribute(k_train_warp<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   int nb = 0;
-  cudaFuncSetAttribute(k_train<S, BM>, cudaFuncAttributeMaxDynamicSharedMemorySize, lay.total);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_train<S, BM>, TM_TRAIN_THREADS, lay.total);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_train_warp<7>, TM_WARP_THREADS, bytes);
   return nb;
 }
 
-int train_occupancy(const TrainSmem &lay, bool smem_state, uint32_t Bmax) {
+cudaError_t launch_train_warp(const TrainDev *machines, const WorkItem *work, uint32_t nwork,
+                              uint32_t *counter, uint32_t e_begin, uint32_t e_end, uint32_t Wpmax,
+                              uint32_t Bmax, uint32_t smax, int grid, cudaStream_t st) {
+  const uint32_t ovf_cap = smax / 4 > 0 ? smax / 4 : 1;
+  const uint32_t slice = 8 * Bmax * Wpmax;
+  const uint32_t stride = warp_slice_words(Wpmax, Bmax, Wpmax, ovf_cap);
+  const size_t bytes = (size_t)(TM_WARP_THREADS / 32) * stride * 4;
+  k_train_warp<7><<<grid, TM_WARP_THREADS, bytes, st>>>(machines, work, nwork, counter, e_begin,
+                                                        e_end, slice, Wpmax, ovf_cap, stride);
+  return cudaGetLastError();
+}
+
+template <bool S, bool P, int BM>
+static int occ_of(const TrainSmem &lay) {
+  cudaFuncSetAttribute(k_train<S, P, BM>, cudaFuncAttributeMaxDynamicSharedMemorySize, lay.total);
+  if (!P) {
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_train<S, P, BM>, TM_TRAIN_THREADS,
+                                                  lay.total);
+    return nb;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = 2;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(2, 1, 1);
+  cfg.blockDim = dim3(2 * TM_TRAIN_THREADS, 1, 1);
+  cfg.dynamicSmemBytes = lay.total;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  int nc = 0;
+  if (cudaOccupancyMaxActiveClusters(&nc, k_train<S, P, BM>, &cfg) != cudaSuccess) return 0;
+  return nc;
+}
+
+// Single: co-resident CTAs per SM.  Pair: co-resident clusters per device.
+int train_occupancy(const TrainSmem &lay, int mode, uint32_t Bmax) {
   const bool small = Bmax <= 8;
-  if (smem_state) return small ? occ_of<true, 7>(lay) : occ_of<true, 31>(lay);
-  return small ? occ_of<false, 7>(lay) : occ_of<false, 31>(lay);
+  if (mode == TM_MODE_PAIR) return occ_of<true, true, 7>(lay);
+  if (mode == TM_MODE_SMEM) return small ? occ_of<true, false, 7>(lay) : occ_of<true, false, 31>(lay);
+  return small ? occ_of<false, false, 7>(lay) : occ_of<false, false, 31>(lay);
 }
 
 cudaError_t launch_train(const TrainDev *machines, const WorkItem *work, uint32_t nwork,
                          uint32_t *counter, uint32_t e_begin, uint32_t e_end, const TrainSmem &lay,
-                         bool smem_state, uint32_t Bmax, int grid, uint32_t *err, cudaStream_t st) {
+                         int mode, uint32_t Bmax, int grid, uint32_t *err, cudaStream_t st) {
   const bool small = Bmax <= 8;
-#define TM_LAUNCH(S, BM)                                                                   \
-  k_train<S, BM><<<grid, TM_TRAIN_THREADS, lay.total, st>>>(machines, work, nwork, counter, \
-                                                          e_begin, e_end, lay, err)
-  if (smem_state) {
+  if (mode == TM_MODE_PAIR) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = 2;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(grid, 1, 1);
+    cfg.blockDim = dim3(2 * TM_TRAIN_THREADS, 1, 1);
+    cfg.dynamicSmemBytes = lay.total;
+    cfg.stream = st;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_train<true, true, 7>, machines, work, nwork, counter,
+                              e_begin, e_end, lay, err);
+  }
+#define TM_LAUNCH(S, BM)                                                                     \
+  k_train<S, false, BM><<<grid, TM_TRAIN_THREADS, lay.total, st>>>(machines, work, nwork, counter, \
+                                                                   e_begin, e_end, lay, err)
+  if (mode == TM_MODE_SMEM) {
     if (small) TM_LAUNCH(true, 7);
     else TM_LAUNCH(true, 31);
   } else {

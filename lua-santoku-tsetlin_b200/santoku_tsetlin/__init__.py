@@ -101,6 +101,7 @@ class Stats(ctypes.Structure):
         ("predict_kernel_ms", ctypes.c_double),
         ("kernel_launches", ctypes.c_uint64),
         ("train_unit_steps", ctypes.c_uint64),
+        ("train_mode", ctypes.c_int32),
     ]
 
     def as_dict(self):

@@ -66,8 +66,13 @@ def predict_args(inp):
     return (inp["xt"], inp["nt"])
 
 
+@pytest.mark.parametrize("variant", ["auto", "cta"])
 @pytest.mark.parametrize("case", PHILOX_CASES, ids=[c["name"] for c in PHILOX_CASES])
-def test_train_matches_reference_fixture(tm, case):
+def test_train_matches_reference_fixture(tm, monkeypatch, case, variant):
+    # "auto": short rows train with one warp per unit; "cta": the one-CTA-per-
+    # unit kernel on the same rows
+    if variant == "cta":
+        monkeypatch.setenv("TSETLIN_B200_NO_WARP", "1")
     case = dict(case, create=dict(case["create"]))
     inp = make_inputs(case)
     fx = load_fixture(case["name"])
@@ -283,3 +288,35 @@ def test_train_batch_equals_individual(tm):
     for mach, (a, s) in zip(machines, alone):
         a2, s2 = mach.export_state()
         assert np.array_equal(a, a2) and np.array_equal(s, s2)
+
+
+@pytest.mark.parametrize("features,state,pair,mode", [
+    (784, 8, False, 3),     # short rows: one warp per unit
+    (16384, 8, True, 2),    # 256 KB units split over a 2-CTA cluster (on request)
+    (16384, 8, False, 1),   # same rows with the automata in global memory (default)
+    (300, 12, False, 0),    # more than 8 state bits, shared-memory automata
+    (12000, 10, False, 1),  # more than 8 state bits on wide rows: global memory
+], ids=["warp", "pair", "global", "smem_b12", "global_b10"])
+def test_train_variants_match_oracle(tm, monkeypatch, features, state, pair, mode):
+    from santoku_tsetlin import datagen
+    if pair:
+        monkeypatch.setenv("TSETLIN_B200_PAIR", "1")
+    rng = np.random.default_rng(features + state)
+    n, classes = 160, 3
+    x = datagen.flip_pack(rng.random((n + 40, features)) < 0.02)
+    y = rng.integers(0, classes, size=n).astype(np.int64)
+    cfg = dict(type="classifier", classes=classes, features=features, clauses=16,
+               clause_tolerance=32, clause_maximum=300, state=state, include_bits=2,
+               specificity=25.0, target=20)
+    inp = dict(n=n, x=x[:n].ravel(), labels=y)
+    m = _oracle_pair("classifier", cfg, inp, 2, seed=21)
+    kind, tbl = ref_table(cfg, seed=21)
+    t = tm.create(kind, tbl)
+    t.stats_enable(True)
+    t.train(train_table(kind, inp, 2))
+    assert t.stats()["train_mode"] == mode
+    a, s = t.export_state()
+    assert np.array_equal(a, m.actions())
+    assert np.array_equal(s, m.state())
+    xt = x[n:].ravel()
+    assert np.array_equal(t.predict_scores(xt, 40), m.predict(xt, 40, scores=True)[1])
