@@ -323,13 +323,8 @@ def run_ours(args, w):
         e1.record()
         torch.cuda.synchronize()
         barrier()
-        ms = e0.elapsed_time(e1)
-        if ws > 1:
-            import torch.distributed as dist
-            tt = torch.tensor([ms], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            ms = float(tt.item())
-        return ms
+        from santoku_tsetlin import multi
+        return multi.max_over_ranks(e0.elapsed_time(e1), device=dev)
 
     for _ in range(args.warmup):
         step_dev()
@@ -351,6 +346,14 @@ def run_ours(args, w):
     # events on the library's stream
     occ_units = 2 * 148
     alg = train_algorithmic_bytes(w, occ_units)
+    # DRAM bytes of one k_train launch from an ncu capture of the same kernel
+    # on the large sparse classifier's rows with 280 units and 40,000 samples
+    # (profiles/k_train_c1_small_ncu.md: 2.867 GB read + 22.143 GB written),
+    # scaled by units x samples to this launch.
+    traffic = None
+    if w["name"] == "large-sparse-classifier":
+        per_unit_sample = (2.866907e9 + 22.143480e9) / (280 * 40000)
+        traffic = per_unit_sample * (w["classes"] * w["clauses"] // 8) * w["n_train"]
     avg_ms = st["train_kernel_ms"] / max(1, st["train_launches"])
     achieved = alg / (avg_ms / 1e3) / 1e9
     wp = ((2 * w["features"] + 31) // 32 + 3) // 4 * 4
@@ -366,7 +369,7 @@ def run_ours(args, w):
                                                 else (w["classes"] + 7) // 8))},
         "gpu_launches": int(st["kernel_launches"]),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
-                     "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                     "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                      "kernel": "k_train", "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": alg, "avg_launch_ms": avg_ms},
         "kernels": {
@@ -399,10 +402,16 @@ def run_ours(args, w):
 def run_search(args):
     import torch
     import santoku_tsetlin as tm
-    from santoku_tsetlin import datagen
+    from santoku_tsetlin import datagen, multi
+    ws, rank, local = dist_init()
     count, n_train, n_test = args.machines, 60000, 6000
     epochs = args.epochs or 2
-    params = datagen.search_machines(count)
+    all_params = datagen.search_machines(count)
+    # machines are independent: LPT partition by units across ranks (strong
+    # scaling: the 64-machine round is fixed)
+    parts = multi.partition_lpt([p["clauses"] * (p["features"] + 31) // 32 for p in all_params], ws)
+    params = [all_params[i] for i in parts[rank]]
+    count_local = len(params)
     protos = np.random.default_rng(7919 + 1).random((10, 784)) < 0.2
     xs = {}
     for negated in (True, False):
@@ -411,7 +420,8 @@ def run_search(args):
         xs[negated] = (np.ascontiguousarray(x[:n_train]), np.ascontiguousarray(x[n_train:]))
     yv = y
     y_tr, y_te = np.ascontiguousarray(yv[:n_train]), yv[n_train:]
-    dev = torch.device("cuda", 0)
+    dev = torch.device("cuda", local if ws > 1 else 0)
+    torch.cuda.set_device(dev)
     xd = {k: (torch.from_numpy(v[0]).to(dev), torch.from_numpy(v[1]).to(dev)) for k, v in xs.items()}
     yd = torch.from_numpy(y_tr).to(dev)
 
@@ -430,13 +440,16 @@ def run_search(args):
                  "iterations": epochs} for p in params]
 
     def timed(fn):
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         fn()
         e1.record()
         torch.cuda.synchronize()
-        return e0.elapsed_time(e1)
+        return multi.max_over_ranks(e0.elapsed_time(e1), device=dev)
 
     warm = make()
     tm.train_batch(warm[:4], tables()[:4])
@@ -445,7 +458,7 @@ def run_search(args):
     batched = make()
     clocks = ClockSampler(0)
     clocks.start()
-    ms_b = timed(lambda: tm.train_batch(batched, tables()))
+    ms_b = timed(lambda: tm.train_batch(batched, tables()) if batched else None)
     ck = clocks.stop()
     plain = make()
     tabs = tables()
@@ -457,15 +470,16 @@ def run_search(args):
     acc_p = [float((m.predict(xd[p["negated"]][1], n_test).cpu().numpy() == y_te).mean())
              for m, p in zip(plain, params)]
     samples = count * n_train * epochs
-    units = sum(10 * p["clauses"] // 8 for p in params)
+    units = sum(10 * p["clauses"] // 8 for p in all_params)
     out = {
         "metric": "TM batched search train samples/s", "value": samples / (ms_b / 1e3),
-        "unit": "samples/s", "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": ms_b,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "unit": "samples/s", "n_gpus": ws, "steps": 1, "warmup": 1, "ms_per_step": ms_b,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic",
         "config": {"workload": "batched-search", "machines": count, "units": units,
                    "n_train": n_train, "epochs": epochs,
-                   "clauses_per_class": [p["clauses"] for p in params],
+                   "clauses_per_class": [p["clauses"] for p in all_params],
+                   "parallelism": "machines partitioned across ranks (LPT)" if ws > 1 else "single",
                    "step": "%d machines x %d epochs in one tm_train_batch" % (count, epochs)},
         "plain": {"value": samples / (ms_p / 1e3), "ms": ms_p,
                   "form": "one tm_train call (one launch group) per machine, in sequence"},
@@ -475,7 +489,11 @@ def run_search(args):
     }
     if ck:
         out["clocks"] = ck
-    print(json.dumps(out), flush=True)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
 
 
 # ---------------------------------------------------------------------------

@@ -168,6 +168,25 @@ int tm_get_info(const tm_machine *m, uint64_t *out);
 int tm_export_state(tm_machine *m, uint8_t *actions, uint8_t *state);
 int tm_import_state(tm_machine *m, const uint8_t *actions, const uint8_t *state);
 
+/* ---- evaluator metrics and input packing (device) --------------------- */
+/* evaluator.class_accuracy(predicted, expected, n_samples, n_classes):
+ * evaluator/capi.c:119-202.  out[3 + 3 * n_classes] = macro precision,
+ * recall, f1, then per class precision, recall, f1. */
+int tm_class_accuracy(const int64_t *predicted, const int64_t *expected, uint64_t n,
+                      uint32_t classes, int32_t on_device, int32_t device, double *out);
+/* evaluator.encoding_accuracy(predicted, expected, n_samples, n_hidden):
+ * evaluator/capi.c:497-574.  out[4 + n_hidden] = mean_hamming, ber_min,
+ * ber_max, ber_std, then the per-bit error rates. */
+int tm_encoding_accuracy(const uint8_t *predicted, const uint8_t *expected, uint64_t n,
+                         uint32_t hidden, int32_t on_device, int32_t device, double *out);
+/* santoku-matrix's bits_to_cvec(n, features, flip) on the set-bit list
+ * `sample * features + feature` (as built by the reference's dataset
+ * readers, dataset.lua:11-41): out[n * ceil((flip ? 2 : 1) * features / 8)];
+ * with flip, bits features..2*features-1 are the complements
+ * (doc/sth.md:70-78).  The input packing of the reference's tests. */
+int tm_bits_to_cvec(const int64_t *set_bits, uint64_t n_set, uint64_t n, uint32_t features,
+                    int32_t flip, int32_t on_device, int32_t device, uint8_t *out);
+
 /* Predict without allocating.  No counterpart in the reference.  For
  * callers that must not call cudaMalloc / cudaFree while they run -- a
  * serving loop that cannot absorb the device-wide synchronisation those

@@ -1225,7 +1225,7 @@ cudaError_t launch_lits(const uint32_t *act, const ClassDev *cls, uint32_t class
 // ---------------------------------------------------------------------------
 constexpr int PT_S = 64, PT_C = 64, PT_K = 32, PT_LD = PT_K + 4;
 
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 2)
     k_predict(const uint32_t *__restrict__ act, const int32_t *__restrict__ lits,
               const ClassDev *__restrict__ cls, uint32_t clauses, uint32_t tiles_per_class,
               uint32_t tol, const uint32_t *__restrict__ x, uint32_t n, uint32_t classes,
@@ -1238,11 +1238,15 @@ __global__ void __launch_bounds__(256)
   const uint32_t s0 = blockIdx.x * PT_S;
   const ClassDev C = cls[h];
   const uint32_t tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  uint32_t acc[4][4];
+  // Failed-literal counts popc(a & ~x) per (clause, sample), accumulated
+  // carry-save: `ones` and `twos` hold bit-sliced partial counts and only
+  // the weight-4 carries are popcounted -- one POPC per four words instead
+  // of four.  Count = 4 * acc + 2 * popc(twos) + popc(ones), exact.
+  uint32_t acc[4][4], ones[4][4], twos[4][4];
 #pragma unroll
   for (int a = 0; a < 4; a++)
 #pragma unroll
-    for (int b = 0; b < 4; b++) acc[a][b] = 0;
+    for (int b = 0; b < 4; b++) acc[a][b] = ones[a][b] = twos[a][b] = 0;
   const uint32_t *arow = act + C.act_off;
   const uint32_t *xrow = x + C.x_off;
   for (uint32_t k0 = 0; k0 < C.Wp; k0 += PT_K) {
@@ -1277,12 +1281,29 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
       for (int c = 0; c < 4; c++)
 #pragma unroll
-        for (int i = 0; i < 4; i++)
-          acc[c][i] += __popc(a4[c].x & ~x4[i].x) + __popc(a4[c].y & ~x4[i].y) +
-                       __popc(a4[c].z & ~x4[i].z) + __popc(a4[c].w & ~x4[i].w);
+        for (int i = 0; i < 4; i++) {
+          const uint32_t t0 = a4[c].x & ~x4[i].x, t1 = a4[c].y & ~x4[i].y;
+          const uint32_t t2 = a4[c].z & ~x4[i].z, t3 = a4[c].w & ~x4[i].w;
+          uint32_t o = ones[c][i];
+          // carry-save adders: (sum, carry) = (a ^ b ^ c, majority(a, b, c))
+          const uint32_t h1 = (o & t0) | (o & t1) | (t0 & t1);
+          o ^= t0 ^ t1;
+          const uint32_t h2 = (o & t2) | (o & t3) | (t2 & t3);
+          o ^= t2 ^ t3;
+          const uint32_t tw = twos[c][i];
+          const uint32_t f4 = (tw & h1) | (tw & h2) | (h1 & h2);
+          twos[c][i] = tw ^ h1 ^ h2;
+          ones[c][i] = o;
+          acc[c][i] += __popc(f4);
+        }
     }
     __syncthreads();
   }
+#pragma unroll
+  for (int c = 0; c < 4; c++)
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+      acc[c][i] = 4 * acc[c][i] + 2 * __popc(twos[c][i]) + __popc(ones[c][i]);
   int32_t part[4] = {0, 0, 0, 0};
 #pragma unroll
   for (int c = 0; c < 4; c++) {

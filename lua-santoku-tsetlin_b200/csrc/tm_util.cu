@@ -1,0 +1,276 @@
+// Device-side neighbours of the hot path: the evaluator metrics the
+// reference's search driver computes after every epoch, and the packing of
+// set-bit lists into flip-interleaved sample rows.
+//
+//   tm_class_accuracy     evaluator/capi.c:119-202 (per-class precision,
+//                         recall, F1 and their macro averages)
+//   tm_encoding_accuracy  evaluator/capi.c:497-574 (bitwise Hamming
+//                         agreement of codes: mean, min, max, std of the
+//                         per-bit error rates)
+//   tm_bits_to_cvec       santoku-matrix's bits_to_cvec(n, F, flip), the
+//                         packing the reference's tests apply to their
+//                         inputs (doc/sth.md:70-78)
+//
+// Counting runs in kernels; the per-class / per-bit finish (a few hundred
+// doubles) runs in one small kernel in the reference's summation order, so
+// the results are the reference's to the last bit.
+#include <math.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "../../include/tsetlin_b200.h"
+#include "tm_internal.h"
+
+namespace {
+
+struct DevScratch {
+  void *p = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t n) {
+    if (n <= cap) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc(&p, n);
+    if (e == cudaSuccess) cap = n;
+    return e;
+  }
+  ~DevScratch() {
+    if (p) cudaFree(p);
+  }
+};
+
+// capi.c:141-153 of the evaluator: TP/FP/FN per class; samples whose
+// predicted or true class is out of range are skipped.
+__global__ void k_class_counts(const int64_t *__restrict__ pred, const int64_t *__restrict__ truth,
+                               uint64_t n, uint32_t classes, unsigned long long *__restrict__ tp,
+                               unsigned long long *__restrict__ fp,
+                               unsigned long long *__restrict__ fn) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t yp = (uint32_t)pred[i], yt = (uint32_t)truth[i];
+    if (yp >= classes || yt >= classes) continue;
+    if (yp == yt) {
+      atomicAdd(&tp[yt], 1ull);
+    } else {
+      atomicAdd(&fp[yp], 1ull);
+      atomicAdd(&fn[yt], 1ull);
+    }
+  }
+}
+
+// capi.c:155-172 of the evaluator, in its order: out = [precision, recall,
+// f1 (macro), then per class precision, recall, f1]
+__global__ void k_class_finish(const unsigned long long *__restrict__ tp,
+                               const unsigned long long *__restrict__ fp,
+                               const unsigned long long *__restrict__ fn, uint32_t classes,
+                               double *__restrict__ out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double pa = 0.0, ra = 0.0, fa = 0.0;
+  for (uint32_t c = 0; c < classes; c++) {
+    const unsigned long long t = tp[c], f = fp[c], g = fn[c];
+    // explicit round-to-nearest operations: no fused multiply-add, so each
+    // operation rounds as in a plain IEEE evaluation of the formula
+    const double p = (t + f) > 0 ? __ddiv_rn((double)t, (double)(t + f)) : 0.0;
+    const double r = (t + g) > 0 ? __ddiv_rn((double)t, (double)(t + g)) : 0.0;
+    const double pr = __dadd_rn(p, r);
+    const double f1 = pr > 0 ? __ddiv_rn(__dmul_rn(__dmul_rn(2.0, p), r), pr) : 0.0;
+    out[3 + 3 * c] = p;
+    out[3 + 3 * c + 1] = r;
+    out[3 + 3 * c + 2] = f1;
+    pa = __dadd_rn(pa, p);
+    ra = __dadd_rn(ra, r);
+    fa = __dadd_rn(fa, f1);
+  }
+  out[0] = __ddiv_rn(pa, (double)classes);
+  out[1] = __ddiv_rn(ra, (double)classes);
+  out[2] = __ddiv_rn(fa, (double)classes);
+}
+
+// capi.c:520-535 of the evaluator: per-bit disagreements.  One thread per
+// (sample, code byte).
+__global__ void k_code_diffs(const uint8_t *__restrict__ pred, const uint8_t *__restrict__ truth,
+                             uint64_t n, uint32_t hidden, unsigned long long *__restrict__ bdiff) {
+  const uint32_t nb = (hidden + 7) / 8;
+  const uint64_t total = n * nb;
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t b = (uint32_t)(t % nb);
+    uint32_t d = (uint32_t)(pred[t] ^ truth[t]);
+    while (d) {
+      const uint32_t k = __ffs(d) - 1;
+      d &= d - 1;
+      const uint32_t j = b * 8 + k;
+      if (j < hidden) atomicAdd(&bdiff[j], 1ull);
+    }
+  }
+}
+
+// capi.c:544-570 of the evaluator: out = [mean_hamming, ber_min, ber_max,
+// ber_std, then per-bit error rate]
+__global__ void k_code_finish(const unsigned long long *__restrict__ bdiff, uint64_t n,
+                              uint32_t hidden, double *__restrict__ out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double mn = 1.0, mx = 0.0;
+  unsigned long long total = 0;
+  for (uint32_t j = 0; j < hidden; j++) {
+    const double t = __ddiv_rn((double)bdiff[j], (double)n);
+    if (t < mn) mn = t;
+    if (t > mx) mx = t;
+    out[4 + j] = t;
+    total += bdiff[j];
+  }
+  const double mean = __ddiv_rn((double)total, (double)(n * hidden));
+  double var = 0.0;
+  for (uint32_t j = 0; j < hidden; j++) {
+    const double d = __dsub_rn(__ddiv_rn((double)bdiff[j], (double)n), mean);
+    var = __dadd_rn(var, __dmul_rn(d, d));
+  }
+  out[0] = __dsub_rn(1.0, mean);
+  out[1] = __dsub_rn(1.0, mn);
+  out[2] = __dsub_rn(1.0, mx);
+  out[3] = hidden > 1 ? __dsqrt_rn(__ddiv_rn(var, (double)(hidden - 1))) : 0.0;
+}
+
+// bits_to_cvec: set bit f of sample s for every listed index s * F + f;
+// with flip, bit F + f of sample s is set when bit f is not.
+__global__ void k_scatter_bits(const int64_t *__restrict__ idx, uint64_t n_idx, uint64_t n,
+                               uint32_t features, uint32_t row_bits, uint32_t row_words,
+                               uint32_t *__restrict__ rows) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_idx;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const int64_t v = idx[i];
+    if (v < 0) continue;
+    const uint64_t s = (uint64_t)v / features, f = (uint64_t)v % features;
+    if (s >= n) continue;
+    atomicOr(&rows[s * row_words + (uint32_t)(f >> 5)], 1u << (f & 31));
+    (void)row_bits;
+  }
+}
+
+__global__ void k_flip_bits(uint64_t n, uint32_t features, uint32_t row_words,
+                            uint32_t *__restrict__ rows) {
+  const uint64_t total = n * features;
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t s = t / features;
+    const uint32_t f = (uint32_t)(t % features);
+    uint32_t *row = rows + s * row_words;
+    const bool on = (row[f >> 5] >> (f & 31)) & 1u;
+    if (!on) {
+      const uint32_t g = features + f;
+      atomicOr(&row[g >> 5], 1u << (g & 31));
+    }
+  }
+}
+
+// 32-bit word rows -> byte rows of nb bytes (little-endian words)
+__global__ void k_words_to_bytes(const uint32_t *__restrict__ rows, uint64_t n, uint32_t row_words,
+                                 uint32_t nb, uint8_t *__restrict__ out) {
+  const uint64_t total = n * nb;
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t s = t / nb;
+    const uint32_t b = (uint32_t)(t % nb);
+    out[t] = (uint8_t)(rows[s * row_words + (b >> 2)] >> (8 * (b & 3)));
+  }
+}
+
+int grid_for(uint64_t work) {
+  const uint64_t g = (work + 255) / 256;
+  return (int)(g < 148ull * 16 ? (g ? g : 1) : 148ull * 16);
+}
+
+}  // namespace
+
+#define CKU(call)                                                                \
+  do {                                                                           \
+    cudaError_t e_ = (call);                                                     \
+    if (e_ != cudaSuccess) return tmb_fail(TM_ERR_CUDA, cudaGetErrorString(e_)); \
+  } while (0)
+
+extern "C" int tm_class_accuracy(const int64_t *predicted, const int64_t *expected, uint64_t n,
+                                 uint32_t classes, int32_t on_device, int32_t device, double *out) {
+  if (!out || (n && (!predicted || !expected))) return tmb_fail(TM_ERR_ARG, "class_accuracy: bad arguments");
+  if (classes == 0) return tmb_fail(TM_ERR_ARG, "class_accuracy: n_classes must be > 0");
+  CKU(cudaSetDevice(device));
+  DevScratch buf;
+  const size_t cnt = 3 * (size_t)classes * 8, outb = (3 + 3 * (size_t)classes) * 8;
+  const size_t inb = on_device ? 0 : 2 * n * 8;
+  CKU(buf.ensure(cnt + outb + inb + 64));
+  unsigned long long *tp = (unsigned long long *)buf.p, *fp = tp + classes, *fn = fp + classes;
+  double *dout = (double *)((uint8_t *)buf.p + cnt);
+  const int64_t *dp = predicted, *de = expected;
+  if (!on_device && n) {
+    int64_t *st = (int64_t *)((uint8_t *)buf.p + cnt + outb);
+    CKU(cudaMemcpy(st, predicted, n * 8, cudaMemcpyHostToDevice));
+    CKU(cudaMemcpy(st + n, expected, n * 8, cudaMemcpyHostToDevice));
+    dp = st;
+    de = st + n;
+  }
+  CKU(cudaMemset(tp, 0, cnt));
+  if (n) k_class_counts<<<grid_for(n), 256>>>(dp, de, n, classes, tp, fp, fn);
+  k_class_finish<<<1, 32>>>(tp, fp, fn, classes, dout);
+  CKU(cudaGetLastError());
+  CKU(cudaMemcpy(out, dout, outb, cudaMemcpyDeviceToHost));
+  return TM_OK;
+}
+
+extern "C" int tm_encoding_accuracy(const uint8_t *predicted, const uint8_t *expected, uint64_t n,
+                                    uint32_t hidden, int32_t on_device, int32_t device, double *out) {
+  if (!out || !n || !predicted || !expected) return tmb_fail(TM_ERR_ARG, "encoding_accuracy: bad arguments");
+  if (hidden == 0) return tmb_fail(TM_ERR_ARG, "encoding_accuracy: n_hidden must be > 0");
+  CKU(cudaSetDevice(device));
+  const uint64_t nb = (hidden + 7) / 8;
+  DevScratch buf;
+  const size_t cnt = (size_t)hidden * 8, outb = (4 + (size_t)hidden) * 8;
+  const size_t inb = on_device ? 0 : 2 * n * nb;
+  CKU(buf.ensure(cnt + outb + inb + 64));
+  unsigned long long *bd = (unsigned long long *)buf.p;
+  double *dout = (double *)((uint8_t *)buf.p + cnt);
+  const uint8_t *dp = predicted, *de = expected;
+  if (!on_device) {
+    uint8_t *st = (uint8_t *)buf.p + cnt + outb;
+    CKU(cudaMemcpy(st, predicted, n * nb, cudaMemcpyHostToDevice));
+    CKU(cudaMemcpy(st + n * nb, expected, n * nb, cudaMemcpyHostToDevice));
+    dp = st;
+    de = st + n * nb;
+  }
+  CKU(cudaMemset(bd, 0, cnt));
+  k_code_diffs<<<grid_for(n * nb), 256>>>(dp, de, n, hidden, bd);
+  k_code_finish<<<1, 32>>>(bd, n, hidden, dout);
+  CKU(cudaGetLastError());
+  CKU(cudaMemcpy(out, dout, outb, cudaMemcpyDeviceToHost));
+  return TM_OK;
+}
+
+extern "C" int tm_bits_to_cvec(const int64_t *set_bits, uint64_t n_set, uint64_t n,
+                               uint32_t features, int32_t flip, int32_t on_device, int32_t device,
+                               uint8_t *out) {
+  if (!out || (n_set && !set_bits) || features == 0) return tmb_fail(TM_ERR_ARG, "bits_to_cvec: bad arguments");
+  CKU(cudaSetDevice(device));
+  const uint64_t row_bits = flip ? 2ull * features : features;
+  const uint32_t nb = (uint32_t)((row_bits + 7) / 8);
+  const uint32_t rw = (uint32_t)((row_bits + 31) / 32);
+  DevScratch buf;
+  const size_t rows_b = n * rw * 4, idx_b = on_device ? 0 : n_set * 8, out_b = on_device ? 0 : n * nb;
+  CKU(buf.ensure(rows_b + idx_b + out_b + 256));
+  uint32_t *rows = (uint32_t *)buf.p;
+  const int64_t *di = set_bits;
+  uint8_t *dout = out;
+  if (!on_device) {
+    int64_t *st = (int64_t *)((uint8_t *)buf.p + ((rows_b + 7) & ~(size_t)7));
+    if (n_set) CKU(cudaMemcpy(st, set_bits, n_set * 8, cudaMemcpyHostToDevice));
+    di = st;
+    dout = (uint8_t *)st + idx_b;
+  }
+  CKU(cudaMemset(rows, 0, rows_b ? rows_b : 4));
+  if (n_set) k_scatter_bits<<<grid_for(n_set), 256>>>(di, n_set, n, features, (uint32_t)row_bits, rw, rows);
+  if (flip && n) k_flip_bits<<<grid_for(n * features), 256>>>(n, features, rw, rows);
+  if (n) k_words_to_bytes<<<grid_for(n * nb), 256>>>(rows, n, rw, nb, dout);
+  CKU(cudaGetLastError());
+  if (!on_device && n) CKU(cudaMemcpy(out, dout, n * nb, cudaMemcpyDeviceToHost));
+  else CKU(cudaDeviceSynchronize());
+  return TM_OK;
+}

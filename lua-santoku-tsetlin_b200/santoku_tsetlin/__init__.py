@@ -123,7 +123,8 @@ EXPORTS = (
     "tm_predict_scores", "tm_persist", "tm_persist_buf", "tm_free", "tm_load",
     "tm_checkpoint", "tm_restore", "tm_reconfigure", "tm_restrict", "tm_type",
     "tm_destroy", "tm_last_error", "tm_align", "tm_get_info", "tm_export_state",
-    "tm_import_state", "tm_predict_noalloc", "tm_stats_enable", "tm_get_stats", "tm_reset_stats", "tm_serve_open", "tm_serve_submit", "tm_serve_poll",
+    "tm_import_state", "tm_class_accuracy", "tm_encoding_accuracy", "tm_bits_to_cvec",
+    "tm_predict_noalloc", "tm_stats_enable", "tm_get_stats", "tm_reset_stats", "tm_serve_open", "tm_serve_submit", "tm_serve_poll",
     "tm_serve_latency_us", "tm_serve_close",
 )
 
@@ -161,6 +162,9 @@ def lib():
     L.tm_export_state.argtypes = [vp, vp, vp]
     L.tm_import_state.argtypes = [vp, vp, vp]
     L.tm_predict_noalloc.argtypes = [vp, vp, u64, vp, vp]
+    L.tm_class_accuracy.argtypes = [vp, vp, u64, u32, i32, i32, vp]
+    L.tm_encoding_accuracy.argtypes = [vp, vp, u64, u32, i32, i32, vp]
+    L.tm_bits_to_cvec.argtypes = [vp, u64, u64, u32, i32, i32, i32, vp]
     L.tm_stats_enable.argtypes = [vp, i32]
     L.tm_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
     L.tm_reset_stats.argtypes = [vp]
@@ -517,3 +521,55 @@ def train_batch(machines, tbls):
     hs = (ctypes.c_void_p * len(machines))(*[m.handle.value for m in machines])
     _check(lib().tm_train_batch(hs, arr, len(machines)))
     del keeps
+
+
+# ---------------------------------------------------------------------------
+# evaluator metrics (santoku.tsetlin.evaluator) and input packing
+# ---------------------------------------------------------------------------
+def class_accuracy(predicted, expected, n_samples, n_classes, device=0):
+    """evaluator.class_accuracy (evaluator/capi.c:119-202), counted on the
+    GPU: {"classes": [{"precision", "recall", "f1"}, ...], "precision",
+    "recall", "f1"} (macro averages)."""
+    p = _Buf(predicted, np.int64)
+    e = _Buf(expected, np.int64)
+    if p.device != e.device:
+        raise TsetlinError("class_accuracy: predicted and expected on different devices")
+    out = np.zeros(3 + 3 * int(n_classes), dtype=np.float64)
+    _check(lib().tm_class_accuracy(p.ptr, e.ptr, int(n_samples), int(n_classes),
+                                   1 if p.device else 0, device, out.ctypes.data))
+    per = out[3:].reshape(-1, 3)
+    return {"classes": [{"precision": float(a), "recall": float(b), "f1": float(c)}
+                        for a, b, c in per],
+            "precision": float(out[0]), "recall": float(out[1]), "f1": float(out[2])}
+
+
+def encoding_accuracy(predicted, expected, n_samples, n_hidden, device=0):
+    """evaluator.encoding_accuracy (evaluator/capi.c:497-574), counted on the
+    GPU: {"bits": [...], "mean_hamming", "ber_min", "ber_max", "ber_std"}."""
+    p = _Buf(predicted, np.uint8)
+    e = _Buf(expected, np.uint8)
+    if p.device != e.device:
+        raise TsetlinError("encoding_accuracy: predicted and expected on different devices")
+    out = np.zeros(4 + int(n_hidden), dtype=np.float64)
+    _check(lib().tm_encoding_accuracy(p.ptr, e.ptr, int(n_samples), int(n_hidden),
+                                      1 if p.device else 0, device, out.ctypes.data))
+    return {"bits": [float(v) for v in out[4:]], "mean_hamming": float(out[0]),
+            "ber_min": float(out[1]), "ber_max": float(out[2]), "ber_std": float(out[3])}
+
+
+def bits_to_cvec(set_bits, n_samples, n_features, flip=False, device=0):
+    """santoku-matrix's bits_to_cvec on the GPU: set-bit list (sample *
+    n_features + feature) -> packed rows, flip-interleaved when `flip`."""
+    b = _Buf(set_bits, np.int64)
+    nb = ((2 if flip else 1) * int(n_features) + 7) // 8
+    if b.device:
+        import torch
+        out = torch.empty(int(n_samples) * nb, dtype=torch.uint8,
+                          device=torch.device("cuda", device))
+        _check(lib().tm_bits_to_cvec(b.ptr, b.nbytes // 8, int(n_samples), int(n_features),
+                                     1 if flip else 0, 1, device, out.data_ptr()))
+        return out
+    out = np.zeros(int(n_samples) * nb, dtype=np.uint8)
+    _check(lib().tm_bits_to_cvec(b.ptr, b.nbytes // 8, int(n_samples), int(n_features),
+                                 1 if flip else 0, 0, device, out.ctypes.data))
+    return out

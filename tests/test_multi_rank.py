@@ -1,0 +1,90 @@
+"""Multi-rank host path on CPU: world size 2 over gloo.
+
+The per-rank device work is replaced by the oracle's vote sums for the
+rank's class range (test infrastructure); what is under test is the
+partitioning, the exchange of per-class sums, the reference's argmax / sign
+finish (capi.c:934-942, 982-990) and the max-over-ranks timing reduction.
+"""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _worker(rank, world, port, out):
+    import sys
+    import torch.distributed as dist
+    here = os.path.dirname(os.path.abspath(__file__))
+    root = os.path.dirname(here)
+    sys.path.insert(0, os.path.join(root, "lua-santoku-tsetlin_b200"))
+    sys.path.insert(0, os.path.join(root, "oracle"))
+    import oracle as O
+    from santoku_tsetlin import multi
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        res = {}
+        for kind, classes in (("classifier", 7), ("encoder", 13)):
+            rng = np.random.default_rng(3)
+            F, n = 40, 60
+            m = O.Machine(type=kind, classes=classes, features=F, clauses=16, clause_tolerance=6,
+                          clause_maximum=12, specificity=4.0)
+            x = np.packbits(np.concatenate([(b := rng.random((n, F)) < 0.3), ~b], axis=1),
+                            axis=1, bitorder="little").ravel()
+            lab = rng.integers(0, classes, size=n).astype(np.int64)
+            cod = np.packbits(rng.random((n, classes)) < 0.5, axis=1, bitorder="little").ravel()
+            m.train(x, n, 2, labels=lab if kind == "classifier" else None,
+                    codes=cod if kind == "encoder" else None, seed=5)
+            want, scores = m.predict(x, n, scores=True)
+            lo, hi = multi.class_range(classes, world, rank)
+            got, full = multi.gather_predict(scores[:, lo:hi], classes, kind)
+            res[kind] = (np.array_equal(got, want.ravel()), np.array_equal(full, scores))
+        res["max"] = multi.max_over_ranks(10.0 + rank)
+        res["parts"] = multi.partition_lpt([5, 1, 4, 4, 2, 9, 3], world)
+        out[rank] = res
+    finally:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def test_two_ranks_gloo(oracle_lib):
+    world = 2
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    out = ctx.Manager().dict()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=240)
+        assert p.exitcode == 0
+    for r in range(world):
+        res = out[r]
+        assert res["classifier"] == (True, True)
+        assert res["encoder"] == (True, True)
+        assert res["max"] == 11.0
+        assert res["parts"] == out[0]["parts"]
+    parts = out[0]["parts"]
+    assert sorted(parts[0] + parts[1]) == list(range(7))
+
+
+def test_partition_and_ranges():
+    from santoku_tsetlin import multi
+    p = multi.partition_lpt([8, 1, 1, 1, 1, 1, 1, 1, 1], 2)
+    assert p == [[0], [1, 2, 3, 4, 5, 6, 7, 8]]
+    covered = []
+    for r in range(3):
+        lo, hi = multi.class_range(10, 3, r)
+        covered += list(range(lo, hi))
+    assert covered == list(range(10))
