@@ -109,6 +109,19 @@ int tm_train(tm_machine *m, const tm_train_args *a);
  * here (use tm_train for per-epoch control). */
 int tm_train_batch(tm_machine *const *machines, const tm_train_args *args, uint32_t count);
 
+/* Per-epoch callback of a batch: after local epoch `epoch` (1-based) of the
+ * machines still training, set stop[i] = 1 to stop machine i (it keeps its
+ * state as of that epoch); return non-zero to stop every machine.  Plays
+ * the role of each trial's `each` in the reference's search driver
+ * (optimize.lua:586-653). */
+typedef int (*tm_batch_epoch_cb)(void *user, uint32_t epoch, int32_t *stop, uint32_t count);
+
+/* tm_train_batch with per-epoch control: every machine ends exactly as
+ * tm_train would leave it with an `each` that stops it at the same epoch.
+ * No single counterpart in the reference (see tm_train_batch). */
+int tm_train_batch_each(tm_machine *const *machines, const tm_train_args *args, uint32_t count,
+                        tm_batch_epoch_cb each, void *user);
+
 /* machine:predict(problems, n) / (problems, dim_offsets, n): capi.c:1088-1110.
  * Classifier: out_classes[n] (int64, argmax, ties to the lowest class).
  * Encoder: out_codes[n * ceil(hidden/8)]. */

@@ -109,7 +109,10 @@ struct tm_machine {
   int last_mode = -1;     // k_train variant of the last launch
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   tm_stats stats{};
-  DevBuf x, raw, labels, codes, perm, perm_scratch, sums, outc, work, tdev, cls_job, errf;
+  // tx: training rows (kept for all epochs of a train call); x: predict rows.
+  // Separate, so that a predict inside an `each` callback does not replace
+  // the rows the next epoch trains on.
+  DevBuf x, tx, raw, labels, codes, perm, perm_scratch, sums, outc, work, tdev, cls_job, errf;
 };
 
 // Kernels launched by a CUB 64-bit radix sort of pairs: upsweep histogram,
@@ -304,7 +307,7 @@ extern "C" void tm_destroy(tm_machine *m) {
   DevGuard g(m->device);
   if (m->st) cudaStreamSynchronize(m->st);
   free_device(m);
-  for (DevBuf *b : {&m->x, &m->raw, &m->labels, &m->codes, &m->perm, &m->perm_scratch, &m->sums,
+  for (DevBuf *b : {&m->x, &m->tx, &m->raw, &m->labels, &m->codes, &m->perm, &m->perm_scratch, &m->sums,
                     &m->outc, &m->work, &m->tdev, &m->cls_job, &m->errf})
     b->release();
   if (m->ev0) cudaEventDestroy(m->ev0);
@@ -697,7 +700,7 @@ extern "C" int tm_train(tm_machine *m, const tm_train_args *a) {
   std::vector<TrainJob> jobs(1);
   jobs[0].m = m;
   jobs[0].a = a;
-  rc = prepare_job(jobs[0], m->x, m->labels, m->codes, m->cls_job);
+  rc = prepare_job(jobs[0], m->tx, m->labels, m->codes, m->cls_job);
   if (rc) return rc;
   // capi.c:1136-1146: every train call starts from the initial state
   cudaError_t e = launch_setup(m->d_act, m->d_cnt, m->d_cls, m->classes, m->clauses, m->B,
@@ -726,7 +729,21 @@ extern "C" int tm_train(tm_machine *m, const tm_train_args *a) {
   return finish_train(m);
 }
 
+static int train_batch_impl(tm_machine *const *ms, const tm_train_args *args, uint32_t count,
+                            tm_batch_epoch_cb each, void *user);
+
 extern "C" int tm_train_batch(tm_machine *const *ms, const tm_train_args *args, uint32_t count) {
+  return train_batch_impl(ms, args, count, nullptr, nullptr);
+}
+
+extern "C" int tm_train_batch_each(tm_machine *const *ms, const tm_train_args *args, uint32_t count,
+                                   tm_batch_epoch_cb each, void *user) {
+  if (!each) return fail(TM_ERR_ARG, "train_batch_each: callback missing");
+  return train_batch_impl(ms, args, count, each, user);
+}
+
+static int train_batch_impl(tm_machine *const *ms, const tm_train_args *args, uint32_t count,
+                            tm_batch_epoch_cb each, void *user) {
   if (!ms || !args) return fail(TM_ERR_ARG, "null argument");
   if (count == 0) return TM_OK;
   tm_machine *m0 = ms[0];
@@ -777,7 +794,7 @@ extern "C" int tm_train_batch(tm_machine *const *ms, const tm_train_args *args, 
       // stage on machine i's buffers, ordered on the owner stream
       cudaStream_t keep = m->st;
       m->st = m0->st;
-      int rc = prepare_job(J, m->x, m->labels, m->codes, m->cls_job);
+      int rc = prepare_job(J, m->tx, m->labels, m->codes, m->cls_job);
       m->st = keep;
       if (rc) return rc;
     }
@@ -792,11 +809,30 @@ extern "C" int tm_train_batch(tm_machine *const *ms, const tm_train_args *args, 
     E = std::max(E, args[i].iterations);
     maxn = std::max<uint64_t>(maxn, args[i].samples);
   }
-  const uint32_t group = (uint32_t)std::max<uint64_t>(
-      1, std::min<uint64_t>(E, (512ull << 20) / (4 * maxn * std::max<uint32_t>(count, 1))));
-  for (uint32_t e0 = 0; e0 < E; e0 += group) {
-    int rc = run_epochs(jobs, e0, std::min(E, e0 + group), m0);
-    if (rc) return rc;
+  if (!each) {
+    const uint32_t group = (uint32_t)std::max<uint64_t>(
+        1, std::min<uint64_t>(E, (512ull << 20) / (4 * maxn * std::max<uint32_t>(count, 1))));
+    for (uint32_t e0 = 0; e0 < E; e0 += group) {
+      int rc = run_epochs(jobs, e0, std::min(E, e0 + group), m0);
+      if (rc) return rc;
+    }
+  } else {
+    // one epoch per launch; stopped machines leave the launch
+    std::vector<int32_t> stop(count, 0);
+    for (uint32_t e0 = 0; e0 < E; e0++) {
+      std::vector<TrainJob> live;
+      for (uint32_t i = 0; i < count; i++)
+        if (!stop[i] && e0 < args[i].iterations) live.push_back(jobs[i]);
+      if (live.empty()) break;
+      int rc = run_epochs(live, e0, e0 + 1, m0);
+      if (rc) return rc;
+      for (uint32_t i = 0; i < count; i++) ms[i]->lits_valid = false;
+      std::vector<int32_t> req(count, 0);
+      const int all = each(user, e0 + 1, req.data(), count);
+      for (uint32_t i = 0; i < count; i++)
+        if (req[i] || e0 + 1 >= args[i].iterations) stop[i] = 1;
+      if (all) break;
+    }
   }
   for (uint32_t i = 0; i < count; i++) {
     int rc = finish_train(ms[i]);

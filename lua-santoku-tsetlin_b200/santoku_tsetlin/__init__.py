@@ -64,6 +64,8 @@ class _Params(ctypes.Structure):
 
 
 EPOCH_CB = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_uint32)
+BATCH_EPOCH_CB = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_uint32,
+                                  ctypes.POINTER(ctypes.c_int32), ctypes.c_uint32)
 
 
 class _TrainArgs(ctypes.Structure):
@@ -119,7 +121,8 @@ class _ServerConfig(ctypes.Structure):
 
 _lib = None
 EXPORTS = (
-    "tm_params_init", "tm_create", "tm_train", "tm_train_batch", "tm_predict",
+    "tm_params_init", "tm_create", "tm_train", "tm_train_batch", "tm_train_batch_each",
+    "tm_predict",
     "tm_predict_scores", "tm_persist", "tm_persist_buf", "tm_free", "tm_load",
     "tm_checkpoint", "tm_restore", "tm_reconfigure", "tm_restrict", "tm_type",
     "tm_destroy", "tm_last_error", "tm_align", "tm_get_info", "tm_export_state",
@@ -143,6 +146,8 @@ def lib():
     L.tm_create.argtypes = [ctypes.POINTER(_Params), ctypes.POINTER(vp)]
     L.tm_train.argtypes = [vp, ctypes.POINTER(_TrainArgs)]
     L.tm_train_batch.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(_TrainArgs), u32]
+    L.tm_train_batch_each.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(_TrainArgs), u32,
+                                      BATCH_EPOCH_CB, vp]
     L.tm_predict.argtypes = [vp, vp, vp, u64, vp, vp, i32]
     L.tm_predict_scores.argtypes = [vp, vp, vp, u64, vp, i32]
     L.tm_persist.argtypes = [vp, ctypes.c_char_p]
@@ -505,9 +510,11 @@ def load(data, from_string=False, device=0):
     return Machine(h.value, device)
 
 
-def train_batch(machines, tbls):
+def train_batch(machines, tbls, each=None):
     """Train many machines in one persistent launch; each ends exactly as
-    its own train(tbl) would leave it."""
+    its own train(tbl) would leave it.  With `each(epoch)`: called after
+    every epoch; return False to stop all, or a sequence of per-machine
+    flags (true = stop that machine), or None to continue."""
     if len(machines) != len(tbls):
         raise TsetlinError("train_batch: one table per machine")
     arr = (_TrainArgs * len(tbls))()
@@ -519,7 +526,25 @@ def train_batch(machines, tbls):
         arr[i] = a
         keeps.append(keep)
     hs = (ctypes.c_void_p * len(machines))(*[m.handle.value for m in machines])
-    _check(lib().tm_train_batch(hs, arr, len(machines)))
+    if each is None:
+        _check(lib().tm_train_batch(hs, arr, len(machines)))
+    else:
+        def _cb(_user, epoch, stop, count):
+            try:
+                r = each(int(epoch))
+            except Exception as e:  # noqa: BLE001
+                sys.stderr.write("Error in callback: %s\n" % (e,))
+                return 1
+            if r is False:
+                return 1
+            if r is not None:
+                for i, flag in enumerate(r):
+                    if i < count and flag:
+                        stop[i] = 1
+            return 0
+        cb = BATCH_EPOCH_CB(_cb)
+        _check(lib().tm_train_batch_each(hs, arr, len(machines), cb, None))
+        del cb
     del keeps
 
 

@@ -320,3 +320,52 @@ def test_train_variants_match_oracle(tm, monkeypatch, features, state, pair, mod
     assert np.array_equal(s, m.state())
     xt = x[n:].ravel()
     assert np.array_equal(t.predict_scores(xt, 40), m.predict(xt, 40, scores=True)[1])
+
+
+def test_predict_inside_each_does_not_disturb_training(tm):
+    """The reference's search driver predicts a validation set in every
+    epoch's callback (optimize.lua:586-653); training must continue on its
+    own rows."""
+    case = dict(CASES[9], create=dict(CASES[9]["create"]))
+    inp = make_inputs(case)
+    kind, tbl = ref_table(case["create"], seed=6)
+    t = tm.create(kind, tbl)
+    scores = []
+
+    def each(epoch):
+        scores.append(t.predict_scores(inp["xt"], inp["nt"]))
+        return True
+
+    t.train(dict(train_table(kind, inp, 3), each=each))
+    t2 = tm.create(kind, tbl)
+    t2.train(train_table(kind, inp, 3))
+    assert np.array_equal(t.export_state()[1], t2.export_state()[1])
+    assert np.array_equal(scores[-1], t2.predict_scores(inp["xt"], inp["nt"]))
+
+
+def test_train_batch_each_stops_like_each(tm):
+    """A machine stopped by the batch callback ends as tm_train with an
+    `each` that stops at the same epoch; a predict inside the callback does
+    not disturb training."""
+    from santoku_tsetlin import datagen
+    x, y, _ = datagen.prototype_classifier(500, classes=10, seed=8)
+    xt = x[400:].ravel()
+    stops = [1, 3, 2]
+    tbls = [dict(classes=10, features=784, clauses=16, clause_tolerance=16, clause_maximum=16,
+                 specificity=s, target=8, seed=i, reusable=True) for i, s in enumerate((3.0, 9.0, 20.0))]
+    tt = dict(samples=400, problems=x[:400].ravel(), solutions=y[:400], iterations=4)
+    ms = [tm.create("classifier", b) for b in tbls]
+    seen = []
+
+    def each(epoch):
+        for m in ms:
+            m.predict(xt, 100)
+        seen.append(epoch)
+        return [epoch >= s for s in stops]
+
+    tm.train_batch(ms, [tt] * 3, each=each)
+    assert seen == [1, 2, 3]
+    for m, b, s in zip(ms, tbls, stops):
+        alone = tm.create("classifier", b)
+        alone.train(dict(tt, each=lambda e, s=s: e < s))
+        assert np.array_equal(m.export_state()[1], alone.export_state()[1])
