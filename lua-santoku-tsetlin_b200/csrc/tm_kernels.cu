@@ -358,38 +358,34 @@ __device__ __forceinline__ void rg_sub_pow2(uint32_t (&p)[BM], uint32_t &a, uint
   a = na;
 }
 
-// Four consecutive words at once: the B-1 planes and the action of words
-// w0..w0+3 (w0 a multiple of 4) are moved with 128-bit accesses and updated
-// word by word in registers.
+// Two consecutive words at once: the B-1 planes and the action of words
+// w0, w0+1 (w0 even) are moved with 64-bit accesses and updated word by word
+// in registers (two words keep the live state within 128 registers).
 template <int BM>
-__device__ __forceinline__ void ld_quad(const uint32_t *__restrict__ act_c,
+__device__ __forceinline__ void ld_pair(const uint32_t *__restrict__ act_c,
                                         const uint32_t *__restrict__ cnt_c, uint32_t Wp,
-                                        uint32_t m, uint32_t w0, uint32_t (&p)[4][BM],
-                                        uint32_t (&a)[4]) {
+                                        uint32_t m, uint32_t w0, uint32_t (&p)[2][BM],
+                                        uint32_t (&a)[2]) {
 #pragma unroll
   for (int b = 0; b < BM; b++)
     if (b < (int)m) {
-      const uint4 t = *(const uint4 *)(cnt_c + b * Wp + w0);
+      const uint2 t = *(const uint2 *)(cnt_c + b * Wp + w0);
       p[0][b] = t.x;
       p[1][b] = t.y;
-      p[2][b] = t.z;
-      p[3][b] = t.w;
     }
-  const uint4 t = *(const uint4 *)(act_c + w0);
+  const uint2 t = *(const uint2 *)(act_c + w0);
   a[0] = t.x;
   a[1] = t.y;
-  a[2] = t.z;
-  a[3] = t.w;
 }
 
 template <int BM>
-__device__ __forceinline__ void st_quad(uint32_t *__restrict__ act_c, uint32_t *__restrict__ cnt_c,
+__device__ __forceinline__ void st_pair(uint32_t *__restrict__ act_c, uint32_t *__restrict__ cnt_c,
                                         uint32_t Wp, uint32_t m, uint32_t w0,
-                                        const uint32_t (&p)[4][BM], const uint32_t (&a)[4]) {
+                                        const uint32_t (&p)[2][BM], const uint32_t (&a)[2]) {
 #pragma unroll
   for (int b = 0; b < BM; b++)
-    if (b < (int)m) *(uint4 *)(cnt_c + b * Wp + w0) = make_uint4(p[0][b], p[1][b], p[2][b], p[3][b]);
-  *(uint4 *)(act_c + w0) = make_uint4(a[0], a[1], a[2], a[3]);
+    if (b < (int)m) *(uint2 *)(cnt_c + b * Wp + w0) = make_uint2(p[0][b], p[1][b]);
+  *(uint2 *)(act_c + w0) = make_uint2(a[0], a[1]);
 }
 
 // rg_add with no decrements (Type II): plain carry ripple.
@@ -414,10 +410,6 @@ __device__ __forceinline__ void rg_inc(uint32_t (&p)[BM], uint32_t &a, uint32_t 
     na |= c;
   }
   a = na;
-}
-
-__device__ __forceinline__ uint32_t quad_get(const uint4 &v, int k) {
-  return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w));
 }
 
 // Mask of word w0 + k given the last-word mask `last` and W words.
@@ -745,66 +737,62 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
             }
             __syncthreads();
           }
-          // (clause, quad) items: item i -> the (i / Q)-th fed-back clause,
-          // words 4(i % Q) .. 4(i % Q) + 3
+          // (clause, pair) items: item i -> the (i / P)-th fed-back clause,
+          // words 2(i % P) and 2(i % P) + 1
           {
-            const uint32_t Q4 = Wp >> 2;
-            const uint32_t total = __popc(all) * Q4;
+            const uint32_t P2 = Wp >> 1;
+            const uint32_t total = __popc(all) * P2;
             const uint32_t NT = blockDim.x;
-            uint32_t kk = tid / Q4, qi = tid - kk * Q4;
+            uint32_t kk = tid / P2, qi = tid - kk * P2;
             for (uint32_t it = tid; it < total; it += NT) {
               const uint32_t c = __fns(all, 0, kk + 1);
-              const uint32_t w0 = 4 * qi;
+              const uint32_t w0 = 2 * qi;
               uint32_t *act_c = act + c * Wp, *cnt_c = cnt + (size_t)c * m * Wp;
+              uint32_t pq[2][BM], aq[2];
               if ((ibm >> c) & 1u) {
                 uint32_t *l0 = ibase + (size_t)c * 2 * lay.ib_words;
-                const uint4 m0 = *(const uint4 *)(l0 + w0);
-                const uint4 m1 = *(const uint4 *)(l0 + lay.ib_words + w0);
-                if ((m0.x | m0.y | m0.z | m0.w | m1.x | m1.y | m1.z | m1.w) != 0) {
-                  *(uint4 *)(l0 + w0) = make_uint4(0, 0, 0, 0);
-                  *(uint4 *)(l0 + lay.ib_words + w0) = make_uint4(0, 0, 0, 0);
-                  uint32_t pq[4][BM], aq[4];
-                  ld_quad<BM>(act_c, cnt_c, Wp, m, w0, pq, aq);
+                const uint2 m0 = *(const uint2 *)(l0 + w0);
+                const uint2 m1 = *(const uint2 *)(l0 + lay.ib_words + w0);
+                if ((m0.x | m0.y | m1.x | m1.y) != 0) {
+                  *(uint2 *)(l0 + w0) = make_uint2(0, 0);
+                  *(uint2 *)(l0 + lay.ib_words + w0) = make_uint2(0, 0);
+                  ld_pair<BM>(act_c, cnt_c, Wp, m, w0, pq, aq);
 #pragma unroll
-                  for (int k = 0; k < 4; k++) {
+                  for (int k = 0; k < 2; k++) {
                     const uint32_t am = word_mask(w0 + k, W, C.amask);
-                    rg_sub_pow2<BM>(pq[k], aq[k], m, 0, quad_get(m0, k), am);
-                    rg_sub_pow2<BM>(pq[k], aq[k], m, 1, quad_get(m1, k), am);
+                    rg_sub_pow2<BM>(pq[k], aq[k], m, 0, k ? m0.y : m0.x, am);
+                    rg_sub_pow2<BM>(pq[k], aq[k], m, 1, k ? m1.y : m1.x, am);
                   }
-                  st_quad<BM>(act_c, cnt_c, Wp, m, w0, pq, aq);
+                  st_pair<BM>(act_c, cnt_c, Wp, m, w0, pq, aq);
                 }
               } else {
-                const uint4 x4 = *(const uint4 *)(xr + w0);
+                const uint2 x2 = *(const uint2 *)(xr + w0);
                 const bool t1 = (t1m >> c) & 1u;
-                uint32_t vm[4];
-#pragma unroll
-                for (int k = 0; k < 4; k++) vm[k] = word_mask(w0 + k, W, C.vmask);
+                const uint32_t vm0 = word_mask(w0, W, C.vmask), vm1 = word_mask(w0 + 1, W, C.vmask);
                 // Type II changes nothing where every literal is 1
-                const bool need = t1 || ((~x4.x & vm[0]) | (~x4.y & vm[1]) | (~x4.z & vm[2]) |
-                                         (~x4.w & vm[3])) != 0;
+                const bool need = t1 || ((~x2.x & vm0) | (~x2.y & vm1)) != 0;
                 if (need) {
-                  uint32_t pq[4][BM], aq[4];
-                  ld_quad<BM>(act_c, cnt_c, Wp, m, w0, pq, aq);
+                  ld_pair<BM>(act_c, cnt_c, Wp, m, w0, pq, aq);
                   const bool incx = (incm >> c) & 1u;
 #pragma unroll
-                  for (int k = 0; k < 4; k++) {
-                    const uint32_t x = quad_get(x4, k);
+                  for (int k = 0; k < 2; k++) {
+                    const uint32_t x = k ? x2.y : x2.x, vm = k ? vm1 : vm0;
                     const uint32_t am = word_mask(w0 + k, W, C.amask);
-                    const uint32_t nx = ~x & ~rg_included<BM>(pq[k], aq[k], m, M.ib) & vm[k];
+                    const uint32_t nx = ~x & ~rg_included<BM>(pq[k], aq[k], m, M.ib) & vm;
                     // Type Ia (capi.c:177-180): inc where x=1 (if L <= maximum),
                     // dec where x=0 and not included.  Type II (capi.c:192-196):
                     // inc where x=0 and not included.
                     if (t1)
-                      rg_add<BM>(pq[k], aq[k], m, incx ? (x & vm[k]) : 0u, nx, am);
+                      rg_add<BM>(pq[k], aq[k], m, incx ? (x & vm) : 0u, nx, am);
                     else
                       rg_inc<BM>(pq[k], aq[k], m, nx, am);
                   }
-                  st_quad<BM>(act_c, cnt_c, Wp, m, w0, pq, aq);
+                  st_pair<BM>(act_c, cnt_c, Wp, m, w0, pq, aq);
                 }
               }
               qi += NT;
-              while (qi >= Q4) {
-                qi -= Q4;
+              while (qi >= P2) {
+                qi -= P2;
                 kk++;
               }
             }
