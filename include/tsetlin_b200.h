@@ -144,6 +144,20 @@ void tm_free(void *p);
 int tm_load(const uint8_t *data, uint64_t len, int32_t from_string, int32_t device,
             tm_machine **out);
 
+/* Versioned save with optional automaton state.  No counterpart in the
+ * reference: its record (tm_persist) has no version field and drops the
+ * count planes (capi.c:1509-1531, 1696), so a loaded machine cannot train
+ * and files cannot evolve.  The container holds a magic "STMV", a format
+ * version, `negative`, the default seed and the reusable flag, the
+ * reference's record byte for byte, the count planes when flags has
+ * TM_SAVE_STATE, and an FNV-1a 64 checksum.  tm_load reads both this
+ * container and the reference's plain record; a machine loaded with state
+ * trains, reconfigures and exports state like the one that was saved.
+ * tm_save_buf returns a malloc'd buffer (release with tm_free). */
+#define TM_SAVE_STATE 1u
+int tm_save(tm_machine *m, const char *path, uint32_t flags);
+int tm_save_buf(tm_machine *m, uint32_t flags, uint8_t **data, uint64_t *len);
+
 /* machine:checkpoint(cvec) / machine:restore(cvec): capi.c:1564-1588.
  * The checkpoint is the reference's action bytes (action_chunks bytes).
  * With buf == NULL, *len receives the size. */
@@ -199,6 +213,24 @@ int tm_encoding_accuracy(const uint8_t *predicted, const uint8_t *expected, uint
  * (doc/sth.md:70-78).  The input packing of the reference's tests. */
 int tm_bits_to_cvec(const int64_t *set_bits, uint64_t n_set, uint64_t n, uint32_t features,
                     int32_t flip, int32_t on_device, int32_t device, uint8_t *out);
+
+/* santoku-matrix's bits_to_cvec_ind(ind_offsets, feat_offsets, n, flip): the
+ * individualized sample layout the reference reads at capi.c:1020-1023,
+ * 1344-1354 and 1440-1451 (doc/sth.md:42-54).  Dimension h (a class, or a
+ * code bit of an encoder) has k_h = feat_offsets[h+1] - feat_offsets[h]
+ * features; its set bits are set_bits[ind_offsets[h] - ind_offsets[0] ..
+ * ind_offsets[h+1] - ind_offsets[0]) as `sample * k_h + feature` (negative
+ * entries and samples >= n are skipped).  Block h holds n rows of
+ * ceil((flip ? 2 : 1) * k_h / 8) bytes (flip: bits k_h..2k_h-1 are the
+ * complements) and starts at byte dim_offsets[h]; dim_offsets (host,
+ * dims + 1 entries) ends with the total size.  ind_offsets and feat_offsets
+ * are host arrays of dims + 1 entries; set_bits and out are device pointers
+ * when on_device.  out == NULL only fills dim_offsets (a sizing call);
+ * out_cap smaller than the total fails with TM_ERR_ARG. */
+int tm_bits_to_cvec_ind(const int64_t *set_bits, const int64_t *ind_offsets,
+                        const int64_t *feat_offsets, uint32_t dims, uint64_t n, int32_t flip,
+                        int32_t on_device, int32_t device, uint8_t *out, uint64_t out_cap,
+                        int64_t *dim_offsets);
 
 /* Predict without allocating.  No counterpart in the reference.  For
  * callers that must not call cudaMalloc / cudaFree while they run -- a

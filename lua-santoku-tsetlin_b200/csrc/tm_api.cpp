@@ -1097,21 +1097,12 @@ extern "C" int tm_persist_buf(tm_machine *m, uint8_t **data, uint64_t *len) {
   return TM_OK;
 }
 
-extern "C" int tm_load(const uint8_t *data, uint64_t len, int32_t from_string, int32_t device,
+// Parses one record in the reference's persisted layout and builds the
+// machine on `device`; with_state also allocates count planes (left for the
+// caller to fill).
+static int load_record(const uint8_t *data, uint64_t len, int32_t device, bool with_state,
                        tm_machine **out) {
-  if (!data || !out) return fail(TM_ERR_ARG, "null argument");
   *out = nullptr;
-  std::vector<uint8_t> file;
-  if (!from_string) {
-    FILE *f = fopen((const char *)data, "rb");
-    if (!f) return fail(TM_ERR_IO, "load: cannot open %s", (const char *)data);
-    uint8_t buf[1 << 16];
-    size_t r;
-    while ((r = fread(buf, 1, sizeof(buf), f)) > 0) file.insert(file.end(), buf, buf + r);
-    fclose(f);
-    data = file.data();
-    len = file.size();
-  }
   size_t o = 0;
   auto get = [&](void *p, size_t n) {
     if (o + n > len) return false;
@@ -1169,7 +1160,7 @@ extern "C" int tm_load(const uint8_t *data, uint64_t len, int32_t from_string, i
     return fail(TM_ERR_CUDA, "stream creation failed");
   }
   // capi.c:1696: the state is not persisted; a loaded machine predicts only
-  int rc = alloc_device(m, false);
+  int rc = alloc_device(m, with_state);
   if (!rc) rc = tm_import_state(m, acts, nullptr);
   if (rc) {
     tm_destroy(m);
@@ -1178,6 +1169,155 @@ extern "C" int tm_load(const uint8_t *data, uint64_t len, int32_t from_string, i
   m->trained = true;
   *out = m;
   return TM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// versioned container (no counterpart in the reference, whose persisted
+// record has no version and no state, capi.c:1509-1531, 1696):
+//   0  "STMV"            magic (a reference record starts with type 0 or 1)
+//   4  u32 version       1
+//   8  u32 flags         1 = count planes present, 2 = reusable
+//  12  u32 reserved      0
+//  16  f64 negative      (not in the reference record)
+//  24  u64 seed          default training seed
+//  32  u64 record_len    then the reference record, byte for byte
+//      [u64 state_len, state_len bytes]   count planes, reference layout
+//      u64 FNV-1a 64 of every byte before it
+// ---------------------------------------------------------------------------
+static const uint8_t kMagic[4] = {'S', 'T', 'M', 'V'};
+static const uint32_t kVersion = 1;
+
+static uint64_t fnv1a64(const uint8_t *p, size_t n) {
+  uint64_t h = 0xcbf29ce484222325ull;
+  for (size_t i = 0; i < n; i++) {
+    h ^= p[i];
+    h *= 0x100000001b3ull;
+  }
+  return h;
+}
+
+static int save_container(tm_machine *m, uint32_t flags, std::vector<uint8_t> &out) {
+  if (!m) return fail(TM_ERR_ARG, "null machine");
+  if (flags & ~(uint32_t)TM_SAVE_STATE) return fail(TM_ERR_ARG, "save: unknown flags");
+  const bool st = (flags & TM_SAVE_STATE) != 0;
+  if (st && (!m->has_state || !m->d_cnt)) return fail(TM_ERR_STATE, "save: machine has no state");
+  std::vector<uint8_t> rec;
+  int rc = serialize(m, rec);
+  if (rc) return rc;
+  out.clear();
+  auto put = [&](const void *p, size_t n) {
+    const uint8_t *b = (const uint8_t *)p;
+    out.insert(out.end(), b, b + n);
+  };
+  const uint32_t fl = (st ? 1u : 0u) | (m->reusable ? 2u : 0u), zero = 0;
+  const uint64_t rl = rec.size();
+  put(kMagic, 4); put(&kVersion, 4); put(&fl, 4); put(&zero, 4);
+  put(&m->negative, 8); put(&m->seed, 8); put(&rl, 8);
+  put(rec.data(), rec.size());
+  if (st) {
+    const uint64_t sl = m->state_chunks;
+    put(&sl, 8);
+    const size_t at = out.size();
+    out.resize(at + sl);
+    rc = tm_export_state(m, nullptr, out.data() + at);
+    if (rc) return rc;
+  }
+  const uint64_t h = fnv1a64(out.data(), out.size());
+  put(&h, 8);
+  return TM_OK;
+}
+
+extern "C" int tm_save(tm_machine *m, const char *path, uint32_t flags) {
+  if (!m || !path) return fail(TM_ERR_ARG, "null argument");
+  std::vector<uint8_t> d;
+  int rc = save_container(m, flags, d);
+  if (rc) return rc;
+  FILE *f = fopen(path, "wb");
+  if (!f) return fail(TM_ERR_IO, "save: cannot open %s", path);
+  const size_t w = fwrite(d.data(), 1, d.size(), f);
+  const int c = fclose(f);
+  if (w != d.size() || c != 0) return fail(TM_ERR_IO, "save: write failed");
+  return TM_OK;
+}
+
+extern "C" int tm_save_buf(tm_machine *m, uint32_t flags, uint8_t **data, uint64_t *len) {
+  if (!m || !data || !len) return fail(TM_ERR_ARG, "null argument");
+  std::vector<uint8_t> d;
+  int rc = save_container(m, flags, d);
+  if (rc) return rc;
+  *data = (uint8_t *)malloc(d.size());
+  if (!*data) return fail(TM_ERR_OOM, "save: out of memory");
+  memcpy(*data, d.data(), d.size());
+  *len = d.size();
+  return TM_OK;
+}
+
+static int load_container(const uint8_t *data, uint64_t len, int32_t device, tm_machine **out) {
+  if (len < 48) return fail(TM_ERR_IO, "load: truncated model data");
+  uint32_t version, flags, reserved;
+  double negative;
+  uint64_t seed, rl, h;
+  memcpy(&version, data + 4, 4);
+  memcpy(&flags, data + 8, 4);
+  memcpy(&reserved, data + 12, 4);
+  if (version == 0 || version > kVersion)
+    return fail(TM_ERR_ARG, "load: unsupported format version %u (this library reads 1)", version);
+  memcpy(&h, data + len - 8, 8);
+  if (fnv1a64(data, len - 8) != h) return fail(TM_ERR_IO, "load: checksum mismatch (corrupt model data)");
+  if ((flags & ~3u) || reserved) return fail(TM_ERR_ARG, "load: unknown flags");
+  memcpy(&negative, data + 16, 8);
+  memcpy(&seed, data + 24, 8);
+  memcpy(&rl, data + 32, 8);
+  const uint64_t body = len - 8;
+  if (rl > body - 40) return fail(TM_ERR_IO, "load: truncated model data");
+  const bool st = flags & 1u;
+  uint64_t o = 40 + rl, sl = 0;
+  if (st) {
+    if (body - o < 8) return fail(TM_ERR_IO, "load: truncated model data");
+    memcpy(&sl, data + o, 8);
+    o += 8;
+    if (sl > body - o) return fail(TM_ERR_IO, "load: truncated model data");
+  }
+  if (o + sl != body) return fail(TM_ERR_IO, "load: trailing bytes in model data");
+  tm_machine *m = nullptr;
+  int rc = load_record(data + 40, rl, device, st, &m);
+  if (rc) return rc;
+  m->negative = negative;
+  m->seed = seed;
+  m->reusable = (flags & 2u) != 0;
+  if (st) {
+    if (sl != m->state_chunks) {
+      tm_destroy(m);
+      return fail(TM_ERR_ARG, "load: state size mismatch: expected %u bytes, got %llu",
+                  m->state_chunks, (unsigned long long)sl);
+    }
+    rc = tm_import_state(m, nullptr, data + o);
+    if (rc) {
+      tm_destroy(m);
+      return rc;
+    }
+  }
+  *out = m;
+  return TM_OK;
+}
+
+extern "C" int tm_load(const uint8_t *data, uint64_t len, int32_t from_string, int32_t device,
+                       tm_machine **out) {
+  if (!data || !out) return fail(TM_ERR_ARG, "null argument");
+  *out = nullptr;
+  std::vector<uint8_t> file;
+  if (!from_string) {
+    FILE *f = fopen((const char *)data, "rb");
+    if (!f) return fail(TM_ERR_IO, "load: cannot open %s", (const char *)data);
+    uint8_t buf[1 << 16];
+    size_t r;
+    while ((r = fread(buf, 1, sizeof(buf), f)) > 0) file.insert(file.end(), buf, buf + r);
+    fclose(f);
+    data = file.data();
+    len = file.size();
+  }
+  if (len >= 4 && memcmp(data, kMagic, 4) == 0) return load_container(data, len, device, out);
+  return load_record(data, len, device, false, out);
 }
 
 // ---------------------------------------------------------------------------

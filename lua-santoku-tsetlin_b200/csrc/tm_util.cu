@@ -10,6 +10,10 @@
 //   tm_bits_to_cvec       santoku-matrix's bits_to_cvec(n, F, flip), the
 //                         packing the reference's tests apply to their
 //                         inputs (doc/sth.md:70-78)
+//   tm_bits_to_cvec_ind   santoku-matrix's bits_to_cvec_ind: the
+//                         individualized layout, one block of rows per
+//                         class / code bit (doc/sth.md:42-54, consumed at
+//                         capi.c:1020-1023, 1344-1354, 1440-1451)
 //
 // Counting runs in kernels; the per-class / per-bit finish (a few hundred
 // doubles) runs in one small kernel in the reference's summation order, so
@@ -177,6 +181,82 @@ __global__ void k_words_to_bytes(const uint32_t *__restrict__ rows, uint64_t n, 
   }
 }
 
+// bits_to_cvec_ind, step 1: set bit f of row s of dimension h's staging
+// block for every entry s * k_h + f of dimension h's list.  meta holds four
+// int64 arrays of dims + 1 entries: list offsets, feature offsets, staging
+// word offsets, output byte offsets.
+__device__ __forceinline__ uint32_t find_block(const int64_t *__restrict__ off, uint32_t dims,
+                                               int64_t v) {
+  // largest h with off[h] <= v (off nondecreasing, off[0] <= v < off[dims])
+  uint32_t lo = 0, hi = dims;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (off[mid] <= v) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void k_scatter_bits_ind(const int64_t *__restrict__ idx, const int64_t *__restrict__ meta,
+                                   uint32_t dims, uint64_t n, uint32_t *__restrict__ stage) {
+  const int64_t *lists = meta, *feats = meta + (dims + 1), *woff = meta + 2 * (dims + 1);
+  const uint64_t first = (uint64_t)lists[0], total = (uint64_t)lists[dims] - first;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const int64_t v = idx[i];
+    if (v < 0) continue;
+    const uint32_t h = find_block(lists, dims, (int64_t)(first + i));
+    const uint64_t k = (uint64_t)(feats[h + 1] - feats[h]);
+    if (k == 0) continue;
+    const uint64_t s = (uint64_t)v / k, f = (uint64_t)v % k;
+    if (s >= n) continue;
+    const uint64_t rw = (k + 31) / 32;
+    atomicOr(&stage[woff[h] + s * rw + (f >> 5)], 1u << (f & 31));
+  }
+}
+
+// 8 bits of a staged row starting at bit o; bits outside [0, 32 rw) read 0
+__device__ __forceinline__ uint32_t row_byte_at(const uint32_t *__restrict__ row, uint64_t rw,
+                                                int64_t o) {
+  if (o <= -8) return 0;
+  const uint32_t lead = o < 0 ? (uint32_t)(-o) : 0u;  // bits below 0 read 0
+  const uint64_t q = o < 0 ? 0 : (uint64_t)o;
+  const uint64_t w = q >> 5;
+  if (w >= rw) return 0;
+  uint64_t v = row[w];
+  if (w + 1 < rw) v |= (uint64_t)row[w + 1] << 32;
+  return ((uint32_t)(v >> (q & 31)) << lead) & 0xffu;
+}
+
+// step 2: byte b of row s of block h: bits 0..k_h-1 are the staged bits,
+// with flip bits k_h..2k_h-1 their complements, padding bits 0.
+__global__ void k_pack_bytes_ind(const uint32_t *__restrict__ stage, const int64_t *__restrict__ meta,
+                                 uint32_t dims, uint64_t n, int32_t flip, uint8_t *__restrict__ out) {
+  const int64_t *feats = meta + (dims + 1), *woff = meta + 2 * (dims + 1),
+                *boff = meta + 3 * (dims + 1);
+  const uint64_t total = (uint64_t)boff[dims];
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t h = find_block(boff, dims, (int64_t)t);
+    const uint64_t k = (uint64_t)(feats[h + 1] - feats[h]);
+    const uint64_t nb = ((flip ? 2 * k : k) + 7) / 8, rw = (k + 31) / 32;
+    const uint64_t local = t - (uint64_t)boff[h];
+    const uint64_t s = local / nb, b = local % nb;
+    const uint32_t *row = stage + woff[h] + s * rw;
+    const int64_t p0 = (int64_t)(8 * b);
+    uint32_t lo_mask = 0, fl_mask = 0;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      const int64_t p = p0 + j;
+      if (p < (int64_t)k) lo_mask |= 1u << j;
+      else if (flip && p < 2 * (int64_t)k) fl_mask |= 1u << j;
+    }
+    uint32_t v = row_byte_at(row, rw, p0) & lo_mask;
+    if (fl_mask) v |= ~row_byte_at(row, rw, p0 - (int64_t)k) & fl_mask;
+    out[t] = (uint8_t)v;
+  }
+}
+
 int grid_for(uint64_t work) {
   const uint64_t g = (work + 255) / 256;
   return (int)(g < 148ull * 16 ? (g ? g : 1) : 148ull * 16);
@@ -271,6 +351,63 @@ extern "C" int tm_bits_to_cvec(const int64_t *set_bits, uint64_t n_set, uint64_t
   if (n) k_words_to_bytes<<<grid_for(n * nb), 256>>>(rows, n, rw, nb, dout);
   CKU(cudaGetLastError());
   if (!on_device && n) CKU(cudaMemcpy(out, dout, n * nb, cudaMemcpyDeviceToHost));
+  else CKU(cudaDeviceSynchronize());
+  return TM_OK;
+}
+
+extern "C" int tm_bits_to_cvec_ind(const int64_t *set_bits, const int64_t *ind_offsets,
+                                   const int64_t *feat_offsets, uint32_t dims, uint64_t n,
+                                   int32_t flip, int32_t on_device, int32_t device, uint8_t *out,
+                                   uint64_t out_cap, int64_t *dim_offsets) {
+  if (!ind_offsets || !feat_offsets || !dim_offsets || dims == 0)
+    return tmb_fail(TM_ERR_ARG, "bits_to_cvec_ind: bad arguments");
+  if (ind_offsets[0] < 0 || feat_offsets[0] < 0)
+    return tmb_fail(TM_ERR_ARG, "bits_to_cvec_ind: offsets must be >= 0");
+  // host side: validate the offsets, lay out staging words and output blocks
+  std::vector<int64_t> meta(4 * ((size_t)dims + 1));
+  int64_t *lists = meta.data(), *feats = lists + dims + 1, *woff = feats + dims + 1,
+          *boff = woff + dims + 1;
+  uint64_t words = 0, bytes = 0;
+  for (uint32_t h = 0; h <= dims; h++) {
+    lists[h] = ind_offsets[h];
+    feats[h] = feat_offsets[h];
+    woff[h] = (int64_t)words;
+    boff[h] = (int64_t)bytes;
+    if (h == dims) break;
+    if (ind_offsets[h + 1] < ind_offsets[h] || feat_offsets[h + 1] < feat_offsets[h])
+      return tmb_fail(TM_ERR_ARG, "bits_to_cvec_ind: offsets must be nondecreasing");
+    const uint64_t k = (uint64_t)(feat_offsets[h + 1] - feat_offsets[h]);
+    words += n * ((k + 31) / 32);
+    bytes += n * (((flip ? 2 * k : k) + 7) / 8);
+  }
+  for (uint32_t h = 0; h <= dims; h++) dim_offsets[h] = boff[h];
+  if (!out) return TM_OK;  // sizing call: dim_offsets only
+  if (out_cap < bytes) return tmb_fail(TM_ERR_ARG, "bits_to_cvec_ind: output too small");
+  const uint64_t n_set = (uint64_t)(ind_offsets[dims] - ind_offsets[0]);
+  if (n_set && !set_bits) return tmb_fail(TM_ERR_ARG, "bits_to_cvec_ind: bad arguments");
+  CKU(cudaSetDevice(device));
+  DevScratch buf;
+  const size_t meta_b = meta.size() * 8, stage_b = ((words * 4 + 255) / 256) * 256;
+  const size_t idx_b = on_device ? 0 : n_set * 8, out_b = on_device ? 0 : bytes;
+  CKU(buf.ensure(meta_b + stage_b + idx_b + out_b + 512));
+  uint8_t *base = (uint8_t *)buf.p;
+  int64_t *dmeta = (int64_t *)base;
+  uint32_t *stage = (uint32_t *)(base + ((meta_b + 255) / 256) * 256);
+  uint8_t *tail = (uint8_t *)stage + stage_b;
+  const int64_t *di = set_bits;
+  uint8_t *dout = out;
+  if (!on_device) {
+    int64_t *st = (int64_t *)tail;
+    if (n_set) CKU(cudaMemcpy(st, set_bits, n_set * 8, cudaMemcpyHostToDevice));
+    di = st;
+    dout = tail + idx_b;
+  }
+  CKU(cudaMemcpy(dmeta, meta.data(), meta_b, cudaMemcpyHostToDevice));
+  if (words) CKU(cudaMemset(stage, 0, words * 4));
+  if (n_set) k_scatter_bits_ind<<<grid_for(n_set), 256>>>(di, dmeta, dims, n, stage);
+  if (bytes) k_pack_bytes_ind<<<grid_for(bytes), 256>>>(stage, dmeta, dims, n, flip, dout);
+  CKU(cudaGetLastError());
+  if (!on_device && bytes) CKU(cudaMemcpy(out, dout, bytes, cudaMemcpyDeviceToHost));
   else CKU(cudaDeviceSynchronize());
   return TM_OK;
 }

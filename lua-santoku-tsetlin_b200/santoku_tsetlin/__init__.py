@@ -36,6 +36,7 @@ align = 8
 
 CLASSIFIER = 0
 ENCODER = 1
+SAVE_STATE = 1  # tm_save flag: include the count planes
 
 
 class TsetlinError(RuntimeError):
@@ -123,10 +124,11 @@ _lib = None
 EXPORTS = (
     "tm_params_init", "tm_create", "tm_train", "tm_train_batch", "tm_train_batch_each",
     "tm_predict",
-    "tm_predict_scores", "tm_persist", "tm_persist_buf", "tm_free", "tm_load",
+    "tm_predict_scores", "tm_persist", "tm_persist_buf", "tm_save", "tm_save_buf", "tm_free",
+    "tm_load",
     "tm_checkpoint", "tm_restore", "tm_reconfigure", "tm_restrict", "tm_type",
     "tm_destroy", "tm_last_error", "tm_align", "tm_get_info", "tm_export_state",
-    "tm_import_state", "tm_class_accuracy", "tm_encoding_accuracy", "tm_bits_to_cvec",
+    "tm_import_state", "tm_class_accuracy", "tm_encoding_accuracy", "tm_bits_to_cvec", "tm_bits_to_cvec_ind",
     "tm_predict_noalloc", "tm_stats_enable", "tm_get_stats", "tm_reset_stats", "tm_serve_open", "tm_serve_submit", "tm_serve_poll",
     "tm_serve_latency_us", "tm_serve_close",
 )
@@ -152,6 +154,8 @@ def lib():
     L.tm_predict_scores.argtypes = [vp, vp, vp, u64, vp, i32]
     L.tm_persist.argtypes = [vp, ctypes.c_char_p]
     L.tm_persist_buf.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(u64)]
+    L.tm_save.argtypes = [vp, ctypes.c_char_p, u32]
+    L.tm_save_buf.argtypes = [vp, u32, ctypes.POINTER(vp), ctypes.POINTER(u64)]
     L.tm_free.argtypes = [vp]
     L.tm_load.argtypes = [vp, u64, i32, i32, ctypes.POINTER(vp)]
     L.tm_checkpoint.argtypes = [vp, vp, u64, ctypes.POINTER(u64)]
@@ -170,6 +174,7 @@ def lib():
     L.tm_class_accuracy.argtypes = [vp, vp, u64, u32, i32, i32, vp]
     L.tm_encoding_accuracy.argtypes = [vp, vp, u64, u32, i32, i32, vp]
     L.tm_bits_to_cvec.argtypes = [vp, u64, u64, u32, i32, i32, i32, vp]
+    L.tm_bits_to_cvec_ind.argtypes = [vp, vp, vp, u32, u64, i32, i32, i32, vp, u64, vp]
     L.tm_stats_enable.argtypes = [vp, i32]
     L.tm_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
     L.tm_reset_stats.argtypes = [vp]
@@ -375,6 +380,24 @@ class Machine:
         p = ctypes.c_void_p()
         n = ctypes.c_uint64()
         _check(lib().tm_persist_buf(self.handle, ctypes.byref(p), ctypes.byref(n)))
+        try:
+            return ctypes.string_at(p, n.value)
+        finally:
+            lib().tm_free(p)
+
+    def save(self, path=None, state=True):
+        """Versioned container (no counterpart in the reference): the
+        reference's persisted record plus `negative`, the default seed, the
+        reusable flag and, with `state`, the count planes, under a format
+        version and a checksum.  `load` reads it back; a machine saved with
+        its state can train again.  Writes `path`, or returns the bytes."""
+        flags = SAVE_STATE if state else 0
+        if path is not None:
+            _check(lib().tm_save(self.handle, os.fsencode(path), flags))
+            return None
+        p = ctypes.c_void_p()
+        n = ctypes.c_uint64()
+        _check(lib().tm_save_buf(self.handle, flags, ctypes.byref(p), ctypes.byref(n)))
         try:
             return ctypes.string_at(p, n.value)
         finally:
@@ -598,3 +621,36 @@ def bits_to_cvec(set_bits, n_samples, n_features, flip=False, device=0):
     _check(lib().tm_bits_to_cvec(b.ptr, b.nbytes // 8, int(n_samples), int(n_features),
                                  1 if flip else 0, 0, device, out.ctypes.data))
     return out
+
+
+def bits_to_cvec_ind(set_bits, ind_offsets, feat_offsets, n_samples, flip=False, device=0):
+    """santoku-matrix's bits_to_cvec_ind on the GPU: per-dimension set-bit
+    lists (dimension h: set_bits[ind_offsets[h]:ind_offsets[h+1]], entries
+    sample * k_h + feature) -> (bitmap, dim_offsets), the individualized
+    layout `train` / `predict` take with `dim_offsets` (capi.c:1344-1354).
+    dim_offsets has one entry per dimension plus the total size."""
+    io = np.ascontiguousarray(ind_offsets, dtype=np.int64)
+    fo = np.ascontiguousarray(feat_offsets, dtype=np.int64)
+    if io.ndim != 1 or fo.ndim != 1 or len(io) != len(fo) or len(io) < 2:
+        raise TsetlinError("ind_offsets and feat_offsets need dims + 1 entries each")
+    dims = len(fo) - 1
+    b = _Buf(set_bits, np.int64)
+    if b.nbytes // 8 < int(io[-1] - io[0]):
+        raise TsetlinError("set_bits is shorter than ind_offsets says")
+    doff = np.zeros(dims + 1, dtype=np.int64)
+    L = lib()
+    _check(L.tm_bits_to_cvec_ind(None, io.ctypes.data, fo.ctypes.data, dims, int(n_samples),
+                                 1 if flip else 0, 0, device, None, 0, doff.ctypes.data))
+    total = int(doff[-1])
+    if b.device:
+        import torch
+        out = torch.empty(max(total, 1), dtype=torch.uint8, device=torch.device("cuda", device))
+        _check(L.tm_bits_to_cvec_ind(b.ptr, io.ctypes.data, fo.ctypes.data, dims,
+                                     int(n_samples), 1 if flip else 0, 1, device,
+                                     out.data_ptr(), total, doff.ctypes.data))
+        return out[:total], doff
+    out = np.zeros(max(total, 1), dtype=np.uint8)
+    _check(L.tm_bits_to_cvec_ind(b.ptr, io.ctypes.data, fo.ctypes.data, dims, int(n_samples),
+                                 1 if flip else 0, 0, device, out.ctypes.data, total,
+                                 doff.ctypes.data))
+    return out[:total], doff

@@ -1,7 +1,7 @@
 """CPU restatements of the evaluator metrics and of the input packing.
 
 TEST INFRASTRUCTURE ONLY (the checker for tm_class_accuracy,
-tm_encoding_accuracy and tm_bits_to_cvec).  Counting uses numpy; the
+tm_encoding_accuracy, tm_bits_to_cvec and tm_bits_to_cvec_ind).  Counting uses numpy; the
 floating-point finish is a plain Python loop in the reference's order, so
 every operation rounds once, as in the reference's C without contraction.
 """
@@ -81,3 +81,28 @@ def bits_to_cvec(set_bits, n, features, flip):
     if flip:
         rows[:, features:] = ~rows[:, :features]
     return np.packbits(rows, axis=1, bitorder="little").ravel()
+
+
+def bits_to_cvec_ind(set_bits, ind_offsets, feat_offsets, n, flip):
+    """santoku-matrix's bits_to_cvec_ind: dimension h's list
+    set_bits[ind_offsets[h]:ind_offsets[h+1]] (entries sample * k_h +
+    feature, k_h = feat_offsets[h+1] - feat_offsets[h]) packed as n rows of
+    its own width, blocks concatenated in dimension order (doc/sth.md:42-54;
+    the reader is capi.c:1344-1354).  Returns (bitmap, dim_offsets) with
+    dims + 1 offsets, the last the total size."""
+    io = np.asarray(ind_offsets, dtype=np.int64)
+    fo = np.asarray(feat_offsets, dtype=np.int64)
+    idx = np.asarray(set_bits, dtype=np.int64)
+    blocks, offs, off = [], [], 0
+    for h in range(len(fo) - 1):
+        k = int(fo[h + 1] - fo[h])
+        offs.append(off)
+        if k == 0:
+            continue
+        lst = idx[io[h] - io[0]:io[h + 1] - io[0]]
+        b = bits_to_cvec(lst, n, k, flip)
+        blocks.append(b)
+        off += b.size
+    offs.append(off)
+    bm = np.concatenate(blocks) if blocks else np.zeros(0, np.uint8)
+    return bm, np.array(offs, dtype=np.int64)

@@ -47,3 +47,64 @@ def test_bits_to_cvec(tm, n, features, flip):
     if flip:
         from santoku_tsetlin import datagen
         assert np.array_equal(got, datagen.flip_pack(bits).ravel())
+
+
+def _ind_lists(rng, n, ks, density):
+    """Per-dimension set-bit lists, as bits_individualize hands them over."""
+    lists, bits = [], []
+    for k in ks:
+        b = rng.random((n, k)) < density
+        s, f = np.nonzero(b)
+        lst = (s * k + f).astype(np.int64)
+        if lst.size:
+            lst = np.concatenate([lst, lst[:3], [-1]])  # duplicates, a negative entry
+        rng.shuffle(lst)
+        lists.append(lst)
+        bits.append(b)
+    io = np.concatenate([[0], np.cumsum([len(x) for x in lists])]).astype(np.int64)
+    fo = np.concatenate([[0], np.cumsum(ks)]).astype(np.int64)
+    idx = np.concatenate(lists) if lists else np.zeros(0, np.int64)
+    return idx, io, fo, bits
+
+
+@pytest.mark.parametrize("n,ks,flip", [(5, [1, 7, 8, 9], True), (300, [40, 0, 33, 64, 100], True),
+                                       (64, [31, 32, 5], False), (1000, [300] * 20, True)])
+def test_bits_to_cvec_ind(tm, n, ks, flip):
+    rng = np.random.default_rng(n + len(ks))
+    idx, io, fo, bits = _ind_lists(rng, n, ks, 0.15)
+    got, doff = tm.bits_to_cvec_ind(idx, io, fo, n, flip)
+    want, woff = R.bits_to_cvec_ind(idx, io, fo, n, flip)
+    assert np.array_equal(doff, woff)
+    assert np.array_equal(got, want)
+    if flip:  # the golden fixtures' individualized layout: flip_pack per block
+        from santoku_tsetlin import datagen
+        blocks = [datagen.flip_pack(b).ravel() for b, k in zip(bits, ks) if k]
+        assert np.array_equal(got, np.concatenate(blocks))
+
+
+def test_bits_to_cvec_ind_device_and_train(tm):
+    """Device lists in, device bitmap out; the bitmap trains an individualized
+    classifier exactly as the same rows packed on the host do."""
+    import torch
+    rng = np.random.default_rng(77)
+    n, ks = 400, [60, 23, 90, 41]
+    idx, io, fo, bits = _ind_lists(rng, n, ks, 0.2)
+    got, doff = tm.bits_to_cvec_ind(torch.from_numpy(idx).cuda(), io, fo, n, True)
+    want, _ = R.bits_to_cvec_ind(idx, io, fo, n, True)
+    assert np.array_equal(got.cpu().numpy(), want)
+    y = rng.integers(0, len(ks), size=n).astype(np.int64)
+    outs = []
+    for x, yy in ((got, torch.from_numpy(y).cuda()), (want, y)):
+        t = tm.create("classifier", dict(classes=len(ks), clauses=16,
+                                         clause_tolerance=8, clause_maximum=16, target=8,
+                                         specificity=5, individualized=True, feat_offsets=fo,
+                                         reusable=True, seed=3))
+        t.train(dict(samples=n, problems=x, solutions=yy, iterations=2, dim_offsets=doff[:-1]))
+        outs.append(np.asarray(t.predict(want, doff[:-1], n)))
+        t.destroy()
+    assert np.array_equal(outs[0], outs[1])
+
+
+def test_bits_to_cvec_ind_rejects_short_list(tm):
+    with pytest.raises(tm.TsetlinError):
+        tm.bits_to_cvec_ind(np.zeros(3, np.int64), [0, 5], [0, 8], 4, True)

@@ -137,3 +137,28 @@ def test_oracle_vs_reference_random(oracle_lib, seed):
         assert np.array_equal(res[0][1], res[1][1])
         assert np.array_equal(res[0][2], res[1][2])
         assert res[0][3] == res[1][3]
+
+
+@pytest.mark.parametrize("case", ["cls_ind", "enc_ind"])
+def test_bits_to_cvec_ind_restatement_matches_fixture_layout(case):
+    """The restated bits_to_cvec_ind rebuilds the individualized inputs that
+    the reference-code fixtures were trained and predicted on: per-block
+    flip-interleaved rows at the recorded dim_offsets."""
+    import evaluator_ref as R
+    d = np.load(os.path.join(HERE, "golden", case + ".npz"))
+    fo = d["in_feat_offsets"]
+    for xk, ok, n in (("in_x", "in_dim_offsets", max(int(d["in_n"]), 1)),
+                      ("in_xt", "in_dim_offsets_t", int(d["in_nt"]))):
+        x, offs = d[xk], d[ok]
+        lists = []
+        for h in range(len(fo) - 1):
+            k = int(fo[h + 1] - fo[h])
+            nb = (2 * k + 7) // 8
+            blk = x[offs[h]:offs[h] + n * nb].reshape(n, nb)
+            bits = np.unpackbits(blk, axis=1, bitorder="little", count=k).astype(bool)
+            s, f = np.nonzero(bits)
+            lists.append((s * k + f).astype(np.int64))
+        io = np.concatenate([[0], np.cumsum([len(v) for v in lists])]).astype(np.int64)
+        got, doff = R.bits_to_cvec_ind(np.concatenate(lists), io, fo, n, True)
+        assert np.array_equal(doff[:-1], offs)
+        assert np.array_equal(got, x)
