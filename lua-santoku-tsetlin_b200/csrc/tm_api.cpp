@@ -503,7 +503,7 @@ static int run_epochs(std::vector<TrainJob> &jobs, uint32_t e0, uint32_t e1, tm_
   // machine table + work list
   std::vector<TrainDev> td(jobs.size());
   std::vector<WorkItem> work;
-  uint32_t Wpmax = 4, Bmax = 2, smax = 0;
+  uint32_t Wpmax = 4, Bmin = 32, Bmax = 2, smax = 0;
   for (size_t i = 0; i < jobs.size(); i++) {
     TrainJob &J = jobs[i];
     tm_machine *m = J.m;
@@ -542,6 +542,7 @@ static int run_epochs(std::vector<TrainJob> &jobs, uint32_t e0, uint32_t e1, tm_
         work.push_back(WorkItem{(uint32_t)i, h, k, (uint32_t)std::min(cost / 64.0, 4e9)});
     }
     Bmax = std::max(Bmax, m->B);
+    Bmin = std::min(Bmin, m->B);
   }
   if (work.empty()) return TM_OK;
   std::stable_sort(work.begin(), work.end(),
@@ -602,7 +603,7 @@ static int run_epochs(std::vector<TrainJob> &jobs, uint32_t e0, uint32_t e1, tm_
   if ((int)lay.total > optin)
     return fail(TM_ERR_ARG, "train: rows too wide for one CTA (%u bytes of shared memory)",
                 lay.total);
-  const int occ = train_occupancy(lay, mode, Bmax);
+  const int occ = train_occupancy(lay, mode, Bmin, Bmax);
   if (occ <= 0) return fail(TM_ERR_CUDA, "train: kernel cannot be resident (smem %u)", lay.total);
   const int grid = mode == TM_MODE_PAIR
                        ? 2 * (int)std::min<uint64_t>(work.size(), (uint64_t)occ)
@@ -623,7 +624,7 @@ static int run_epochs(std::vector<TrainJob> &jobs, uint32_t e0, uint32_t e1, tm_
   uint32_t *err = counter + 1;
   if (m0->timing) CK(cudaEventRecord(m0->ev0, st));
   CK(launch_train((const TrainDev *)base, (const WorkItem *)(base + off_w), (uint32_t)work.size(),
-                  counter, e0, e1, lay, mode, Bmax, grid, err, st));
+                  counter, e0, e1, lay, mode, Bmin, Bmax, grid, err, st));
   if (m0->timing) CK(cudaEventRecord(m0->ev1, st));
   note_launch(m0, 1);
   uint32_t herr = 0;

@@ -98,8 +98,9 @@ constexpr int TM_MODE_GLOBAL = 1;
 constexpr int TM_MODE_PAIR = 2;
 cudaError_t launch_train(const TrainDev *machines, const WorkItem *work, uint32_t nwork,
                          uint32_t *counter, uint32_t e_begin, uint32_t e_end, const TrainSmem &lay,
-                         int mode, uint32_t Bmax, int grid, uint32_t *err, cudaStream_t st);
-int train_occupancy(const TrainSmem &lay, int mode, uint32_t Bmax);
+                         int mode, uint32_t Bmin, uint32_t Bmax, int grid, uint32_t *err,
+                         cudaStream_t st);
+int train_occupancy(const TrainSmem &lay, int mode, uint32_t Bmin, uint32_t Bmax);
 // k_train_warp: one warp per unit for rows of at most 64 words and B <= 8
 constexpr int TM_MODE_WARP = 3;
 int train_warp_occupancy(uint32_t Wpmax, uint32_t Bmax, uint32_t smax, size_t *smem_bytes);

@@ -461,7 +461,9 @@ __device__ __forceinline__ void unit_sync() {
 
 // Single-CTA variants (256 threads) are capped at 128 registers, two CTAs
 // per SM; a pair CTA (512 threads, its shared memory fills the SM) too.
-template <bool SMEM_STATE, bool PAIR, int BM>
+// EXACT: every machine of the launch has exactly BM count planes, so the
+// plane loops have no run-time bound.
+template <bool SMEM_STATE, bool PAIR, int BM, bool EXACT = false>
 __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS, PAIR ? 1 : 2)
     k_train(const TrainDev *__restrict__ machines, const WorkItem *__restrict__ work,
             uint32_t nwork, uint32_t *__restrict__ counter, uint32_t e_begin, uint32_t e_end,
@@ -516,7 +518,7 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
     const WorkItem wi = work[u];
     const TrainDev &M = machines[wi.m];
     const ClassDev C = M.cls[wi.h];
-    const uint32_t m = M.B - 1;
+    const uint32_t m = EXACT ? (uint32_t)BM : M.B - 1;
     const uint32_t Wp = C.Wp, W = C.W;
     const uint32_t g = wi.h * M.clause_chunks + wi.k;
     // this CTA's clauses: rows rank*CPC .. rank*CPC+CPC-1 of the unit
@@ -740,12 +742,16 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
           // (clause, pair) items: item i -> the (i / P)-th fed-back clause,
           // words 2(i % P) and 2(i % P) + 1
           {
+            // fed-back clauses in ascending order, 4 bits each
+            uint32_t clist = 0, nfed = 0;
+            for (uint32_t cm = all; cm; cm &= cm - 1, nfed++)
+              clist |= (uint32_t)(__ffs(cm) - 1) << (4 * nfed);
             const uint32_t P2 = Wp >> 1;
-            const uint32_t total = __popc(all) * P2;
+            const uint32_t total = nfed * P2;
             const uint32_t NT = blockDim.x;
             uint32_t kk = tid / P2, qi = tid - kk * P2;
             for (uint32_t it = tid; it < total; it += NT) {
-              const uint32_t c = __fns(all, 0, kk + 1);
+              const uint32_t c = (clist >> (4 * kk)) & 15u;
               const uint32_t w0 = 2 * qi;
               uint32_t *act_c = act + c * Wp, *cnt_c = cnt + (size_t)c * m * Wp;
               uint32_t pq[2][BM], aq[2];
@@ -1109,12 +1115,13 @@ cudaError_t launch_train_warp(const TrainDev *machines, const WorkItem *work, ui
   return cudaGetLastError();
 }
 
-template <bool S, bool P, int BM>
+template <bool S, bool P, int BM, bool EX = false>
 static int occ_of(const TrainSmem &lay) {
-  cudaFuncSetAttribute(k_train<S, P, BM>, cudaFuncAttributeMaxDynamicSharedMemorySize, lay.total);
+  cudaFuncSetAttribute(k_train<S, P, BM, EX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       lay.total);
   if (!P) {
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_train<S, P, BM>, TM_TRAIN_THREADS,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_train<S, P, BM, EX>, TM_TRAIN_THREADS,
                                                   lay.total);
     return nb;
   }
@@ -1135,17 +1142,21 @@ static int occ_of(const TrainSmem &lay) {
 }
 
 // Single: co-resident CTAs per SM.  Pair: co-resident clusters per device.
-int train_occupancy(const TrainSmem &lay, int mode, uint32_t Bmax) {
-  const bool small = Bmax <= 8;
+int train_occupancy(const TrainSmem &lay, int mode, uint32_t Bmin, uint32_t Bmax) {
+  const bool small = Bmax <= 8, exact = Bmin == 8 && Bmax == 8;
   if (mode == TM_MODE_PAIR) return occ_of<true, true, 7>(lay);
-  if (mode == TM_MODE_SMEM) return small ? occ_of<true, false, 7>(lay) : occ_of<true, false, 31>(lay);
-  return small ? occ_of<false, false, 7>(lay) : occ_of<false, false, 31>(lay);
+  if (mode == TM_MODE_SMEM)
+    return exact ? occ_of<true, false, 7, true>(lay)
+                 : (small ? occ_of<true, false, 7>(lay) : occ_of<true, false, 31>(lay));
+  return exact ? occ_of<false, false, 7, true>(lay)
+               : (small ? occ_of<false, false, 7>(lay) : occ_of<false, false, 31>(lay));
 }
 
 cudaError_t launch_train(const TrainDev *machines, const WorkItem *work, uint32_t nwork,
                          uint32_t *counter, uint32_t e_begin, uint32_t e_end, const TrainSmem &lay,
-                         int mode, uint32_t Bmax, int grid, uint32_t *err, cudaStream_t st) {
-  const bool small = Bmax <= 8;
+                         int mode, uint32_t Bmin, uint32_t Bmax, int grid, uint32_t *err,
+                         cudaStream_t st) {
+  const bool small = Bmax <= 8, exact = Bmin == 8 && Bmax == 8;
   if (mode == TM_MODE_PAIR) {
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute at[1];
@@ -1162,15 +1173,18 @@ cudaError_t launch_train(const TrainDev *machines, const WorkItem *work, uint32_
     return cudaLaunchKernelEx(&cfg, k_train<true, true, 7>, machines, work, nwork, counter,
                               e_begin, e_end, lay, err);
   }
-#define TM_LAUNCH(S, BM)                                                                     \
-  k_train<S, false, BM><<<grid, TM_TRAIN_THREADS, lay.total, st>>>(machines, work, nwork, counter, \
-                                                                   e_begin, e_end, lay, err)
+#define TM_LAUNCH(S, BM, EX)                                                                  \
+  k_train<S, false, BM, EX><<<grid, TM_TRAIN_THREADS, lay.total, st>>>(machines, work, nwork,     \
+                                                                       counter, e_begin, e_end, \
+                                                                       lay, err)
   if (mode == TM_MODE_SMEM) {
-    if (small) TM_LAUNCH(true, 7);
-    else TM_LAUNCH(true, 31);
+    if (exact) TM_LAUNCH(true, 7, true);
+    else if (small) TM_LAUNCH(true, 7, false);
+    else TM_LAUNCH(true, 31, false);
   } else {
-    if (small) TM_LAUNCH(false, 7);
-    else TM_LAUNCH(false, 31);
+    if (exact) TM_LAUNCH(false, 7, true);
+    else if (small) TM_LAUNCH(false, 7, false);
+    else TM_LAUNCH(false, 31, false);
   }
 #undef TM_LAUNCH
   return cudaGetLastError();
