@@ -554,7 +554,7 @@ static int run_epochs(std::vector<TrainJob> &jobs, uint32_t e0, uint32_t e1, tm_
   if (Wpmax <= 64 && Bmax <= 8 && !m0->no_warp) {
     // short rows: one warp per unit
     size_t wsm = 0;
-    const int occ = train_warp_occupancy(Wpmax, Bmax, smax, &wsm);
+    const int occ = train_warp_occupancy(Wpmax, Bmin, Bmax, smax, &wsm);
     if (occ > 0 && (int)wsm <= optin) {
       const int grid = (int)std::min<uint64_t>((work.size() + 3) / 4, (uint64_t)num_sms(dev) * occ);
       m0->last_mode = TM_MODE_WARP;
@@ -571,7 +571,8 @@ static int run_epochs(std::vector<TrainJob> &jobs, uint32_t e0, uint32_t e1, tm_
       uint32_t *counter = (uint32_t *)(base + off_c);
       if (m0->timing) CK(cudaEventRecord(m0->ev0, st));
       CK(launch_train_warp((const TrainDev *)base, (const WorkItem *)(base + off_w),
-                           (uint32_t)work.size(), counter, e0, e1, Wpmax, Bmax, smax, grid, st));
+                           (uint32_t)work.size(), counter, e0, e1, Wpmax, Bmin, Bmax, smax,
+                           grid, st));
       if (m0->timing) CK(cudaEventRecord(m0->ev1, st));
       note_launch(m0, 1);
       CK(cudaStreamSynchronize(st));

@@ -103,10 +103,12 @@ cudaError_t launch_train(const TrainDev *machines, const WorkItem *work, uint32_
 int train_occupancy(const TrainSmem &lay, int mode, uint32_t Bmin, uint32_t Bmax);
 // k_train_warp: one warp per unit for rows of at most 64 words and B <= 8
 constexpr int TM_MODE_WARP = 3;
-int train_warp_occupancy(uint32_t Wpmax, uint32_t Bmax, uint32_t smax, size_t *smem_bytes);
+int train_warp_occupancy(uint32_t Wpmax, uint32_t Bmin, uint32_t Bmax, uint32_t smax,
+                         size_t *smem_bytes);
 cudaError_t launch_train_warp(const TrainDev *machines, const WorkItem *work, uint32_t nwork,
                               uint32_t *counter, uint32_t e_begin, uint32_t e_end, uint32_t Wpmax,
-                              uint32_t Bmax, uint32_t smax, int grid, cudaStream_t st);
+                              uint32_t Bmin, uint32_t Bmax, uint32_t smax, int grid,
+                              cudaStream_t st);
 cudaError_t launch_lits(const uint32_t *act, const ClassDev *cls, uint32_t classes,
                         uint32_t clauses, int32_t *lits, cudaStream_t st);
 cudaError_t launch_predict(const uint32_t *act, const int32_t *lits, const ClassDev *cls,

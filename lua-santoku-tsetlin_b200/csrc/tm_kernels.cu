@@ -412,6 +412,31 @@ __device__ __forceinline__ void rg_inc(uint32_t (&p)[BM], uint32_t &a, uint32_t 
   a = na;
 }
 
+// rg_add with no increments (Type Ia when L > clause_maximum): plain borrow
+// ripple, saturating at zero.
+template <int BM>
+__device__ __forceinline__ void rg_dec(uint32_t (&p)[BM], uint32_t &a, uint32_t m, uint32_t D,
+                                       uint32_t am) {
+  uint32_t bw = D;
+#pragma unroll
+  for (int b = 0; b < BM; b++)
+    if (b < (int)m) {
+      const uint32_t q = p[b];
+      p[b] = q ^ bw;
+      bw &= ~q;
+    }
+  const uint32_t ba = bw & am;
+  uint32_t na = a ^ ba;
+  bw = ~a & ba;
+  if (bw) {
+#pragma unroll
+    for (int b = 0; b < BM; b++)
+      if (b < (int)m) p[b] &= ~bw;
+    na &= ~bw;
+  }
+  a = na;
+}
+
 // Mask of word w0 + k given the last-word mask `last` and W words.
 __device__ __forceinline__ uint32_t word_mask(uint32_t w, uint32_t W, uint32_t last) {
   return w + 1 < W ? 0xFFFFFFFFu : (w + 1 == W ? last : 0u);
@@ -788,8 +813,10 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
                     // Type Ia (capi.c:177-180): inc where x=1 (if L <= maximum),
                     // dec where x=0 and not included.  Type II (capi.c:192-196):
                     // inc where x=0 and not included.
-                    if (t1)
-                      rg_add<BM>(pq[k], aq[k], m, incx ? (x & vm) : 0u, nx, am);
+                    if (t1 && incx)
+                      rg_add<BM>(pq[k], aq[k], m, x & vm, nx, am);
+                    else if (t1)
+                      rg_dec<BM>(pq[k], aq[k], m, nx, am);
                     else
                       rg_inc<BM>(pq[k], aq[k], m, nx, am);
                   }
@@ -866,7 +893,7 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
 // ---------------------------------------------------------------------------
 constexpr int TM_WARP_THREADS = 128;
 
-template <int BM>
+template <int BM, bool EXACT = false>
 __global__ void __launch_bounds__(TM_WARP_THREADS)
     k_train_warp(const TrainDev *__restrict__ machines, const WorkItem *__restrict__ work,
                  uint32_t nwork, uint32_t *__restrict__ counter, uint32_t e_begin, uint32_t e_end,
@@ -888,7 +915,7 @@ __global__ void __launch_bounds__(TM_WARP_THREADS)
     const WorkItem wi = work[u];
     const TrainDev &M = machines[wi.m];
     const ClassDev C = M.cls[wi.h];
-    const uint32_t m = M.B - 1;
+    const uint32_t m = EXACT ? (uint32_t)BM : M.B - 1;
     const uint32_t Wp = C.Wp, W = C.W;
     const uint32_t g = wi.h * M.clause_chunks + wi.k;
     uint32_t *gact = M.act + C.act_off + (uint64_t)wi.k * 8 * Wp;
@@ -1015,8 +1042,10 @@ __global__ void __launch_bounds__(TM_WARP_THREADS)
               uint32_t pp[BM], aq;
               ld_word<BM>(act_c, cnt_c, Wp, m, w, pp, aq);
               const uint32_t nx = ~x & ~rg_included<BM>(pp, aq, m, M.ib) & vm;
-              if (t1)
-                rg_add<BM>(pp, aq, m, incx ? (x & vm) : 0u, nx, am);
+              if (t1 && incx)
+                rg_add<BM>(pp, aq, m, x & vm, nx, am);
+              else if (t1)
+                rg_dec<BM>(pp, aq, m, nx, am);
               else
                 rg_inc<BM>(pp, aq, m, nx, am);
               st_word<BM>(act_c, cnt_c, Wp, m, w, pp, aq);
@@ -1093,25 +1122,36 @@ static uint32_t warp_slice_words(uint32_t Wpmax, uint32_t Bmax, uint32_t ib_word
   return (8 * Bmax * Wpmax + 2 * ib_words + ovf_cap + 32 + 31) / 32 * 32;
 }
 
-int train_warp_occupancy(uint32_t Wpmax, uint32_t Bmax, uint32_t smax, size_t *smem_bytes) {
+int train_warp_occupancy(uint32_t Wpmax, uint32_t Bmin, uint32_t Bmax, uint32_t smax,
+                         size_t *smem_bytes) {
   const uint32_t ovf_cap = smax / 4 > 0 ? smax / 4 : 1;
   const size_t bytes = (size_t)(TM_WARP_THREADS / 32) * warp_slice_words(Wpmax, Bmax, Wpmax, ovf_cap) * 4;
   *smem_bytes = bytes;
-  cudaFuncSetAttribute(k_train_warp<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  const bool exact = Bmin == 8 && Bmax == 8;
+  cudaFuncSetAttribute(k_train_warp<7, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaFuncSetAttribute(k_train_warp<7, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   int nb = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_train_warp<7>, TM_WARP_THREADS, bytes);
+  if (exact)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_train_warp<7, true>, TM_WARP_THREADS, bytes);
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_train_warp<7, false>, TM_WARP_THREADS, bytes);
   return nb;
 }
 
 cudaError_t launch_train_warp(const TrainDev *machines, const WorkItem *work, uint32_t nwork,
                               uint32_t *counter, uint32_t e_begin, uint32_t e_end, uint32_t Wpmax,
-                              uint32_t Bmax, uint32_t smax, int grid, cudaStream_t st) {
+                              uint32_t Bmin, uint32_t Bmax, uint32_t smax, int grid,
+                              cudaStream_t st) {
   const uint32_t ovf_cap = smax / 4 > 0 ? smax / 4 : 1;
   const uint32_t slice = 8 * Bmax * Wpmax;
   const uint32_t stride = warp_slice_words(Wpmax, Bmax, Wpmax, ovf_cap);
   const size_t bytes = (size_t)(TM_WARP_THREADS / 32) * stride * 4;
-  k_train_warp<7><<<grid, TM_WARP_THREADS, bytes, st>>>(machines, work, nwork, counter, e_begin,
-                                                        e_end, slice, Wpmax, ovf_cap, stride);
+  if (Bmin == 8 && Bmax == 8)
+    k_train_warp<7, true><<<grid, TM_WARP_THREADS, bytes, st>>>(
+        machines, work, nwork, counter, e_begin, e_end, slice, Wpmax, ovf_cap, stride);
+  else
+    k_train_warp<7, false><<<grid, TM_WARP_THREADS, bytes, st>>>(
+        machines, work, nwork, counter, e_begin, e_end, slice, Wpmax, ovf_cap, stride);
   return cudaGetLastError();
 }
 
