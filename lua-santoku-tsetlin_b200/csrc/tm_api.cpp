@@ -422,17 +422,19 @@ static TrainSmem plan_smem(uint32_t Wpmax, uint32_t Bmax, uint32_t smax, int mod
     return at;
   };
   const uint32_t cpc = mode == TM_MODE_PAIR ? 4 : 8;  // clauses held by one CTA
-  L.state_words = mode == TM_MODE_GLOBAL ? 0 : cpc * Bmax * Wpmax;
+  // GLOBAL: the action plane only (count planes stay in global memory)
+  L.state_words = mode == TM_MODE_GLOBAL ? cpc * Wpmax : cpc * Bmax * Wpmax;
   L.state_off = take(L.state_words * 4);
   L.ring_words = Wpmax;
   L.ring_off = take(TM_RING * Wpmax * 4);
   L.bar_off = take(TM_RING * 8);
-  L.list_off = take(2 * TM_BATCH * 4 * 9);  // one entry per thread (pair CTAs: 512)
+  L.list_off = take((mode == TM_MODE_PAIR ? 2 : 1) * TM_BATCH * 4 * 9);  // one entry per thread
   L.votes_off = take(128 * 4);
   L.ib_words = Wpmax;
-  L.ib_off = take(2 * cpc * Wpmax * 4);
+  // Type Ib levels and overflow lists: one slot per clause pair
+  L.ib_off = take(2 * (cpc / 2) * Wpmax * 4);
   L.ovf_cap = std::max<uint32_t>(1, smax / 4);
-  L.ovf_off = take(cpc * L.ovf_cap * 4);
+  L.ovf_off = take((cpc / 2) * L.ovf_cap * 4);
   L.misc_off = take(32 * 4);
   L.total = o;
   return L;

@@ -60,13 +60,13 @@ struct WorkItem {
 
 // Shared-memory plan of one training launch (byte offsets).
 struct TrainSmem {
-  uint32_t state_off, state_words;  // per-unit state copy (state_words == 0: global)
+  uint32_t state_off, state_words;  // per-unit state copy (global-planes variant: actions only)
   uint32_t ring_off, ring_words;    // sample ring: TM_RING slots of ring_words
   uint32_t bar_off;                 // TM_RING mbarriers
   uint32_t list_off;                // active-sample list
   uint32_t votes_off;               // 2 x 8 x 2 clause partial sums
-  uint32_t ib_off, ib_words;        // per CTA clause: 2 levels x ib_words
-  uint32_t ovf_off, ovf_cap;        // per CTA clause: overflow entries
+  uint32_t ib_off, ib_words;        // per clause pair of the CTA: 2 levels x ib_words
+  uint32_t ovf_off, ovf_cap;        // per clause pair of the CTA: overflow entries
   uint32_t misc_off;
   uint32_t total;
 };

@@ -522,7 +522,9 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
     mbar_fence_init();
     misc[20] = 0;
   }
-  for (uint32_t i = tid; i < 2 * CPC * lay.ib_words; i += blockDim.x)
+  // Type Ib level counters: one slot per clause pair (each pair has exactly
+  // one Type I clause per sample), slot = local clause >> 1
+  for (uint32_t i = tid; i < CPC * lay.ib_words; i += blockDim.x)
     ((uint32_t *)(smem + lay.ib_off))[i] = 0;
   if (tid < 8) misc[24 + tid] = 0;
   unit_sync<PAIR>();
@@ -560,8 +562,13 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
         ((uint4 *)cnt)[i] = ((const uint4 *)gcnt)[i];
       __syncthreads();
     } else {
-      act = gact;
+      // count planes stay in global memory (L2-resident working set); the
+      // action plane, read by every evaluation, is held in shared memory
+      act = (uint32_t *)(smem + lay.state_off);
       cnt = gcnt;
+      const uint32_t na4 = CPC * Wp / 4;
+      for (uint32_t i = tid; i < na4; i += blockDim.x) ((uint4 *)act)[i] = ((const uint4 *)gact)[i];
+      __syncthreads();
     }
     uint32_t *act_j = act + lc * Wp;
     uint32_t *cnt_j = cnt + (size_t)lc * m * Wp;
@@ -742,8 +749,8 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
             const uint32_t nq = (npk + 3) >> 2;
             for (uint32_t cm = ibm; cm; cm &= cm - 1) {
               const uint32_t c = __ffs(cm) - 1, jj = rank * CPC + c;
-              uint32_t *l0 = ibase + (size_t)c * 2 * lay.ib_words, *l1 = l0 + lay.ib_words;
-              uint32_t *ov = (uint32_t *)(smem + lay.ovf_off) + (size_t)c * lay.ovf_cap;
+              uint32_t *l0 = ibase + (size_t)(c >> 1) * 2 * lay.ib_words, *l1 = l0 + lay.ib_words;
+              uint32_t *ov = (uint32_t *)(smem + lay.ovf_off) + (size_t)(c >> 1) * lay.ovf_cap;
               for (uint32_t q = tid; q < nq; q += blockDim.x) {
                 uint32_t o[4];
                 philox(sp, ee, g, ST_IB | (jj << 20) | q, M.seed, o);
@@ -754,7 +761,7 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
                     const uint32_t w = bit >> 5, mk = 1u << (bit & 31);
                     if (atomicXor(&l0[w], mk) & mk) {
                       if (atomicXor(&l1[w], mk) & mk) {
-                        const uint32_t at = atomicAdd(&misc[24 + c], 1u);
+                        const uint32_t at = atomicAdd(&misc[24 + (c >> 1)], 1u);
                         if (at < lay.ovf_cap) ov[at] = bit;
                       }
                     }
@@ -781,7 +788,7 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
               uint32_t *act_c = act + c * Wp, *cnt_c = cnt + (size_t)c * m * Wp;
               uint32_t pq[2][BM], aq[2];
               if ((ibm >> c) & 1u) {
-                uint32_t *l0 = ibase + (size_t)c * 2 * lay.ib_words;
+                uint32_t *l0 = ibase + (size_t)(c >> 1) * 2 * lay.ib_words;
                 const uint2 m0 = *(const uint2 *)(l0 + w0);
                 const uint2 m1 = *(const uint2 *)(l0 + lay.ib_words + w0);
                 if ((m0.x | m0.y | m1.x | m1.y) != 0) {
@@ -833,15 +840,15 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
           if (all & (1u << lc)) dirty = true;
           if (ibm) {
             uint32_t novf = 0;
-            for (uint32_t cm = ibm; cm; cm &= cm - 1) novf += misc[24 + __ffs(cm) - 1];
+            for (uint32_t cm = ibm; cm; cm &= cm - 1) novf += misc[24 + ((__ffs(cm) - 1) >> 1)];
             if (novf) {
               // bits picked 4 or more times: rare, applied by one thread
               __syncthreads();
               if (tid == 0) {
                 for (uint32_t cm = ibm; cm; cm &= cm - 1) {
                   const uint32_t c = __ffs(cm) - 1;
-                  const uint32_t *ov = (uint32_t *)(smem + lay.ovf_off) + (size_t)c * lay.ovf_cap;
-                  const uint32_t no = misc[24 + c];
+                  const uint32_t *ov = (uint32_t *)(smem + lay.ovf_off) + (size_t)(c >> 1) * lay.ovf_cap;
+                  const uint32_t no = misc[24 + (c >> 1)];
                   for (uint32_t t = 0; t < no && t < lay.ovf_cap; t++) {
                     const uint32_t bit = ov[t], w = bit >> 5;
                     const uint32_t am = w + 1 == W ? C.amask : 0xFFFFFFFFu;
@@ -850,7 +857,7 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
                     rg_sub_pow2<BM>(pp, aq, m, 2, 1u << (bit & 31), am);
                     st_word<BM>(act + c * Wp, cnt + (size_t)c * m * Wp, Wp, m, w, pp, aq);
                   }
-                  misc[24 + c] = 0;
+                  misc[24 + (c >> 1)] = 0;
                 }
               }
             }
@@ -863,11 +870,14 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
       }
     }
     if (aborted) break;
-    if (SMEM_STATE) {
-      __syncthreads();
-      const uint32_t na4 = CPC * Wp / 4, nc4 = CPC * m * Wp / 4;
+    __syncthreads();
+    {
+      const uint32_t na4 = CPC * Wp / 4;
       for (uint32_t i = tid; i < na4; i += blockDim.x)
         ((uint4 *)gact)[i] = ((const uint4 *)act)[i];
+    }
+    if (SMEM_STATE) {
+      const uint32_t nc4 = CPC * m * Wp / 4;
       for (uint32_t i = tid; i < nc4; i += blockDim.x)
         ((uint4 *)gcnt)[i] = ((const uint4 *)cnt)[i];
     }
