@@ -296,7 +296,8 @@ def test_train_batch_equals_individual(tm):
     (16384, 8, False, 1),   # same rows with the automata in global memory (default)
     (300, 12, False, 0),    # more than 8 state bits, shared-memory automata
     (12000, 10, False, 1),  # more than 8 state bits on wide rows: global memory
-], ids=["warp", "pair", "global", "smem_b12", "global_b10"])
+    (8192, 8, False, 1),    # planes fit shared memory at one CTA per SM; global planes at two win
+], ids=["warp", "pair", "global", "smem_b12", "global_b10", "global_by_occupancy"])
 def test_train_variants_match_oracle(tm, monkeypatch, features, state, pair, mode):
     from santoku_tsetlin import datagen
     if pair:
