@@ -348,11 +348,11 @@ def run_ours(args, w):
     alg = train_algorithmic_bytes(w, occ_units)
     # DRAM bytes of one k_train launch from an ncu capture of the same kernel
     # on the large sparse classifier's rows with 280 units and 40,000 samples
-    # (profiles/k_train_c1_small_ncu.md: 2.867 GB read + 22.143 GB written),
+    # (profiles/k_train_c1_small_ncu.md: 1.856 GB read + 8.695 GB written),
     # scaled by units x samples to this launch.
     traffic = None
     if w["name"] == "large-sparse-classifier":
-        per_unit_sample = (2.866907e9 + 22.143480e9) / (280 * 40000)
+        per_unit_sample = (1.855563e9 + 8.695468e9) / (280 * 40000)
         traffic = per_unit_sample * (w["classes"] * w["clauses"] // 8) * w["n_train"]
     avg_ms = st["train_kernel_ms"] / max(1, st["train_launches"])
     achieved = alg / (avg_ms / 1e3) / 1e9
