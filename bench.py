@@ -382,6 +382,16 @@ def run_ours(args, w):
                                            (st["predict_kernel_ms"] / max(1, st["predict_launches"]) / 1e3 + 1e-12),
         },
     }
+    if rank == 0:
+        # integer-pipe roofline of clause evaluation (after the timed region):
+        # k_predict's inner loop issues 11 ALU-pipe instructions (4 AND-NOT,
+        # 6 carry-save LOP3, 1 add) and 1 POPC per 4 words
+        pk = tm.int_peaks(dev.index if dev.index is not None else 0)
+        wops = out["kernels"]["predict_literal_evals_per_s"] / 32
+        bound = min(4 * pk["lop3"] / 11, 4 * pk["popc"])
+        out["kernels"].update({"int_peaks_ops_per_s": pk, "predict_word_ops_per_s": wops,
+                               "predict_int_bound_word_ops_per_s": bound,
+                               "predict_frac_of_int_bound": wops / bound})
     if ck:
         out["clocks"] = ck
     if rank == 0 and ws == 1 and not args.no_cpu:

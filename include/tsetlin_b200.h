@@ -232,6 +232,13 @@ int tm_bits_to_cvec_ind(const int64_t *set_bits, const int64_t *ind_offsets,
                         int32_t on_device, int32_t device, uint8_t *out, uint64_t out_cap,
                         int64_t *dim_offsets);
 
+/* Integer-pipe peaks of `device`, measured by microbenchmark kernels (16
+ * independent inline-PTX chains per thread, 8 CTAs of 256 threads per SM,
+ * timed with CUDA events): out[0] lop3.b32, out[1] popc.b32, out[2]
+ * add.u32, in thread-operations per second.  The roofline denominators of
+ * the bit-logic kernels.  No counterpart in the reference. */
+int tm_int_peaks(int32_t device, double *out);
+
 /* Predict without allocating.  No counterpart in the reference.  For
  * callers that must not call cudaMalloc / cudaFree while they run -- a
  * serving loop that cannot absorb the device-wide synchronisation those
@@ -259,9 +266,20 @@ typedef struct tm_stats {
   uint64_t kernel_launches;   /* every kernel the library launched */
   uint64_t train_unit_steps;  /* (unit, sample) steps examined by train kernels */
   int32_t train_mode;         /* last train kernel variant: 0 automata in shared memory,
-                                 1 in global memory, 2 split over a 2-CTA cluster,
-                                 3 one warp per unit (rows of at most 64 words) */
+                                 1 count planes in global memory, 2 split over a 2-CTA
+                                 cluster, 3 one warp per unit (rows of at most 64 words) */
+  int32_t train_autotuned;    /* 1 if the autotuner chose that variant */
 } tm_stats;
+/* Train-kernel variant choice.  All variants end in the same automaton
+ * state; they differ in speed.  mode 0: heuristic (resident CTAs per SM);
+ * 1 (default, or TSETLIN_B200_AUTOTUNE at create): the first train call of
+ * a launch shape times every feasible variant on a short trial (up to 1,024
+ * samples of epoch 0 on up to eight units per SM, on the freshly reset
+ * automata, which are reset again afterwards) and caches the fastest for
+ * the process; 2: tune on every train call.  No counterpart in the
+ * reference (it has one CPU code path). */
+int tm_set_autotune(tm_machine *m, int32_t mode);
+
 /* on != 0 starts timing (events around every train / predict kernel). */
 int tm_stats_enable(tm_machine *m, int32_t on);
 int tm_get_stats(const tm_machine *m, tm_stats *out);

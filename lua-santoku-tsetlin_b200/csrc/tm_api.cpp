@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -106,6 +107,8 @@ struct tm_machine {
   bool pair = false;      // TSETLIN_B200_PAIR=1: split units too large for one SM over a
                           // 2-CTA cluster instead of keeping their automata in global memory
   bool no_warp = false;   // TSETLIN_B200_NO_WARP=1: never train a unit with one warp
+  int autotune = 1;       // 0 heuristic variant choice, 1 tuned (cached per shape),
+                          // 2 tuned afresh on every train call; TSETLIN_B200_AUTOTUNE
   int last_mode = -1;     // k_train variant of the last launch
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   tm_stats stats{};
@@ -255,6 +258,8 @@ extern "C" int tm_create(const tm_params *p, tm_machine **out) {
     m->pair = e && e[0] == '1';
     const char *w = getenv("TSETLIN_B200_NO_WARP");
     m->no_warp = w && w[0] == '1';
+    const char *t = getenv("TSETLIN_B200_AUTOTUNE");
+    m->autotune = t && t[0] >= '0' && t[0] <= '2' ? t[0] - '0' : 1;
   }
   if (m->individualized) {
     // capi.c:528-606 leaves features, input_bits, input_chunks and tail_mask
@@ -314,6 +319,13 @@ extern "C" void tm_destroy(tm_machine *m) {
   if (m->ev1) cudaEventDestroy(m->ev1);
   if (m->st) cudaStreamDestroy(m->st);
   delete m;
+}
+
+extern "C" int tm_set_autotune(tm_machine *m, int32_t mode) {
+  if (!m) return fail(TM_ERR_ARG, "null machine");
+  if (mode < 0 || mode > 2) return fail(TM_ERR_ARG, "autotune: mode must be 0, 1 or 2");
+  m->autotune = mode;
+  return TM_OK;
 }
 
 extern "C" int tm_stats_enable(tm_machine *m, int32_t on) {
@@ -467,6 +479,198 @@ static int validate_train(tm_machine *m, const tm_train_args *a) {
   return TM_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Train kernel variants.  All end in the same automaton state (every draw is
+// keyed, §draw contract), so the choice is a matter of speed only: a
+// heuristic by resident CTAs per SM, or an autotuner that times the
+// feasible variants on a short trial of the actual launch and caches the
+// fastest per launch shape for the life of the process.
+// ---------------------------------------------------------------------------
+struct TrainShape {
+  uint32_t Wpmax, Bmin, Bmax, smax, units;
+  int optin, sms;
+};
+
+struct TrainPlan {
+  int mode = TM_MODE_GLOBAL;
+  TrainSmem lay{};
+  int grid = 0;
+};
+
+// Fills `p` for `mode` when that variant can run this launch.
+static bool plan_mode(int mode, const TrainShape &sh, TrainPlan &p) {
+  p = TrainPlan{};
+  p.mode = mode;
+  if (mode == TM_MODE_WARP) {
+    if (sh.Wpmax > 64 || sh.Bmax > 8) return false;
+    size_t wsm = 0;
+    const int occ = train_warp_occupancy(sh.Wpmax, sh.Bmin, sh.Bmax, sh.smax, &wsm);
+    if (occ <= 0 || (int)wsm > sh.optin) return false;
+    p.grid = (int)std::min<uint64_t>((sh.units + 3) / 4, (uint64_t)sh.sms * occ);
+    return true;
+  }
+  if (mode == TM_MODE_PAIR && sh.Bmax > 8) return false;
+  p.lay = plan_smem(sh.Wpmax, sh.Bmax, sh.smax, mode);
+  if ((int)p.lay.total > sh.optin) return false;
+  const int occ = train_occupancy(p.lay, mode, sh.Bmin, sh.Bmax);
+  if (occ <= 0) return false;
+  p.grid = mode == TM_MODE_PAIR ? 2 * (int)std::min<uint64_t>(sh.units, (uint64_t)occ)
+                                : (int)std::min<uint64_t>(sh.units, (uint64_t)sh.sms * occ);
+  return true;
+}
+
+static int heuristic_plan(const TrainShape &sh, const tm_machine *m0, TrainPlan &out) {
+  // short rows: one warp per unit
+  if (!m0->no_warp && plan_mode(TM_MODE_WARP, sh, out)) return TM_OK;
+  // all planes in shared memory when a unit fits one SM, unless global
+  // planes give more resident CTAs (measured on B200: 8,192-feature rows
+  // train 26 % faster with global planes at two CTAs per SM than with shared
+  // planes at one); a 2-CTA cluster only on request (its per-sample cluster
+  // barrier costs more than the L2 round trips it saves)
+  TrainPlan s, g, c;
+  const bool hs = plan_mode(TM_MODE_SMEM, sh, s);
+  const bool hg = plan_mode(TM_MODE_GLOBAL, sh, g);
+  if (!hs && m0->pair && plan_mode(TM_MODE_PAIR, sh, c)) {
+    out = c;
+    return TM_OK;
+  }
+  if (hs && (!hg || s.grid >= g.grid)) {
+    out = s;
+    return TM_OK;
+  }
+  if (hg) {
+    out = g;
+    return TM_OK;
+  }
+  return fail(TM_ERR_ARG, "train: rows too wide for one CTA (%u words, %u state bits)", sh.Wpmax,
+              sh.Bmax);
+}
+
+// Uploads the machine table and work list and launches `p` over epochs
+// [e0, e1).  `ms` (optional) receives the kernel's device time.
+static int launch_plan(const TrainPlan &p, const TrainShape &sh, const std::vector<TrainDev> &td,
+                       const std::vector<WorkItem> &work, uint32_t e0, uint32_t e1,
+                       tm_machine *m0, float *ms, uint32_t *herr) {
+  cudaStream_t st = m0->st;
+  const size_t tb = td.size() * sizeof(TrainDev);
+  const size_t wb = work.size() * sizeof(WorkItem);
+  const size_t off_w = (tb + 255) & ~(size_t)255;
+  const size_t off_c = (off_w + wb + 255) & ~(size_t)255;
+  CK(m0->tdev.ensure(off_c + 256));
+  uint8_t *base = m0->tdev.as<uint8_t>();
+  CK(cudaMemcpyAsync(base, td.data(), tb, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(base + off_w, work.data(), wb, cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(base + off_c, 0, 8, st));
+  uint32_t *counter = (uint32_t *)(base + off_c);
+  uint32_t *err = counter + 1;
+  if (ms) CK(cudaEventRecord(m0->ev0, st));
+  if (p.mode == TM_MODE_WARP)
+    CK(launch_train_warp((const TrainDev *)base, (const WorkItem *)(base + off_w),
+                         (uint32_t)work.size(), counter, e0, e1, sh.Wpmax, sh.Bmin, sh.Bmax,
+                         sh.smax, p.grid, st));
+  else
+    CK(launch_train((const TrainDev *)base, (const WorkItem *)(base + off_w),
+                    (uint32_t)work.size(), counter, e0, e1, p.lay, p.mode, sh.Bmin, sh.Bmax,
+                    p.grid, err, st));
+  if (ms) CK(cudaEventRecord(m0->ev1, st));
+  note_launch(m0, 1);
+  *herr = 0;
+  CK(cudaMemcpyAsync(herr, err, 4, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (ms) CK(cudaEventElapsedTime(ms, m0->ev0, m0->ev1));
+  return TM_OK;
+}
+
+// Process-wide cache of tuned variants, keyed by launch shape.
+static std::mutex g_tune_mu;
+static std::map<std::string, int> g_tuned;
+
+static std::string tune_key(const TrainShape &sh, const tm_machine *m0) {
+  char k[160];
+  // units bucketed by powers of two: the wave count matters, not the exact count
+  uint32_t ub = 0;
+  while ((1u << ub) < sh.units && ub < 31) ub++;
+  snprintf(k, sizeof k, "%d:%u:%u:%u:%u:%u:%d:%d", m0->device, sh.Wpmax, sh.Bmin, sh.Bmax, sh.smax,
+           ub, m0->no_warp ? 1 : 0, m0->pair ? 1 : 0);
+  return k;
+}
+
+static bool lookup_tuned(const TrainShape &sh, const tm_machine *m0, TrainPlan &out) {
+  int mode;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tuned.find(tune_key(sh, m0));
+    if (it == g_tuned.end()) return false;
+    mode = it->second;
+  }
+  return plan_mode(mode, sh, out);
+}
+
+// Times every feasible variant on the first `trial` samples of epoch 0 of
+// (at most) the first few waves of units, keeps the fastest, and resets the
+// automata of every job to their initial state.
+static int autotune_plan(std::vector<TrainJob> &jobs, const std::vector<TrainDev> &td,
+                         const std::vector<WorkItem> &work, const TrainShape &sh,
+                         tm_machine *m0, TrainPlan &out, bool &tuned) {
+  tuned = false;
+  if (m0->autotune == 1 && lookup_tuned(sh, m0, out)) {
+    tuned = true;
+    return TM_OK;
+  }
+  if (!m0->ev0) {
+    CK(cudaEventCreate(&m0->ev0));
+    CK(cudaEventCreate(&m0->ev1));
+  }
+  std::vector<TrainPlan> cand;
+  for (int mode : {TM_MODE_WARP, TM_MODE_SMEM, TM_MODE_GLOBAL, TM_MODE_PAIR}) {
+    if (mode == TM_MODE_WARP && m0->no_warp) continue;
+    TrainPlan p;
+    if (plan_mode(mode, sh, p)) cand.push_back(p);
+  }
+  if (cand.size() < 2) return TM_OK;  // nothing to choose: the heuristic plan
+  // trial: up to 2 x 4 waves of the heaviest units, up to 1024 samples each
+  std::vector<TrainDev> ttd = td;
+  for (auto &t : ttd) t.n = std::min<uint32_t>(t.n, 1024);
+  const size_t nu = std::min<size_t>(work.size(), (size_t)sh.sms * 8);
+  std::vector<WorkItem> tw(work.begin(), work.begin() + nu);
+  TrainShape tsh = sh;
+  tsh.units = (uint32_t)nu;
+  int best = -1;
+  float best_ms = 0;
+  for (size_t i = 0; i < cand.size(); i++) {
+    TrainPlan p;
+    if (!plan_mode(cand[i].mode, tsh, p)) continue;
+    float t = 0, tmin = 0;
+    for (int rep = 0; rep < 2; rep++) {
+      uint32_t herr = 0;
+      int rc = launch_plan(p, tsh, ttd, tw, 0, 1, m0, &t, &herr);
+      if (rc) return rc;
+      if (herr) return fail(TM_ERR_DEVICE, "train: a sample copy did not complete (status %u)", herr);
+      tmin = rep == 0 ? t : std::min(tmin, t);
+    }
+    if (best < 0 || tmin < best_ms) {
+      best = (int)i;
+      best_ms = tmin;
+    }
+  }
+  // back to the initial state (capi.c:1136-1146)
+  for (auto &J : jobs) {
+    tm_machine *m = J.m;
+    cudaError_t e = launch_setup(m->d_act, m->d_cnt, m->d_cls, m->classes, m->clauses, m->B,
+                                 m->act_words, m0->st);
+    if (e != cudaSuccess) return fail(TM_ERR_CUDA, "setup: %s", cudaGetErrorString(e));
+    note_launch(m0, 1);
+  }
+  if (best < 0) return TM_OK;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tuned[tune_key(sh, m0)] = cand[best].mode;
+  }
+  if (!plan_mode(cand[best].mode, sh, out)) return TM_OK;
+  tuned = true;
+  return TM_OK;
+}
+
 // Runs local epochs [e0, e1) of every job in one launch (units of all jobs
 // share the grid).  Permutations are built per job for those epochs.
 static int run_epochs(std::vector<TrainJob> &jobs, uint32_t e0, uint32_t e1, tm_machine *owner) {
@@ -549,109 +753,37 @@ static int run_epochs(std::vector<TrainJob> &jobs, uint32_t e0, uint32_t e1, tm_
   if (work.empty()) return TM_OK;
   std::stable_sort(work.begin(), work.end(),
                    [](const WorkItem &a, const WorkItem &b) { return a.cost > b.cost; });
-  // automata in shared memory when a unit fits one SM, else in global
-  // memory (L2-resident working set) or, on request, split over a 2-CTA
-  // cluster
-  const int optin = max_smem_optin(dev);
-  if (Wpmax <= 64 && Bmax <= 8 && !m0->no_warp) {
-    // short rows: one warp per unit
-    size_t wsm = 0;
-    const int occ = train_warp_occupancy(Wpmax, Bmin, Bmax, smax, &wsm);
-    if (occ > 0 && (int)wsm <= optin) {
-      const int grid = (int)std::min<uint64_t>((work.size() + 3) / 4, (uint64_t)num_sms(dev) * occ);
-      m0->last_mode = TM_MODE_WARP;
-      m0->stats.train_mode = TM_MODE_WARP;
-      const size_t tb = td.size() * sizeof(TrainDev);
-      const size_t wb = work.size() * sizeof(WorkItem);
-      const size_t off_w = (tb + 255) & ~(size_t)255;
-      const size_t off_c = (off_w + wb + 255) & ~(size_t)255;
-      CK(m0->tdev.ensure(off_c + 256));
-      uint8_t *base = m0->tdev.as<uint8_t>();
-      CK(cudaMemcpyAsync(base, td.data(), tb, cudaMemcpyHostToDevice, st));
-      CK(cudaMemcpyAsync(base + off_w, work.data(), wb, cudaMemcpyHostToDevice, st));
-      CK(cudaMemsetAsync(base + off_c, 0, 8, st));
-      uint32_t *counter = (uint32_t *)(base + off_c);
-      if (m0->timing) CK(cudaEventRecord(m0->ev0, st));
-      CK(launch_train_warp((const TrainDev *)base, (const WorkItem *)(base + off_w),
-                           (uint32_t)work.size(), counter, e0, e1, Wpmax, Bmin, Bmax, smax,
-                           grid, st));
-      if (m0->timing) CK(cudaEventRecord(m0->ev1, st));
-      note_launch(m0, 1);
-      CK(cudaStreamSynchronize(st));
-      m0->stats.train_launches++;
-      for (auto &J : jobs)
-        m0->stats.train_unit_steps += (uint64_t)J.m->classes * J.m->clause_chunks * J.a->samples *
-                                      (std::min<uint32_t>(J.a->iterations, e1) > e0
-                                           ? std::min<uint32_t>(J.a->iterations, e1) - e0 : 0);
-      if (m0->timing) {
-        float ms = 0;
-        CK(cudaEventElapsedTime(&ms, m0->ev0, m0->ev1));
-        m0->stats.train_kernel_ms += ms;
-      }
-      return TM_OK;
+  TrainShape sh{Wpmax, Bmin, Bmax, smax, (uint32_t)work.size(), max_smem_optin(dev),
+                num_sms(dev)};
+  TrainPlan plan;
+  bool tuned = false;
+  if (m0->autotune && e0 == 0) {
+    // the automata hold their initial state here (every train call starts
+    // from it), so trial launches may run on them and a setup restores them
+    int rc = autotune_plan(jobs, td, work, sh, m0, plan, tuned);
+    if (rc) return rc;
+  }
+  if (!tuned) {
+    if (m0->autotune && lookup_tuned(sh, m0, plan)) {
+      tuned = true;
+    } else {
+      int rc = heuristic_plan(sh, m0, plan);
+      if (rc) return rc;
     }
   }
-  int mode = TM_MODE_SMEM;
-  TrainSmem lay = plan_smem(Wpmax, Bmax, smax, mode);
-  // (measured on B200: the pair's per-sample cluster barrier costs more than
-  // the L2 round trips it saves, so global memory is the default)
-  if ((int)lay.total > optin && Bmax <= 8 && m0->pair) {
-    mode = TM_MODE_PAIR;
-    lay = plan_smem(Wpmax, Bmax, smax, mode);
-  }
-  int occ = (int)lay.total <= optin ? train_occupancy(lay, mode, Bmin, Bmax) : 0;
-  if (mode == TM_MODE_SMEM) {
-    // Count planes in shared memory save L2 round trips but can cost
-    // resident CTAs; the variant with more CTAs per SM wins, shared memory
-    // on a tie (measured on B200: 8,192-feature rows train 26 % faster with
-    // global planes at two CTAs per SM than with shared planes at one).
-    const TrainSmem lg = plan_smem(Wpmax, Bmax, smax, TM_MODE_GLOBAL);
-    const int og = (int)lg.total <= optin ? train_occupancy(lg, TM_MODE_GLOBAL, Bmin, Bmax) : 0;
-    if (og > occ) {
-      mode = TM_MODE_GLOBAL;
-      lay = lg;
-      occ = og;
-    }
-  }
-  if ((int)lay.total > optin)
-    return fail(TM_ERR_ARG, "train: rows too wide for one CTA (%u bytes of shared memory)",
-                lay.total);
-  if (occ <= 0) return fail(TM_ERR_CUDA, "train: kernel cannot be resident (smem %u)", lay.total);
-  const int grid = mode == TM_MODE_PAIR
-                       ? 2 * (int)std::min<uint64_t>(work.size(), (uint64_t)occ)
-                       : (int)std::min<uint64_t>(work.size(), (uint64_t)num_sms(dev) * occ);
-  m0->last_mode = mode;
-  m0->stats.train_mode = mode;
-  // device tables: [TrainDev...][WorkItem...][counter][err]
-  const size_t tb = td.size() * sizeof(TrainDev);
-  const size_t wb = work.size() * sizeof(WorkItem);
-  const size_t off_w = (tb + 255) & ~(size_t)255;
-  const size_t off_c = (off_w + wb + 255) & ~(size_t)255;
-  CK(m0->tdev.ensure(off_c + 256));
-  uint8_t *base = m0->tdev.as<uint8_t>();
-  CK(cudaMemcpyAsync(base, td.data(), tb, cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(base + off_w, work.data(), wb, cudaMemcpyHostToDevice, st));
-  CK(cudaMemsetAsync(base + off_c, 0, 8, st));
-  uint32_t *counter = (uint32_t *)(base + off_c);
-  uint32_t *err = counter + 1;
-  if (m0->timing) CK(cudaEventRecord(m0->ev0, st));
-  CK(launch_train((const TrainDev *)base, (const WorkItem *)(base + off_w), (uint32_t)work.size(),
-                  counter, e0, e1, lay, mode, Bmin, Bmax, grid, err, st));
-  if (m0->timing) CK(cudaEventRecord(m0->ev1, st));
-  note_launch(m0, 1);
+  m0->last_mode = plan.mode;
+  m0->stats.train_mode = plan.mode;
+  m0->stats.train_autotuned = tuned ? 1 : 0;
+  float ms = 0;
   uint32_t herr = 0;
-  CK(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
+  int rc = launch_plan(plan, sh, td, work, e0, e1, m0, m0->timing ? &ms : nullptr, &herr);
+  if (rc) return rc;
   m0->stats.train_launches++;
   for (auto &J : jobs)
     m0->stats.train_unit_steps += (uint64_t)J.m->classes * J.m->clause_chunks * J.a->samples *
                                   (std::min<uint32_t>(J.a->iterations, e1) > e0
                                        ? std::min<uint32_t>(J.a->iterations, e1) - e0 : 0);
-  if (m0->timing) {
-    float ms = 0;
-    CK(cudaEventElapsedTime(&ms, m0->ev0, m0->ev1));
-    m0->stats.train_kernel_ms += ms;
-  }
+  if (m0->timing) m0->stats.train_kernel_ms += ms;
   if (herr) return fail(TM_ERR_DEVICE, "train: a sample copy did not complete (status %u)", herr);
   return TM_OK;
 }

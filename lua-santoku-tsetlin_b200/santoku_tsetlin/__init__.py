@@ -105,6 +105,7 @@ class Stats(ctypes.Structure):
         ("kernel_launches", ctypes.c_uint64),
         ("train_unit_steps", ctypes.c_uint64),
         ("train_mode", ctypes.c_int32),
+        ("train_autotuned", ctypes.c_int32),
     ]
 
     def as_dict(self):
@@ -129,7 +130,7 @@ EXPORTS = (
     "tm_checkpoint", "tm_restore", "tm_reconfigure", "tm_restrict", "tm_type",
     "tm_destroy", "tm_last_error", "tm_align", "tm_get_info", "tm_export_state",
     "tm_import_state", "tm_class_accuracy", "tm_encoding_accuracy", "tm_bits_to_cvec", "tm_bits_to_cvec_ind",
-    "tm_predict_noalloc", "tm_stats_enable", "tm_get_stats", "tm_reset_stats", "tm_serve_open", "tm_serve_submit", "tm_serve_poll",
+    "tm_predict_noalloc", "tm_int_peaks", "tm_set_autotune", "tm_stats_enable", "tm_get_stats", "tm_reset_stats", "tm_serve_open", "tm_serve_submit", "tm_serve_poll",
     "tm_serve_latency_us", "tm_serve_close",
 )
 
@@ -171,6 +172,8 @@ def lib():
     L.tm_export_state.argtypes = [vp, vp, vp]
     L.tm_import_state.argtypes = [vp, vp, vp]
     L.tm_predict_noalloc.argtypes = [vp, vp, u64, vp, vp]
+    L.tm_int_peaks.argtypes = [i32, vp]
+    L.tm_set_autotune.argtypes = [vp, i32]
     L.tm_class_accuracy.argtypes = [vp, vp, u64, u32, i32, i32, vp]
     L.tm_encoding_accuracy.argtypes = [vp, vp, u64, u32, i32, i32, vp]
     L.tm_bits_to_cvec.argtypes = [vp, u64, u64, u32, i32, i32, i32, vp]
@@ -444,6 +447,12 @@ class Machine:
     def stats_enable(self, on=True):
         _check(lib().tm_stats_enable(self.handle, 1 if on else 0))
 
+    def set_autotune(self, mode=1):
+        """Train-kernel variant choice: 0 heuristic, 1 tuned once per launch
+        shape (default), 2 tuned on every train call.  Results are the same
+        in every mode."""
+        _check(lib().tm_set_autotune(self.handle, int(mode)))
+
     def stats(self):
         st = Stats()
         _check(lib().tm_get_stats(self.handle, ctypes.byref(st)))
@@ -603,6 +612,14 @@ def encoding_accuracy(predicted, expected, n_samples, n_hidden, device=0):
                                       1 if p.device else 0, device, out.ctypes.data))
     return {"bits": [float(v) for v in out[4:]], "mean_hamming": float(out[0]),
             "ber_min": float(out[1]), "ber_max": float(out[2]), "ber_std": float(out[3])}
+
+
+def int_peaks(device=0):
+    """Measured integer-pipe peaks of the GPU (thread-operations/s):
+    {"lop3": .., "popc": .., "iadd": ..}."""
+    o = np.zeros(3, dtype=np.float64)
+    _check(lib().tm_int_peaks(int(device), o.ctypes.data))
+    return {"lop3": float(o[0]), "popc": float(o[1]), "iadd": float(o[2])}
 
 
 def bits_to_cvec(set_bits, n_samples, n_features, flip=False, device=0):

@@ -108,3 +108,11 @@ def test_bits_to_cvec_ind_device_and_train(tm):
 def test_bits_to_cvec_ind_rejects_short_list(tm):
     with pytest.raises(tm.TsetlinError):
         tm.bits_to_cvec_ind(np.zeros(3, np.int64), [0, 5], [0, 8], 4, True)
+
+
+def test_int_peaks_are_sane(tm):
+    """The integer-pipe microbenchmarks return plausible rates: POPC runs
+    at a fraction of the logic-op rate, and all are far above zero."""
+    pk = tm.int_peaks()
+    assert all(v > 1e11 for v in pk.values())
+    assert pk["popc"] < pk["lop3"]

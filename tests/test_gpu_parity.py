@@ -296,10 +296,11 @@ def test_train_batch_equals_individual(tm):
     (16384, 8, False, 1),   # same rows with the automata in global memory (default)
     (300, 12, False, 0),    # more than 8 state bits, shared-memory automata
     (12000, 10, False, 1),  # more than 8 state bits on wide rows: global memory
-    (8192, 8, False, 1),    # planes fit shared memory at one CTA per SM; global planes at two win
-], ids=["warp", "pair", "global", "smem_b12", "global_b10", "global_by_occupancy"])
+    (8192, 8, False, 0),    # 128 KB units, fewer than the SMs: shared planes
+], ids=["warp", "pair", "global", "smem_b12", "global_b10", "smem_few_units"])
 def test_train_variants_match_oracle(tm, monkeypatch, features, state, pair, mode):
     from santoku_tsetlin import datagen
+    monkeypatch.setenv("TSETLIN_B200_AUTOTUNE", "0")  # the heuristic choice is asserted
     if pair:
         monkeypatch.setenv("TSETLIN_B200_PAIR", "1")
     rng = np.random.default_rng(features + state)
@@ -370,3 +371,60 @@ def test_train_batch_each_stops_like_each(tm):
         alone = tm.create("classifier", b)
         alone.train(dict(tt, each=lambda e, s=s: e < s))
         assert np.array_equal(m.export_state()[1], alone.export_state()[1])
+
+
+@pytest.mark.parametrize("features", [784, 8192])
+def test_autotuned_training_matches_heuristic(tm, features):
+    """The tuner's trial launches run on the freshly reset automata and reset
+    them again, so tuned training ends in the heuristic's state, bit for
+    bit, on the first call (tuning) and on a cached second call."""
+    from santoku_tsetlin import datagen
+    rng = np.random.default_rng(features)
+    n, classes = 300, 4
+    x = datagen.flip_pack(rng.random((n, features)) < 0.05).ravel()
+    y = rng.integers(0, classes, size=n).astype(np.int64)
+    tbl = dict(classes=classes, features=features, clauses=32, clause_tolerance=16,
+               clause_maximum=64, specificity=8.0, target=16, reusable=True, seed=5)
+    tt = dict(samples=n, problems=x, solutions=y, iterations=3)
+    ref = tm.create("classifier", tbl)
+    ref.set_autotune(0)
+    ref.train(tt)
+    want = ref.export_state()
+    for mode in (2, 1):
+        t = tm.create("classifier", tbl)
+        t.set_autotune(mode)
+        t.stats_enable(True)
+        t.train(tt)
+        st = t.stats()
+        assert st["train_autotuned"] == 1
+        for a, b in zip(t.export_state(), want):
+            assert np.array_equal(a, b)
+        assert np.array_equal(t.predict(x, n), ref.predict(x, n))
+        t.destroy()
+    with pytest.raises(tm.TsetlinError):
+        ref.set_autotune(3)
+    ref.destroy()
+
+
+def test_global_planes_chosen_by_occupancy(tm, monkeypatch):
+    """160 units of 128 KB: shared planes fit one CTA per SM, global planes
+    two; with more units than SMs the heuristic takes global planes."""
+    from santoku_tsetlin import datagen
+    monkeypatch.setenv("TSETLIN_B200_AUTOTUNE", "0")
+    rng = np.random.default_rng(8192)
+    n, classes, features = 120, 10, 8192
+    x = datagen.flip_pack(rng.random((n + 20, features)) < 0.02)
+    y = rng.integers(0, classes, size=n).astype(np.int64)
+    cfg = dict(type="classifier", classes=classes, features=features, clauses=128,
+               clause_tolerance=32, clause_maximum=300, include_bits=1,
+               specificity=25.0, target=20)
+    inp = dict(n=n, x=x[:n].ravel(), labels=y)
+    m = _oracle_pair("classifier", cfg, inp, 1, seed=23)
+    kind, tbl = ref_table(cfg, seed=23)
+    t = tm.create(kind, tbl)
+    t.stats_enable(True)
+    t.train(train_table(kind, inp, 1))
+    assert t.stats()["train_mode"] == 1
+    a, st = t.export_state()
+    assert np.array_equal(a, m.actions())
+    assert np.array_equal(st, m.state())
