@@ -443,10 +443,10 @@ static TrainSmem plan_smem(uint32_t Wpmax, uint32_t Bmax, uint32_t smax, int mod
   L.list_off = take((mode == TM_MODE_PAIR ? 2 : 1) * TM_BATCH * 4 * 9);  // one entry per thread
   L.votes_off = take(128 * 4);
   L.ib_words = Wpmax;
-  // Type Ib levels and overflow lists: one slot per clause pair
-  L.ib_off = take(2 * (cpc / 2) * Wpmax * 4);
+  // Type Ib levels and overflow lists: TM_IB_SLOTS slots
+  L.ib_off = take(2 * TM_IB_SLOTS * Wpmax * 4);
   L.ovf_cap = std::max<uint32_t>(1, smax / 4);
-  L.ovf_off = take((cpc / 2) * L.ovf_cap * 4);
+  L.ovf_off = take(TM_IB_SLOTS * L.ovf_cap * 4);
   L.misc_off = take(32 * 4);
   L.total = o;
   return L;

@@ -65,14 +65,15 @@ struct TrainSmem {
   uint32_t bar_off;                 // TM_RING mbarriers
   uint32_t list_off;                // active-sample list
   uint32_t votes_off;               // 2 x 8 x 2 clause partial sums
-  uint32_t ib_off, ib_words;        // per clause pair of the CTA: 2 levels x ib_words
-  uint32_t ovf_off, ovf_cap;        // per clause pair of the CTA: overflow entries
+  uint32_t ib_off, ib_words;        // TM_IB_SLOTS slots: 2 levels x ib_words
+  uint32_t ovf_off, ovf_cap;        // TM_IB_SLOTS slots: overflow entries
   uint32_t misc_off;
   uint32_t total;
 };
 
 constexpr int TM_TRAIN_THREADS = 256;  // 8 warps: warp j owns clause j of the unit
-constexpr int TM_RING = 4;             // sample ring depth
+constexpr int TM_RING = 3;             // sample ring depth
+constexpr int TM_IB_SLOTS = 2;         // Type Ib level-counter slots per CTA
 constexpr int TM_BATCH = 256;          // samples examined per batch phase
 
 // Draw-contract stream words (4th Philox counter word).

@@ -484,12 +484,14 @@ __device__ __forceinline__ void unit_sync() {
     __syncthreads();
 }
 
-// Single-CTA variants (256 threads) are capped at 128 registers, two CTAs
-// per SM; a pair CTA (512 threads, its shared memory fills the SM) too.
 // EXACT: every machine of the launch has exactly BM count planes, so the
-// plane loops have no run-time bound.
+// plane loops have no run-time bound; those single-CTA variants (256
+// threads) fit in 85 registers, three CTAs per SM, the others are capped at
+// 128 registers, two CTAs per SM; a pair CTA (512 threads, its shared
+// memory fills the SM) at 128.
 template <bool SMEM_STATE, bool PAIR, int BM, bool EXACT = false>
-__global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS, PAIR ? 1 : 2)
+__global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS,
+                                  PAIR ? 1 : (EXACT ? 3 : 2))
     k_train(const TrainDev *__restrict__ machines, const WorkItem *__restrict__ work,
             uint32_t nwork, uint32_t *__restrict__ counter, uint32_t e_begin, uint32_t e_end,
             TrainSmem lay, uint32_t *__restrict__ err) {
@@ -522,9 +524,8 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
     mbar_fence_init();
     misc[20] = 0;
   }
-  // Type Ib level counters: one slot per clause pair (each pair has exactly
-  // one Type I clause per sample), slot = local clause >> 1
-  for (uint32_t i = tid; i < CPC * lay.ib_words; i += blockDim.x)
+  // Type Ib level counters: TM_IB_SLOTS slots of two levels
+  for (uint32_t i = tid; i < 2 * TM_IB_SLOTS * lay.ib_words; i += blockDim.x)
     ((uint32_t *)(smem + lay.ib_off))[i] = 0;
   if (tid < 8) misc[24 + tid] = 0;
   unit_sync<PAIR>();
@@ -736,132 +737,149 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
           if (!all) continue;
           // Feedback work is shared by the whole CTA: Type Ib picks of every
           // Ib clause are drawn by all threads, then (clause, word) items of
-          // every fed-back clause are spread over all threads.
+          // every fed-back clause are spread over all threads.  Ib clauses
+          // go in groups of TM_IB_SLOTS (one level-counter slot each); a
+          // sample with more Ib clauses than slots takes further rounds.
           uint32_t *ibase = (uint32_t *)(smem + lay.ib_off);
           const uint32_t sp = ent & 0x7FFFFFFFu;
-          if (ibm) {
-            // Type Ib (capi.c:181-190): s single-automaton decrements with
-            // replacement, counted per bit in binary (two levels in shared
-            // memory, larger counts as overflow entries of 4 each), then
-            // applied as saturating subtractions -- order-free, so equal to
-            // the reference's sequential decrements.
-            const uint32_t npk = C.s_picks;
-            const uint32_t nq = (npk + 3) >> 2;
-            for (uint32_t cm = ibm; cm; cm &= cm - 1) {
-              const uint32_t c = __ffs(cm) - 1, jj = rank * CPC + c;
-              uint32_t *l0 = ibase + (size_t)(c >> 1) * 2 * lay.ib_words, *l1 = l0 + lay.ib_words;
-              uint32_t *ov = (uint32_t *)(smem + lay.ovf_off) + (size_t)(c >> 1) * lay.ovf_cap;
-              for (uint32_t q = tid; q < nq; q += blockDim.x) {
-                uint32_t o[4];
-                philox(sp, ee, g, ST_IB | (jj << 20) | q, M.seed, o);
+          uint32_t rest = ibm, pass = fbm;
+          while (true) {
+            uint32_t grp = 0;
+            for (int q = 0; q < TM_IB_SLOTS && rest; q++) {
+              grp |= rest & (0u - rest);
+              rest &= rest - 1u;
+            }
+            pass |= grp;
+            if (grp) {
+              // Type Ib (capi.c:181-190): s single-automaton decrements with
+              // replacement, counted per bit in binary (two levels in shared
+              // memory, larger counts as overflow entries of 4 each), then
+              // applied as saturating subtractions -- order-free, so equal to
+              // the reference's sequential decrements.
+              const uint32_t npk = C.s_picks;
+              const uint32_t nq = (npk + 3) >> 2;
+              uint32_t slot = 0;
+              for (uint32_t cm = grp; cm; cm &= cm - 1, slot++) {
+                const uint32_t c = __ffs(cm) - 1, jj = rank * CPC + c;
+                uint32_t *l0 = ibase + (size_t)slot * 2 * lay.ib_words, *l1 = l0 + lay.ib_words;
+                uint32_t *ov = (uint32_t *)(smem + lay.ovf_off) + (size_t)slot * lay.ovf_cap;
+                for (uint32_t q = tid; q < nq; q += blockDim.x) {
+                  uint32_t o[4];
+                  philox(sp, ee, g, ST_IB | (jj << 20) | q, M.seed, o);
 #pragma unroll
-                for (uint32_t r = 0; r < 4; r++) {
-                  if (4 * q + r < npk) {
-                    const uint32_t bit = __umulhi(o[r], C.input_bits);
-                    const uint32_t w = bit >> 5, mk = 1u << (bit & 31);
-                    if (atomicXor(&l0[w], mk) & mk) {
-                      if (atomicXor(&l1[w], mk) & mk) {
-                        const uint32_t at = atomicAdd(&misc[24 + (c >> 1)], 1u);
-                        if (at < lay.ovf_cap) ov[at] = bit;
+                  for (uint32_t r = 0; r < 4; r++) {
+                    if (4 * q + r < npk) {
+                      const uint32_t bit = __umulhi(o[r], C.input_bits);
+                      const uint32_t w = bit >> 5, mk = 1u << (bit & 31);
+                      if (atomicXor(&l0[w], mk) & mk) {
+                        if (atomicXor(&l1[w], mk) & mk) {
+                          const uint32_t at = atomicAdd(&misc[24 + slot], 1u);
+                          if (at < lay.ovf_cap) ov[at] = bit;
+                        }
                       }
                     }
                   }
                 }
               }
+              __syncthreads();
             }
+            // (clause, pair) items: item i -> the (i / P)-th fed-back clause,
+            // words 2(i % P) and 2(i % P) + 1
+            {
+              // fed-back clauses in ascending order, 4 bits each
+              uint32_t clist = 0, nfed = 0;
+              for (uint32_t cm = pass; cm; cm &= cm - 1, nfed++)
+                clist |= (uint32_t)(__ffs(cm) - 1) << (4 * nfed);
+              const uint32_t P2 = Wp >> 1;
+              const uint32_t total = nfed * P2;
+              const uint32_t NT = blockDim.x;
+              uint32_t kk = tid / P2, qi = tid - kk * P2;
+              for (uint32_t it = tid; it < total; it += NT) {
+                const uint32_t c = (clist >> (4 * kk)) & 15u;
+                const uint32_t w0 = 2 * qi;
+                uint32_t *act_c = act + c * Wp, *cnt_c = cnt + (size_t)c * m * Wp;
+                uint32_t pq[2][BM], aq[2];
+                if ((grp >> c) & 1u) {
+                  uint32_t *l0 = ibase + (size_t)__popc(grp & ((1u << c) - 1u)) * 2 * lay.ib_words;
+                  const uint2 m0 = *(const uint2 *)(l0 + w0);
+                  const uint2 m1 = *(const uint2 *)(l0 + lay.ib_words + w0);
+                  if ((m0.x | m0.y | m1.x | m1.y) != 0) {
+                    *(uint2 *)(l0 + w0) = make_uint2(0, 0);
+                    *(uint2 *)(l0 + lay.ib_words + w0) = make_uint2(0, 0);
+                    ld_pair<BM>(act_c, cnt_c, Wp, m, w0, pq, aq);
+  #pragma unroll
+                    for (int k = 0; k < 2; k++) {
+                      const uint32_t am = word_mask(w0 + k, W, C.amask);
+                      rg_sub_pow2<BM>(pq[k], aq[k], m, 0, k ? m0.y : m0.x, am);
+                      rg_sub_pow2<BM>(pq[k], aq[k], m, 1, k ? m1.y : m1.x, am);
+                    }
+                    st_pair<BM>(act_c, cnt_c, Wp, m, w0, pq, aq);
+                  }
+                } else {
+                  const uint2 x2 = *(const uint2 *)(xr + w0);
+                  const bool t1 = (t1m >> c) & 1u;
+                  const uint32_t vm0 = word_mask(w0, W, C.vmask), vm1 = word_mask(w0 + 1, W, C.vmask);
+                  // Type II changes nothing where every literal is 1
+                  const bool need = t1 || ((~x2.x & vm0) | (~x2.y & vm1)) != 0;
+                  if (need) {
+                    ld_pair<BM>(act_c, cnt_c, Wp, m, w0, pq, aq);
+                    const bool incx = (incm >> c) & 1u;
+  #pragma unroll
+                    for (int k = 0; k < 2; k++) {
+                      const uint32_t x = k ? x2.y : x2.x, vm = k ? vm1 : vm0;
+                      const uint32_t am = word_mask(w0 + k, W, C.amask);
+                      const uint32_t nx = ~x & ~rg_included<BM>(pq[k], aq[k], m, M.ib) & vm;
+                      // Type Ia (capi.c:177-180): inc where x=1 (if L <= maximum),
+                      // dec where x=0 and not included.  Type II (capi.c:192-196):
+                      // inc where x=0 and not included.
+                      if (t1 && incx)
+                        rg_add<BM>(pq[k], aq[k], m, x & vm, nx, am);
+                      else if (t1)
+                        rg_dec<BM>(pq[k], aq[k], m, nx, am);
+                      else
+                        rg_inc<BM>(pq[k], aq[k], m, nx, am);
+                    }
+                    st_pair<BM>(act_c, cnt_c, Wp, m, w0, pq, aq);
+                  }
+                }
+                qi += NT;
+                while (qi >= P2) {
+                  qi -= P2;
+                  kk++;
+                }
+              }
+            }
+            if (grp) {
+              uint32_t novf = 0;
+              for (uint32_t q = 0; q < (uint32_t)__popc(grp); q++) novf += misc[24 + q];
+              if (novf) {
+                // bits picked 4 or more times: rare, applied by one thread
+                __syncthreads();
+                if (tid == 0) {
+                  uint32_t slot = 0;
+                  for (uint32_t cm = grp; cm; cm &= cm - 1, slot++) {
+                    const uint32_t c = __ffs(cm) - 1;
+                    const uint32_t *ov = (uint32_t *)(smem + lay.ovf_off) + (size_t)slot * lay.ovf_cap;
+                    const uint32_t no = misc[24 + slot];
+                    for (uint32_t t = 0; t < no && t < lay.ovf_cap; t++) {
+                      const uint32_t bit = ov[t], w = bit >> 5;
+                      const uint32_t am = w + 1 == W ? C.amask : 0xFFFFFFFFu;
+                      uint32_t pp[BM], aq;
+                      ld_word<BM>(act + c * Wp, cnt + (size_t)c * m * Wp, Wp, m, w, pp, aq);
+                      rg_sub_pow2<BM>(pp, aq, m, 2, 1u << (bit & 31), am);
+                      st_word<BM>(act + c * Wp, cnt + (size_t)c * m * Wp, Wp, m, w, pp, aq);
+                    }
+                    misc[24 + slot] = 0;
+                  }
+                }
+              }
+            }
+            if (!rest) break;
+            // the next group's picks reuse the level slots
             __syncthreads();
-          }
-          // (clause, pair) items: item i -> the (i / P)-th fed-back clause,
-          // words 2(i % P) and 2(i % P) + 1
-          {
-            // fed-back clauses in ascending order, 4 bits each
-            uint32_t clist = 0, nfed = 0;
-            for (uint32_t cm = all; cm; cm &= cm - 1, nfed++)
-              clist |= (uint32_t)(__ffs(cm) - 1) << (4 * nfed);
-            const uint32_t P2 = Wp >> 1;
-            const uint32_t total = nfed * P2;
-            const uint32_t NT = blockDim.x;
-            uint32_t kk = tid / P2, qi = tid - kk * P2;
-            for (uint32_t it = tid; it < total; it += NT) {
-              const uint32_t c = (clist >> (4 * kk)) & 15u;
-              const uint32_t w0 = 2 * qi;
-              uint32_t *act_c = act + c * Wp, *cnt_c = cnt + (size_t)c * m * Wp;
-              uint32_t pq[2][BM], aq[2];
-              if ((ibm >> c) & 1u) {
-                uint32_t *l0 = ibase + (size_t)(c >> 1) * 2 * lay.ib_words;
-                const uint2 m0 = *(const uint2 *)(l0 + w0);
-                const uint2 m1 = *(const uint2 *)(l0 + lay.ib_words + w0);
-                if ((m0.x | m0.y | m1.x | m1.y) != 0) {
-                  *(uint2 *)(l0 + w0) = make_uint2(0, 0);
-                  *(uint2 *)(l0 + lay.ib_words + w0) = make_uint2(0, 0);
-                  ld_pair<BM>(act_c, cnt_c, Wp, m, w0, pq, aq);
-#pragma unroll
-                  for (int k = 0; k < 2; k++) {
-                    const uint32_t am = word_mask(w0 + k, W, C.amask);
-                    rg_sub_pow2<BM>(pq[k], aq[k], m, 0, k ? m0.y : m0.x, am);
-                    rg_sub_pow2<BM>(pq[k], aq[k], m, 1, k ? m1.y : m1.x, am);
-                  }
-                  st_pair<BM>(act_c, cnt_c, Wp, m, w0, pq, aq);
-                }
-              } else {
-                const uint2 x2 = *(const uint2 *)(xr + w0);
-                const bool t1 = (t1m >> c) & 1u;
-                const uint32_t vm0 = word_mask(w0, W, C.vmask), vm1 = word_mask(w0 + 1, W, C.vmask);
-                // Type II changes nothing where every literal is 1
-                const bool need = t1 || ((~x2.x & vm0) | (~x2.y & vm1)) != 0;
-                if (need) {
-                  ld_pair<BM>(act_c, cnt_c, Wp, m, w0, pq, aq);
-                  const bool incx = (incm >> c) & 1u;
-#pragma unroll
-                  for (int k = 0; k < 2; k++) {
-                    const uint32_t x = k ? x2.y : x2.x, vm = k ? vm1 : vm0;
-                    const uint32_t am = word_mask(w0 + k, W, C.amask);
-                    const uint32_t nx = ~x & ~rg_included<BM>(pq[k], aq[k], m, M.ib) & vm;
-                    // Type Ia (capi.c:177-180): inc where x=1 (if L <= maximum),
-                    // dec where x=0 and not included.  Type II (capi.c:192-196):
-                    // inc where x=0 and not included.
-                    if (t1 && incx)
-                      rg_add<BM>(pq[k], aq[k], m, x & vm, nx, am);
-                    else if (t1)
-                      rg_dec<BM>(pq[k], aq[k], m, nx, am);
-                    else
-                      rg_inc<BM>(pq[k], aq[k], m, nx, am);
-                  }
-                  st_pair<BM>(act_c, cnt_c, Wp, m, w0, pq, aq);
-                }
-              }
-              qi += NT;
-              while (qi >= P2) {
-                qi -= P2;
-                kk++;
-              }
-            }
+            pass = 0;
           }
           if (all & (1u << lc)) dirty = true;
-          if (ibm) {
-            uint32_t novf = 0;
-            for (uint32_t cm = ibm; cm; cm &= cm - 1) novf += misc[24 + ((__ffs(cm) - 1) >> 1)];
-            if (novf) {
-              // bits picked 4 or more times: rare, applied by one thread
-              __syncthreads();
-              if (tid == 0) {
-                for (uint32_t cm = ibm; cm; cm &= cm - 1) {
-                  const uint32_t c = __ffs(cm) - 1;
-                  const uint32_t *ov = (uint32_t *)(smem + lay.ovf_off) + (size_t)(c >> 1) * lay.ovf_cap;
-                  const uint32_t no = misc[24 + (c >> 1)];
-                  for (uint32_t t = 0; t < no && t < lay.ovf_cap; t++) {
-                    const uint32_t bit = ov[t], w = bit >> 5;
-                    const uint32_t am = w + 1 == W ? C.amask : 0xFFFFFFFFu;
-                    uint32_t pp[BM], aq;
-                    ld_word<BM>(act + c * Wp, cnt + (size_t)c * m * Wp, Wp, m, w, pp, aq);
-                    rg_sub_pow2<BM>(pp, aq, m, 2, 1u << (bit & 31), am);
-                    st_word<BM>(act + c * Wp, cnt + (size_t)c * m * Wp, Wp, m, w, pp, aq);
-                  }
-                  misc[24 + (c >> 1)] = 0;
-                }
-              }
-            }
-          }
           // the next sample's evaluation reads clauses this step updated
           __syncthreads();
         }
