@@ -384,11 +384,12 @@ def run_ours(args, w):
     }
     if rank == 0:
         # integer-pipe roofline of clause evaluation (after the timed region):
-        # k_predict's inner loop issues 11 ALU-pipe instructions (4 AND-NOT,
-        # 6 carry-save LOP3, 1 add) and 1 POPC per 4 words
+        # per 32 words k_predict's inner loop issues 68 logic ops (6 carry-save
+        # steps of 4 AND-NOT + 6 LOP3, 2 direct steps of 4 AND-NOT) and 14
+        # POPC (6 + 8); POPC and the logic ops issue on separate pipes
         pk = tm.int_peaks(dev.index if dev.index is not None else 0)
         wops = out["kernels"]["predict_literal_evals_per_s"] / 32
-        bound = min(4 * pk["lop3"] / 11, 4 * pk["popc"])
+        bound = min(32 * pk["lop3"] / 68, 32 * pk["popc"] / 14)
         out["kernels"].update({"int_peaks_ops_per_s": pk, "predict_word_ops_per_s": wops,
                                "predict_int_bound_word_ops_per_s": bound,
                                "predict_frac_of_int_bound": wops / bound})

@@ -817,13 +817,13 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
                   }
                 } else {
                   const uint2 x2 = *(const uint2 *)(xr + w0);
-                  const bool t1 = (t1m >> c) & 1u;
+                  const bool t1 = (t1m >> c) & 1u, incx = (incm >> c) & 1u;
                   const uint32_t vm0 = word_mask(w0, W, C.vmask), vm1 = word_mask(w0 + 1, W, C.vmask);
-                  // Type II changes nothing where every literal is 1
-                  const bool need = t1 || ((~x2.x & vm0) | (~x2.y & vm1)) != 0;
+                  // only Type Ia with increments changes words whose literals
+                  // are all 1: Type II and the Type Ia decrements act where x = 0
+                  const bool need = (t1 && incx) || ((~x2.x & vm0) | (~x2.y & vm1)) != 0;
                   if (need) {
                     ld_pair<BM>(act_c, cnt_c, Wp, m, w0, pq, aq);
-                    const bool incx = (incm >> c) & 1u;
   #pragma unroll
                     for (int k = 0; k < 2; k++) {
                       const uint32_t x = k ? x2.y : x2.x, vm = k ? vm1 : vm0;
@@ -1066,7 +1066,8 @@ __global__ void __launch_bounds__(TM_WARP_THREADS)
               const uint32_t w = h ? w1 : w0, x = h ? xb : xa, vm = h ? vm1 : vm0;
               const uint32_t am = h ? am1 : am0;
               if (w >= W) continue;
-              if (!t1 && (~x & vm) == 0) continue;
+              // only Type Ia with increments changes a word whose literals are all 1
+              if (!(t1 && incx) && (~x & vm) == 0) continue;
               uint32_t pp[BM], aq;
               ld_word<BM>(act_c, cnt_c, Wp, m, w, pp, aq);
               const uint32_t nx = ~x & ~rg_included<BM>(pp, aq, m, M.ib) & vm;
@@ -1308,10 +1309,14 @@ __global__ void __launch_bounds__(256, 2)
   const uint32_t s0 = blockIdx.x * PT_S;
   const ClassDev C = cls[h];
   const uint32_t tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  // Failed-literal counts popc(a & ~x) per (clause, sample), accumulated
-  // carry-save: `ones` and `twos` hold bit-sliced partial counts and only
-  // the weight-4 carries are popcounted -- one POPC per four words instead
-  // of four.  Count = 4 * acc + 2 * popc(twos) + popc(ones), exact.
+  // Failed-literal counts popc(a & ~x) per (clause, sample).  Six of every
+  // eight 4-word steps go through carry-save adders: `ones` and `twos` hold
+  // bit-sliced partial counts and only the weight-4 carries are popcounted
+  // (one POPC per four words, ten logic ops); the other two steps popcount
+  // their words directly (four POPC, four logic ops).  POPC and the logic
+  // ops issue on separate pipes (measured on B200: they overlap fully), and
+  // this mix keeps both busy.  acc is the exact count of everything
+  // already reduced: count = acc + 2 * popc(twos) + popc(ones).
   uint32_t acc[4][4], ones[4][4], twos[4][4];
 #pragma unroll
   for (int a = 0; a < 4; a++)
@@ -1354,17 +1359,22 @@ __global__ void __launch_bounds__(256, 2)
         for (int i = 0; i < 4; i++) {
           const uint32_t t0 = a4[c].x & ~x4[i].x, t1 = a4[c].y & ~x4[i].y;
           const uint32_t t2 = a4[c].z & ~x4[i].z, t3 = a4[c].w & ~x4[i].w;
-          uint32_t o = ones[c][i];
-          // carry-save adders: (sum, carry) = (a ^ b ^ c, majority(a, b, c))
-          const uint32_t h1 = (o & t0) | (o & t1) | (t0 & t1);
-          o ^= t0 ^ t1;
-          const uint32_t h2 = (o & t2) | (o & t3) | (t2 & t3);
-          o ^= t2 ^ t3;
-          const uint32_t tw = twos[c][i];
-          const uint32_t f4 = (tw & h1) | (tw & h2) | (h1 & h2);
-          twos[c][i] = tw ^ h1 ^ h2;
-          ones[c][i] = o;
-          acc[c][i] += __popc(f4);
+          if ((kk & 12) == 12) {
+            // steps 3 and 7 of 8: direct popcounts
+            acc[c][i] += __popc(t0) + __popc(t1) + __popc(t2) + __popc(t3);
+          } else {
+            uint32_t o = ones[c][i];
+            // carry-save adders: (sum, carry) = (a ^ b ^ c, majority(a, b, c))
+            const uint32_t h1 = (o & t0) | (o & t1) | (t0 & t1);
+            o ^= t0 ^ t1;
+            const uint32_t h2 = (o & t2) | (o & t3) | (t2 & t3);
+            o ^= t2 ^ t3;
+            const uint32_t tw = twos[c][i];
+            const uint32_t f4 = (tw & h1) | (tw & h2) | (h1 & h2);
+            twos[c][i] = tw ^ h1 ^ h2;
+            ones[c][i] = o;
+            acc[c][i] += 4 * __popc(f4);
+          }
         }
     }
     __syncthreads();
@@ -1373,7 +1383,7 @@ __global__ void __launch_bounds__(256, 2)
   for (int c = 0; c < 4; c++)
 #pragma unroll
     for (int i = 0; i < 4; i++)
-      acc[c][i] = 4 * acc[c][i] + 2 * __popc(twos[c][i]) + __popc(ones[c][i]);
+      acc[c][i] += 2 * __popc(twos[c][i]) + __popc(ones[c][i]);
   int32_t part[4] = {0, 0, 0, 0};
 #pragma unroll
   for (int c = 0; c < 4; c++) {
