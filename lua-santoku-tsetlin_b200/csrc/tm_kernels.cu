@@ -644,6 +644,12 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
           const uint32_t *xr = ring + sl * lay.ring_words;
           const uint32_t ent = list_s[a];
           const uint32_t pa = ent >> 31;
+          // lane c (< CPC) decides local clause c below; its chance draw and
+          // the draw's scaled value do not depend on the automata, so they
+          // are read before the evaluation, off the decision's critical path
+          const uint32_t cl = lane % CPC, jj = rank * CPC + cl;
+          const bool type1 = pa ? !(jj & 1u) : (jj & 1u);
+          const uint64_t drv = bounded64(list_d[a * 8 + 2 * (jj >> 1) + (type1 ? 0 : 1)], T2);
 
           // clause j: literal count L and failed count F (capi.c:97-122).
           // L only changes when the clause is updated, so it is recounted
@@ -721,14 +727,15 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
           // feedback of this CTA's clauses (capi.c:226-242), lane c deciding
           // local clause c: draw 2p decides Type I of pair p, draw 2p+1 Type
           // II; the positive case gives Type I to the even clause.  Masks over
-          // local clauses: Ia/II, Ib, Type I, Ia increments where x = 1.
-          const uint32_t cl = lane % CPC, jj = rank * CPC + cl;
-          const int32_t vj = __shfl_sync(0xFFFFFFFFu, vq, jj);
-          const uint32_t lj = __shfl_sync(0xFFFFFFFFu, Lq, jj);
-          const uint32_t odd = jj & 1u;
-          const bool type1 = pa ? !odd : odd;
-          const uint32_t dr = list_d[a * 8 + 2 * (jj >> 1) + (type1 ? 0 : 1)];
-          const bool fire = lane < CPC && bounded64(dr, T2) < av;
+          // local clauses: Ia/II, Ib, Type I, Ia increments where x = 1.  In a
+          // single CTA lane c already holds clause c's vote and literal count.
+          int32_t vj = vq;
+          uint32_t lj = Lq;
+          if constexpr (PAIR) {
+            vj = __shfl_sync(0xFFFFFFFFu, vq, jj);
+            lj = __shfl_sync(0xFFFFFFFFu, Lq, jj);
+          }
+          const bool fire = lane < CPC && drv < av;
           const uint32_t ibm = __ballot_sync(0xFFFFFFFFu, fire && type1 && vj == 0);
           const uint32_t fbm = __ballot_sync(0xFFFFFFFFu, fire && vj > 0);
           const uint32_t t1m = __ballot_sync(0xFFFFFFFFu, fire && type1 && vj > 0);
