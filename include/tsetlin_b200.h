@@ -269,6 +269,7 @@ typedef struct tm_stats {
                                  1 count planes in global memory, 2 split over a 2-CTA
                                  cluster, 3 one warp per unit (rows of at most 64 words) */
   int32_t train_autotuned;    /* 1 if the autotuner chose that variant */
+  int32_t train_cpw;          /* clauses per warp of that variant */
 } tm_stats;
 /* Train-kernel variant choice.  All variants end in the same automaton
  * state; they differ in speed.  mode 0: heuristic (resident CTAs per SM);
@@ -279,6 +280,13 @@ typedef struct tm_stats {
  * the process; 2: tune on every train call.  No counterpart in the
  * reference (it has one CPU code path). */
 int tm_set_autotune(tm_machine *m, int32_t mode);
+
+/* Pins the train-kernel variant (train_mode values of tm_stats; cpw, the
+ * clauses evaluated per warp in a single-CTA variant with 8 state bits: 1,
+ * 2 or 4 -- 256 / cpw threads per unit); mode -1 returns to the automatic
+ * choice.  A train call that the pinned variant cannot run fails with
+ * TM_ERR_ARG.  For tests and measurements; no counterpart in the reference. */
+int tm_force_variant(tm_machine *m, int32_t mode, int32_t cpw);
 
 /* on != 0 starts timing (events around every train / predict kernel). */
 int tm_stats_enable(tm_machine *m, int32_t on);

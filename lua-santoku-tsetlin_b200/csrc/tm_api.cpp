@@ -107,6 +107,8 @@ struct tm_machine {
   bool pair = false;      // TSETLIN_B200_PAIR=1: split units too large for one SM over a
                           // 2-CTA cluster instead of keeping their automata in global memory
   bool no_warp = false;   // TSETLIN_B200_NO_WARP=1: never train a unit with one warp
+  int force_mode = -1;    // >= 0: train with this variant (tm_force_variant)
+  int force_cpw = 1;
   int autotune = 1;       // 0 heuristic variant choice, 1 tuned (cached per shape),
                           // 2 tuned afresh on every train call; TSETLIN_B200_AUTOTUNE
   int last_mode = -1;     // k_train variant of the last launch
@@ -321,6 +323,15 @@ extern "C" void tm_destroy(tm_machine *m) {
   delete m;
 }
 
+extern "C" int tm_force_variant(tm_machine *m, int32_t mode, int32_t cpw) {
+  if (!m) return fail(TM_ERR_ARG, "null machine");
+  if (mode < -1 || mode > TM_MODE_WARP || (cpw != 1 && cpw != 2 && cpw != 4))
+    return fail(TM_ERR_ARG, "force_variant: mode -1..3, clauses per warp 1, 2 or 4");
+  m->force_mode = mode;
+  m->force_cpw = cpw;
+  return TM_OK;
+}
+
 extern "C" int tm_set_autotune(tm_machine *m, int32_t mode) {
   if (!m) return fail(TM_ERR_ARG, "null machine");
   if (mode < 0 || mode > 2) return fail(TM_ERR_ARG, "autotune: mode must be 0, 1 or 2");
@@ -425,7 +436,7 @@ struct TrainJob {
   uint64_t seed = 0;
 };
 
-static TrainSmem plan_smem(uint32_t Wpmax, uint32_t Bmax, uint32_t smax, int mode) {
+static TrainSmem plan_smem(uint32_t Wpmax, uint32_t Bmax, uint32_t smax, int mode, int cpw = 1) {
   TrainSmem L{};
   uint32_t o = 0;
   auto take = [&](uint32_t bytes) {
@@ -440,7 +451,7 @@ static TrainSmem plan_smem(uint32_t Wpmax, uint32_t Bmax, uint32_t smax, int mod
   L.ring_words = Wpmax;
   L.ring_off = take(TM_RING * Wpmax * 4);
   L.bar_off = take(TM_RING * 8);
-  L.list_off = take((mode == TM_MODE_PAIR ? 2 : 1) * TM_BATCH * 4 * 9);  // one entry per thread
+  L.list_off = take(train_threads(mode, cpw) * 4 * 9);  // one entry per thread
   L.votes_off = take(128 * 4);
   L.ib_words = Wpmax;
   // Type Ib levels and overflow lists: TM_IB_SLOTS slots
@@ -493,14 +504,19 @@ struct TrainShape {
 
 struct TrainPlan {
   int mode = TM_MODE_GLOBAL;
+  int cpw = 1;  // clauses per warp (single-CTA variants, 8 state bits)
   TrainSmem lay{};
   int grid = 0;
 };
 
-// Fills `p` for `mode` when that variant can run this launch.
-static bool plan_mode(int mode, const TrainShape &sh, TrainPlan &p) {
+// Fills `p` for `mode` (and `cpw` clauses per warp) when that variant can
+// run this launch.
+static bool plan_mode(int mode, const TrainShape &sh, TrainPlan &p, int cpw = 1) {
   p = TrainPlan{};
   p.mode = mode;
+  p.cpw = cpw;
+  if (cpw != 1 && (mode == TM_MODE_WARP || mode == TM_MODE_PAIR || sh.Bmin != 8 || sh.Bmax != 8))
+    return false;
   if (mode == TM_MODE_WARP) {
     if (sh.Wpmax > 64 || sh.Bmax > 8) return false;
     size_t wsm = 0;
@@ -510,9 +526,9 @@ static bool plan_mode(int mode, const TrainShape &sh, TrainPlan &p) {
     return true;
   }
   if (mode == TM_MODE_PAIR && sh.Bmax > 8) return false;
-  p.lay = plan_smem(sh.Wpmax, sh.Bmax, sh.smax, mode);
+  p.lay = plan_smem(sh.Wpmax, sh.Bmax, sh.smax, mode, cpw);
   if ((int)p.lay.total > sh.optin) return false;
-  const int occ = train_occupancy(p.lay, mode, sh.Bmin, sh.Bmax);
+  const int occ = train_occupancy(p.lay, mode, sh.Bmin, sh.Bmax, cpw);
   if (occ <= 0) return false;
   p.grid = mode == TM_MODE_PAIR ? 2 * (int)std::min<uint64_t>(sh.units, (uint64_t)occ)
                                 : (int)std::min<uint64_t>(sh.units, (uint64_t)sh.sms * occ);
@@ -571,7 +587,7 @@ static int launch_plan(const TrainPlan &p, const TrainShape &sh, const std::vect
   else
     CK(launch_train((const TrainDev *)base, (const WorkItem *)(base + off_w),
                     (uint32_t)work.size(), counter, e0, e1, p.lay, p.mode, sh.Bmin, sh.Bmax,
-                    p.grid, err, st));
+                    p.cpw, p.grid, err, st));
   if (ms) CK(cudaEventRecord(m0->ev1, st));
   note_launch(m0, 1);
   *herr = 0;
@@ -583,7 +599,7 @@ static int launch_plan(const TrainPlan &p, const TrainShape &sh, const std::vect
 
 // Process-wide cache of tuned variants, keyed by launch shape.
 static std::mutex g_tune_mu;
-static std::map<std::string, int> g_tuned;
+static std::map<std::string, std::pair<int, int>> g_tuned;  // -> (mode, clauses per warp)
 
 static std::string tune_key(const TrainShape &sh, const tm_machine *m0) {
   char k[160];
@@ -596,14 +612,14 @@ static std::string tune_key(const TrainShape &sh, const tm_machine *m0) {
 }
 
 static bool lookup_tuned(const TrainShape &sh, const tm_machine *m0, TrainPlan &out) {
-  int mode;
+  std::pair<int, int> v;
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tuned.find(tune_key(sh, m0));
     if (it == g_tuned.end()) return false;
-    mode = it->second;
+    v = it->second;
   }
-  return plan_mode(mode, sh, out);
+  return plan_mode(v.first, sh, out, v.second);
 }
 
 // Times every feasible variant on the first `trial` samples of epoch 0 of
@@ -624,8 +640,10 @@ static int autotune_plan(std::vector<TrainJob> &jobs, const std::vector<TrainDev
   std::vector<TrainPlan> cand;
   for (int mode : {TM_MODE_WARP, TM_MODE_SMEM, TM_MODE_GLOBAL, TM_MODE_PAIR}) {
     if (mode == TM_MODE_WARP && m0->no_warp) continue;
-    TrainPlan p;
-    if (plan_mode(mode, sh, p)) cand.push_back(p);
+    for (int cpw : {1, 2, 4}) {
+      TrainPlan p;
+      if (plan_mode(mode, sh, p, cpw)) cand.push_back(p);
+    }
   }
   if (cand.size() < 2) return TM_OK;  // nothing to choose: the heuristic plan
   // trial: up to 2 x 4 waves of the heaviest units, up to 1024 samples each
@@ -639,7 +657,7 @@ static int autotune_plan(std::vector<TrainJob> &jobs, const std::vector<TrainDev
   float best_ms = 0;
   for (size_t i = 0; i < cand.size(); i++) {
     TrainPlan p;
-    if (!plan_mode(cand[i].mode, tsh, p)) continue;
+    if (!plan_mode(cand[i].mode, tsh, p, cand[i].cpw)) continue;
     float t = 0, tmin = 0;
     for (int rep = 0; rep < 2; rep++) {
       uint32_t herr = 0;
@@ -664,9 +682,9 @@ static int autotune_plan(std::vector<TrainJob> &jobs, const std::vector<TrainDev
   if (best < 0) return TM_OK;
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tuned[tune_key(sh, m0)] = cand[best].mode;
+    g_tuned[tune_key(sh, m0)] = std::make_pair(cand[best].mode, cand[best].cpw);
   }
-  if (!plan_mode(cand[best].mode, sh, out)) return TM_OK;
+  if (!plan_mode(cand[best].mode, sh, out, cand[best].cpw)) return TM_OK;
   tuned = true;
   return TM_OK;
 }
@@ -757,13 +775,17 @@ static int run_epochs(std::vector<TrainJob> &jobs, uint32_t e0, uint32_t e1, tm_
                 num_sms(dev)};
   TrainPlan plan;
   bool tuned = false;
-  if (m0->autotune && e0 == 0) {
+  if (m0->force_mode >= 0) {
+    if (!plan_mode(m0->force_mode, sh, plan, m0->force_cpw))
+      return fail(TM_ERR_ARG, "train: variant %d with %d clauses per warp cannot run this launch",
+                  m0->force_mode, m0->force_cpw);
+  } else if (m0->autotune && e0 == 0) {
     // the automata hold their initial state here (every train call starts
     // from it), so trial launches may run on them and a setup restores them
     int rc = autotune_plan(jobs, td, work, sh, m0, plan, tuned);
     if (rc) return rc;
   }
-  if (!tuned) {
+  if (!tuned && m0->force_mode < 0) {
     if (m0->autotune && lookup_tuned(sh, m0, plan)) {
       tuned = true;
     } else {
@@ -774,6 +796,7 @@ static int run_epochs(std::vector<TrainJob> &jobs, uint32_t e0, uint32_t e1, tm_
   m0->last_mode = plan.mode;
   m0->stats.train_mode = plan.mode;
   m0->stats.train_autotuned = tuned ? 1 : 0;
+  m0->stats.train_cpw = plan.cpw;
   float ms = 0;
   uint32_t herr = 0;
   int rc = launch_plan(plan, sh, td, work, e0, e1, m0, m0->timing ? &ms : nullptr, &herr);

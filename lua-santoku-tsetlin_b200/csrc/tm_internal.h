@@ -99,9 +99,11 @@ constexpr int TM_MODE_GLOBAL = 1;
 constexpr int TM_MODE_PAIR = 2;
 cudaError_t launch_train(const TrainDev *machines, const WorkItem *work, uint32_t nwork,
                          uint32_t *counter, uint32_t e_begin, uint32_t e_end, const TrainSmem &lay,
-                         int mode, uint32_t Bmin, uint32_t Bmax, int grid, uint32_t *err,
-                         cudaStream_t st);
-int train_occupancy(const TrainSmem &lay, int mode, uint32_t Bmin, uint32_t Bmax);
+                         int mode, uint32_t Bmin, uint32_t Bmax, int cpw, int grid,
+                         uint32_t *err, cudaStream_t st);
+int train_occupancy(const TrainSmem &lay, int mode, uint32_t Bmin, uint32_t Bmax, int cpw);
+// threads per CTA of a train-kernel variant (cpw: clauses per warp)
+int train_threads(int mode, int cpw);
 // k_train_warp: one warp per unit for rows of at most 64 words and B <= 8
 constexpr int TM_MODE_WARP = 3;
 int train_warp_occupancy(uint32_t Wpmax, uint32_t Bmin, uint32_t Bmax, uint32_t smax,

@@ -489,19 +489,22 @@ __device__ __forceinline__ void unit_sync() {
 // threads) fit in 85 registers, three CTAs per SM, the others are capped at
 // 128 registers, two CTAs per SM; a pair CTA (512 threads, its shared
 // memory fills the SM) at 128.
-template <bool SMEM_STATE, bool PAIR, int BM, bool EXACT = false>
-__global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS,
-                                  PAIR ? 1 : (EXACT ? 3 : 2))
+// CPW: clauses evaluated by one warp (1, 2 or 4): a single CTA has 256 /
+// CPW threads, so small units fit more CTAs per SM.
+template <bool SMEM_STATE, bool PAIR, int BM, bool EXACT = false, int CPW = 1>
+__global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS / CPW,
+                                  PAIR ? 1 : (EXACT ? 3 * CPW : 2))
     k_train(const TrainDev *__restrict__ machines, const WorkItem *__restrict__ work,
             uint32_t nwork, uint32_t *__restrict__ counter, uint32_t e_begin, uint32_t e_end,
             TrainSmem lay, uint32_t *__restrict__ err) {
+  static_assert(CPW == 1 || !PAIR, "clause pairs evaluate one clause per warp group");
   constexpr uint32_t NW = PAIR ? 4 : 1;   // warps per clause
   constexpr uint32_t CPC = PAIR ? 4 : 8;  // clauses per CTA
   constexpr uint32_t GS = 32 * NW;        // lanes per clause group
   extern __shared__ __align__(128) uint8_t smem[];
   const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t rank = PAIR ? cg::this_cluster().block_rank() : 0;
-  const uint32_t lc = warp / NW;            // local clause
+  const uint32_t lc = warp / NW * CPW;      // first local clause of this warp
   const uint32_t gl = (warp % NW) * 32 + lane;  // lane within the clause group
   const uint32_t j = rank * CPC + lc;       // clause of the unit (0..7)
   uint32_t *ring = (uint32_t *)(smem + lay.ring_off);
@@ -573,8 +576,13 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
     }
     uint32_t *act_j = act + lc * Wp;
     uint32_t *cnt_j = cnt + (size_t)lc * m * Wp;
-    bool dirty = true;       // this warp's clause changed since its literal count was taken
-    uint32_t lit_cache = 0;  // its literal count when clean
+    bool dirty[CPW];         // this warp's clauses changed since their literal counts were taken
+    uint32_t lit_cache[CPW];  // their literal counts when clean
+#pragma unroll
+    for (int q = 0; q < CPW; q++) {
+      dirty[q] = true;
+      lit_cache[q] = 0;
+    }
     const uint32_t T = M.T;
     const uint64_t T2 = 2ull * T;
     const uint32_t ep_end = e_end < M.epochs ? e_end : M.epochs;
@@ -651,40 +659,44 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
           const bool type1 = pa ? !(jj & 1u) : (jj & 1u);
           const uint64_t drv = bounded64(list_d[a * 8 + 2 * (jj >> 1) + (type1 ? 0 : 1)], T2);
 
-          // clause j: literal count L and failed count F (capi.c:97-122).
-          // L only changes when the clause is updated, so it is recounted
-          // only after feedback to the clause (`dirty`).
-          uint32_t l = 0, f = 0;
-          const uint32_t Q = Wp >> 2, qlast = (W - 1) >> 2;
-#pragma unroll 4
-          for (uint32_t qi = gl; qi < Q; qi += GS) {
-            uint4 a4 = *(const uint4 *)(act_j + 4 * qi);
-            const uint4 x4 = *(const uint4 *)(xr + 4 * qi);
-            if (qi == qlast) {  // evaluation mask on word W-1 (capi.c:104-106)
-              const uint32_t k = (W - 1) & 3;
-              if (k == 0) a4.x &= C.emask;
-              if (k == 1) a4.y &= C.emask;
-              if (k == 2) a4.z &= C.emask;
-              if (k == 3) a4.w &= C.emask;
-            }
-            f += __popc(a4.x & ~x4.x) + __popc(a4.y & ~x4.y) + __popc(a4.z & ~x4.z) +
-                 __popc(a4.w & ~x4.w);
-            if (dirty) l += __popc(a4.x) + __popc(a4.y) + __popc(a4.z) + __popc(a4.w);
-          }
-          if (dirty) {
-            l = __reduce_add_sync(0xFFFFFFFFu, l);
-          } else {
-            l = (warp % NW == 0) ? lit_cache : 0u;
-          }
-          f = __reduce_add_sync(0xFFFFFFFFu, f);
+          // clauses j .. j+CPW-1: literal count L and failed count F
+          // (capi.c:97-122).  L only changes when the clause is updated, so
+          // it is recounted only after feedback to the clause (`dirty`).
           uint32_t *slot_parts = parts + (a & 1) * 64;
-          if (lane == 0) {
-            const uint32_t at = j * 8 + (warp % NW) * 2;
-            slot_parts[at] = l;
-            slot_parts[at + 1] = f;
-            if constexpr (PAIR) {
-              peer_parts[(a & 1) * 64 + at] = l;
-              peer_parts[(a & 1) * 64 + at + 1] = f;
+#pragma unroll
+          for (int q = 0; q < CPW; q++) {
+            const uint32_t *act_q = act_j + q * Wp;
+            uint32_t l = 0, f = 0;
+            const uint32_t Q = Wp >> 2, qlast = (W - 1) >> 2;
+#pragma unroll 4
+            for (uint32_t qi = gl; qi < Q; qi += GS) {
+              uint4 a4 = *(const uint4 *)(act_q + 4 * qi);
+              const uint4 x4 = *(const uint4 *)(xr + 4 * qi);
+              if (qi == qlast) {  // evaluation mask on word W-1 (capi.c:104-106)
+                const uint32_t k = (W - 1) & 3;
+                if (k == 0) a4.x &= C.emask;
+                if (k == 1) a4.y &= C.emask;
+                if (k == 2) a4.z &= C.emask;
+                if (k == 3) a4.w &= C.emask;
+              }
+              f += __popc(a4.x & ~x4.x) + __popc(a4.y & ~x4.y) + __popc(a4.z & ~x4.z) +
+                   __popc(a4.w & ~x4.w);
+              if (dirty[q]) l += __popc(a4.x) + __popc(a4.y) + __popc(a4.z) + __popc(a4.w);
+            }
+            if (dirty[q]) {
+              l = __reduce_add_sync(0xFFFFFFFFu, l);
+            } else {
+              l = (warp % NW == 0) ? lit_cache[q] : 0u;
+            }
+            f = __reduce_add_sync(0xFFFFFFFFu, f);
+            if (lane == 0) {
+              const uint32_t at = (j + q) * 8 + (warp % NW) * 2;
+              slot_parts[at] = l;
+              slot_parts[at + 1] = f;
+              if constexpr (PAIR) {
+                peer_parts[(a & 1) * 64 + at] = l;
+                peer_parts[(a & 1) * 64 + at + 1] = f;
+              }
             }
           }
           unit_sync<PAIR>();
@@ -722,8 +734,11 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
           v = v > (int32_t)T ? (int32_t)T : v;
           v = v < -(int32_t)T ? -(int32_t)T : v;
           const uint64_t av = (uint64_t)(pa ? (int64_t)T - v : (int64_t)T + v);
-          lit_cache = __shfl_sync(0xFFFFFFFFu, Lq, j);
-          dirty = false;
+#pragma unroll
+          for (int q = 0; q < CPW; q++) {
+            lit_cache[q] = __shfl_sync(0xFFFFFFFFu, Lq, j + q);
+            dirty[q] = false;
+          }
           // feedback of this CTA's clauses (capi.c:226-242), lane c deciding
           // local clause c: draw 2p decides Type I of pair p, draw 2p+1 Type
           // II; the positive case gives Type I to the even clause.  Masks over
@@ -886,7 +901,9 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
             __syncthreads();
             pass = 0;
           }
-          if (all & (1u << lc)) dirty = true;
+#pragma unroll
+          for (int q = 0; q < CPW; q++)
+            if (all & (1u << (lc + q))) dirty[q] = true;
           // the next sample's evaluation reads clauses this step updated
           __syncthreads();
         }
@@ -1191,14 +1208,14 @@ cudaError_t launch_train_warp(const TrainDev *machines, const WorkItem *work, ui
   return cudaGetLastError();
 }
 
-template <bool S, bool P, int BM, bool EX = false>
+template <bool S, bool P, int BM, bool EX = false, int CPW = 1>
 static int occ_of(const TrainSmem &lay) {
-  cudaFuncSetAttribute(k_train<S, P, BM, EX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaFuncSetAttribute(k_train<S, P, BM, EX, CPW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        lay.total);
   if (!P) {
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_train<S, P, BM, EX>, TM_TRAIN_THREADS,
-                                                  lay.total);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_train<S, P, BM, EX, CPW>,
+                                                  TM_TRAIN_THREADS / CPW, lay.total);
     return nb;
   }
   cudaLaunchConfig_t cfg = {};
@@ -1217,22 +1234,36 @@ static int occ_of(const TrainSmem &lay) {
   return nc;
 }
 
+int train_threads(int mode, int cpw) {
+  return mode == TM_MODE_PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS / cpw;
+}
+
 // Single: co-resident CTAs per SM.  Pair: co-resident clusters per device.
-int train_occupancy(const TrainSmem &lay, int mode, uint32_t Bmin, uint32_t Bmax) {
+// cpw > 1 (clauses per warp) exists for 8 state bits only.
+int train_occupancy(const TrainSmem &lay, int mode, uint32_t Bmin, uint32_t Bmax, int cpw) {
   const bool small = Bmax <= 8, exact = Bmin == 8 && Bmax == 8;
+  if (cpw != 1 && (!exact || mode == TM_MODE_PAIR)) return 0;
   if (mode == TM_MODE_PAIR) return occ_of<true, true, 7>(lay);
-  if (mode == TM_MODE_SMEM)
-    return exact ? occ_of<true, false, 7, true>(lay)
-                 : (small ? occ_of<true, false, 7>(lay) : occ_of<true, false, 31>(lay));
-  return exact ? occ_of<false, false, 7, true>(lay)
-               : (small ? occ_of<false, false, 7>(lay) : occ_of<false, false, 31>(lay));
+  if (mode == TM_MODE_SMEM) {
+    if (exact)
+      return cpw == 4 ? occ_of<true, false, 7, true, 4>(lay)
+                      : (cpw == 2 ? occ_of<true, false, 7, true, 2>(lay)
+                                  : occ_of<true, false, 7, true>(lay));
+    return small ? occ_of<true, false, 7>(lay) : occ_of<true, false, 31>(lay);
+  }
+  if (exact)
+    return cpw == 4 ? occ_of<false, false, 7, true, 4>(lay)
+                    : (cpw == 2 ? occ_of<false, false, 7, true, 2>(lay)
+                                : occ_of<false, false, 7, true>(lay));
+  return small ? occ_of<false, false, 7>(lay) : occ_of<false, false, 31>(lay);
 }
 
 cudaError_t launch_train(const TrainDev *machines, const WorkItem *work, uint32_t nwork,
                          uint32_t *counter, uint32_t e_begin, uint32_t e_end, const TrainSmem &lay,
-                         int mode, uint32_t Bmin, uint32_t Bmax, int grid, uint32_t *err,
-                         cudaStream_t st) {
+                         int mode, uint32_t Bmin, uint32_t Bmax, int cpw, int grid,
+                         uint32_t *err, cudaStream_t st) {
   const bool small = Bmax <= 8, exact = Bmin == 8 && Bmax == 8;
+  if (cpw != 1 && (!exact || mode == TM_MODE_PAIR)) return cudaErrorInvalidValue;
   if (mode == TM_MODE_PAIR) {
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute at[1];
@@ -1249,18 +1280,21 @@ cudaError_t launch_train(const TrainDev *machines, const WorkItem *work, uint32_
     return cudaLaunchKernelEx(&cfg, k_train<true, true, 7>, machines, work, nwork, counter,
                               e_begin, e_end, lay, err);
   }
-#define TM_LAUNCH(S, BM, EX)                                                                  \
-  k_train<S, false, BM, EX><<<grid, TM_TRAIN_THREADS, lay.total, st>>>(machines, work, nwork,     \
-                                                                       counter, e_begin, e_end, \
-                                                                       lay, err)
+#define TM_LAUNCH(S, BM, EX, CW)                                                             \
+  k_train<S, false, BM, EX, CW><<<grid, TM_TRAIN_THREADS / CW, lay.total, st>>>(            \
+      machines, work, nwork, counter, e_begin, e_end, lay, err)
   if (mode == TM_MODE_SMEM) {
-    if (exact) TM_LAUNCH(true, 7, true);
-    else if (small) TM_LAUNCH(true, 7, false);
-    else TM_LAUNCH(true, 31, false);
+    if (exact && cpw == 4) TM_LAUNCH(true, 7, true, 4);
+    else if (exact && cpw == 2) TM_LAUNCH(true, 7, true, 2);
+    else if (exact) TM_LAUNCH(true, 7, true, 1);
+    else if (small) TM_LAUNCH(true, 7, false, 1);
+    else TM_LAUNCH(true, 31, false, 1);
   } else {
-    if (exact) TM_LAUNCH(false, 7, true);
-    else if (small) TM_LAUNCH(false, 7, false);
-    else TM_LAUNCH(false, 31, false);
+    if (exact && cpw == 4) TM_LAUNCH(false, 7, true, 4);
+    else if (exact && cpw == 2) TM_LAUNCH(false, 7, true, 2);
+    else if (exact) TM_LAUNCH(false, 7, true, 1);
+    else if (small) TM_LAUNCH(false, 7, false, 1);
+    else TM_LAUNCH(false, 31, false, 1);
   }
 #undef TM_LAUNCH
   return cudaGetLastError();

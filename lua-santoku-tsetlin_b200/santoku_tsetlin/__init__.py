@@ -106,6 +106,7 @@ class Stats(ctypes.Structure):
         ("train_unit_steps", ctypes.c_uint64),
         ("train_mode", ctypes.c_int32),
         ("train_autotuned", ctypes.c_int32),
+        ("train_cpw", ctypes.c_int32),
     ]
 
     def as_dict(self):
@@ -130,7 +131,7 @@ EXPORTS = (
     "tm_checkpoint", "tm_restore", "tm_reconfigure", "tm_restrict", "tm_type",
     "tm_destroy", "tm_last_error", "tm_align", "tm_get_info", "tm_export_state",
     "tm_import_state", "tm_class_accuracy", "tm_encoding_accuracy", "tm_bits_to_cvec", "tm_bits_to_cvec_ind",
-    "tm_predict_noalloc", "tm_int_peaks", "tm_set_autotune", "tm_stats_enable", "tm_get_stats", "tm_reset_stats", "tm_serve_open", "tm_serve_submit", "tm_serve_poll",
+    "tm_predict_noalloc", "tm_int_peaks", "tm_set_autotune", "tm_force_variant", "tm_stats_enable", "tm_get_stats", "tm_reset_stats", "tm_serve_open", "tm_serve_submit", "tm_serve_poll",
     "tm_serve_latency_us", "tm_serve_close",
 )
 
@@ -174,6 +175,7 @@ def lib():
     L.tm_predict_noalloc.argtypes = [vp, vp, u64, vp, vp]
     L.tm_int_peaks.argtypes = [i32, vp]
     L.tm_set_autotune.argtypes = [vp, i32]
+    L.tm_force_variant.argtypes = [vp, i32, i32]
     L.tm_class_accuracy.argtypes = [vp, vp, u64, u32, i32, i32, vp]
     L.tm_encoding_accuracy.argtypes = [vp, vp, u64, u32, i32, i32, vp]
     L.tm_bits_to_cvec.argtypes = [vp, u64, u64, u32, i32, i32, i32, vp]
@@ -452,6 +454,12 @@ class Machine:
         shape (default), 2 tuned on every train call.  Results are the same
         in every mode."""
         _check(lib().tm_set_autotune(self.handle, int(mode)))
+
+    def force_variant(self, mode=-1, cpw=1):
+        """Pin the train-kernel variant (0 shared planes, 1 global planes,
+        2 cluster pair, 3 warp per unit; cpw clauses per warp); -1 returns
+        to the automatic choice."""
+        _check(lib().tm_force_variant(self.handle, int(mode), int(cpw)))
 
     def stats(self):
         st = Stats()

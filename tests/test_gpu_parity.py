@@ -428,3 +428,42 @@ def test_global_planes_chosen_by_occupancy(tm, monkeypatch):
     a, st = t.export_state()
     assert np.array_equal(a, m.actions())
     assert np.array_equal(st, m.state())
+
+
+@pytest.mark.parametrize("features", [784, 4500])
+def test_every_train_variant_matches_oracle(tm, features):
+    """Each train-kernel variant, pinned in turn -- one warp per unit, shared
+    or global count planes with 1, 2 or 4 clauses per warp, the 2-CTA
+    cluster -- ends in the oracle's state, bit for bit."""
+    from santoku_tsetlin import datagen
+    rng = np.random.default_rng(features + 7)
+    n, classes = 200, 4
+    x = datagen.flip_pack(rng.random((n, features)) < 0.03).ravel()
+    y = rng.integers(0, classes, size=n).astype(np.int64)
+    cfg = dict(type="classifier", classes=classes, features=features, clauses=32,
+               clause_tolerance=16, clause_maximum=120, specificity=12.0, target=16)
+    inp = dict(n=n, x=x, labels=y)
+    m = _oracle_pair("classifier", cfg, inp, 2, seed=31)
+    want = (m.actions(), m.state())
+    variants = [(0, 1), (0, 2), (0, 4), (1, 1), (1, 2), (1, 4), (2, 1)]
+    if features <= 1024:
+        variants.append((3, 1))
+    kind, tbl = ref_table(cfg, seed=31)
+    for mode, cpw in variants:
+        t = tm.create(kind, tbl)
+        t.force_variant(mode, cpw)
+        t.stats_enable(True)
+        t.train(train_table(kind, inp, 2))
+        st = t.stats()
+        assert (st["train_mode"], st["train_cpw"]) == (mode, cpw)
+        a, s = t.export_state()
+        assert np.array_equal(a, want[0]), (mode, cpw)
+        assert np.array_equal(s, want[1]), (mode, cpw)
+        t.destroy()
+    t = tm.create(kind, tbl)
+    t.force_variant(3, 2)
+    with pytest.raises(tm.TsetlinError):
+        t.force_variant(1, 3)
+    with pytest.raises(tm.TsetlinError):  # the warp kernel has one clause layout
+        t.train(train_table(kind, inp, 1))
+    t.destroy()
