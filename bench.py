@@ -384,12 +384,12 @@ def run_ours(args, w):
     }
     if rank == 0:
         # integer-pipe roofline of clause evaluation (after the timed region):
-        # per 32 words k_predict's inner loop issues 68 logic ops (6 carry-save
-        # steps of 4 AND-NOT + 6 LOP3, 2 direct steps of 4 AND-NOT) and 14
-        # POPC (6 + 8); POPC and the logic ops issue on separate pipes
+        # per 32 words k_predict's inner loop issues 62 logic ops (5 carry-save
+        # steps of 4 AND-NOT + 6 LOP3, 3 direct steps of 4 AND-NOT) and 17
+        # POPC (5 + 12); POPC and the logic ops issue on separate pipes
         pk = tm.int_peaks(dev.index if dev.index is not None else 0)
         wops = out["kernels"]["predict_literal_evals_per_s"] / 32
-        bound = min(32 * pk["lop3"] / 68, 32 * pk["popc"] / 14)
+        bound = min(32 * pk["lop3"] / 62, 32 * pk["popc"] / 17)
         out["kernels"].update({"int_peaks_ops_per_s": pk, "predict_word_ops_per_s": wops,
                                "predict_int_bound_word_ops_per_s": bound,
                                "predict_frac_of_int_bound": wops / bound})

@@ -1337,26 +1337,43 @@ cudaError_t launch_lits(const uint32_t *act, const ClassDev *cls, uint32_t class
 // ---------------------------------------------------------------------------
 constexpr int PT_S = 64, PT_C = 64, PT_K = 32, PT_LD = PT_K + 4;
 
+// 16-byte asynchronous global -> shared copy; `valid` false zero-fills the
+// destination without reading the source.
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, bool valid) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src),
+               "r"(valid ? 16 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 __global__ void __launch_bounds__(256, 2)
     k_predict(const uint32_t *__restrict__ act, const int32_t *__restrict__ lits,
               const ClassDev *__restrict__ cls, uint32_t clauses, uint32_t tiles_per_class,
               uint32_t tol, const uint32_t *__restrict__ x, uint32_t n, uint32_t classes,
               int32_t *__restrict__ sums) {
-  __shared__ __align__(16) uint32_t As[PT_C * PT_LD];
-  __shared__ __align__(16) uint32_t Xs[PT_S * PT_LD];
+  // two buffers: the next 32-word chunk streams in while this one is used
+  __shared__ __align__(16) uint32_t As[2][PT_C * PT_LD];
+  __shared__ __align__(16) uint32_t Xs[2][PT_S * PT_LD];
   __shared__ int32_t red[16][PT_S + 1];
   const uint32_t h = blockIdx.y / tiles_per_class;
   const uint32_t c0 = (blockIdx.y % tiles_per_class) * PT_C;
   const uint32_t s0 = blockIdx.x * PT_S;
   const ClassDev C = cls[h];
   const uint32_t tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  // Failed-literal counts popc(a & ~x) per (clause, sample).  Six of every
+  // Failed-literal counts popc(a & ~x) per (clause, sample).  Five of every
   // eight 4-word steps go through carry-save adders: `ones` and `twos` hold
   // bit-sliced partial counts and only the weight-4 carries are popcounted
-  // (one POPC per four words, ten logic ops); the other two steps popcount
-  // their words directly (four POPC, four logic ops).  POPC and the logic
-  // ops issue on separate pipes (measured on B200: they overlap fully), and
-  // this mix keeps both busy.  acc is the exact count of everything
+  // (one POPC per four words, ten logic ops); the other three steps
+  // popcount their words directly (four POPC, four logic ops, two 3-input
+  // adds).  POPC and the logic ops issue on separate pipes (measured on
+  // B200: they overlap fully), and this mix balances them.  acc is the exact count of everything
   // already reduced: count = acc + 2 * popc(twos) + popc(ones).
   uint32_t acc[4][4], ones[4][4], twos[4][4];
 #pragma unroll
@@ -1365,43 +1382,50 @@ __global__ void __launch_bounds__(256, 2)
     for (int b = 0; b < 4; b++) acc[a][b] = ones[a][b] = twos[a][b] = 0;
   const uint32_t *arow = act + C.act_off;
   const uint32_t *xrow = x + C.x_off;
-  for (uint32_t k0 = 0; k0 < C.Wp; k0 += PT_K) {
+  auto stage = [&](uint32_t k0, int buf) {
 #pragma unroll
     for (int v = 0; v < 2; v++) {
       const uint32_t idx = tid + 256 * v, r = idx >> 3, c4 = (idx & 7) * 4;
       const uint32_t kw = k0 + c4;
-      uint4 av = make_uint4(0, 0, 0, 0), xv = make_uint4(0, 0, 0, 0);
-      if (c0 + r < clauses && kw < C.Wp) {
-        av = *(const uint4 *)(arow + (uint64_t)(c0 + r) * C.Wp + kw);
-        // evaluation mask on the last word (capi.c:104-106)
-        if (kw <= C.W - 1 && C.W - 1 < kw + 4) {
-          const uint32_t q = C.W - 1 - kw;
-          if (q == 0) av.x &= C.emask;
-          if (q == 1) av.y &= C.emask;
-          if (q == 2) av.z &= C.emask;
-          if (q == 3) av.w &= C.emask;
-        }
-      }
-      if (s0 + r < n && kw < C.Wp) xv = *(const uint4 *)(xrow + (uint64_t)(s0 + r) * C.Wp + kw);
-      *(uint4 *)(As + r * PT_LD + c4) = av;
-      *(uint4 *)(Xs + r * PT_LD + c4) = xv;
+      const bool va = c0 + r < clauses && kw < C.Wp, vx = s0 + r < n && kw < C.Wp;
+      cp_async16(&As[buf][r * PT_LD + c4], va ? arow + (uint64_t)(c0 + r) * C.Wp + kw : arow, va);
+      cp_async16(&Xs[buf][r * PT_LD + c4], vx ? xrow + (uint64_t)(s0 + r) * C.Wp + kw : xrow, vx);
+    }
+    cp_async_commit();
+  };
+  const uint32_t nch = (C.Wp + PT_K - 1) / PT_K;
+  stage(0, 0);
+  for (uint32_t ch = 0; ch < nch; ch++) {
+    const uint32_t k0 = ch * PT_K;
+    const int buf = ch & 1;
+    if (ch + 1 < nch) {
+      stage(k0 + PT_K, buf ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
     __syncthreads();
+    if (k0 <= C.W - 1 && C.W - 1 < k0 + PT_K) {
+      // evaluation mask on the last word (capi.c:104-106)
+      if (tid < PT_C) As[buf][tid * PT_LD + (C.W - 1 - k0)] &= C.emask;
+      __syncthreads();
+    }
+    const uint32_t *Ab = As[buf], *Xb = Xs[buf];
 #pragma unroll
     for (int kk = 0; kk < PT_K; kk += 4) {
       uint4 a4[4], x4[4];
 #pragma unroll
-      for (int c = 0; c < 4; c++) a4[c] = *(const uint4 *)(As + (ty + 16 * c) * PT_LD + kk);
+      for (int c = 0; c < 4; c++) a4[c] = *(const uint4 *)(Ab + (ty + 16 * c) * PT_LD + kk);
 #pragma unroll
-      for (int i = 0; i < 4; i++) x4[i] = *(const uint4 *)(Xs + (tx + 16 * i) * PT_LD + kk);
+      for (int i = 0; i < 4; i++) x4[i] = *(const uint4 *)(Xb + (tx + 16 * i) * PT_LD + kk);
 #pragma unroll
       for (int c = 0; c < 4; c++)
 #pragma unroll
         for (int i = 0; i < 4; i++) {
           const uint32_t t0 = a4[c].x & ~x4[i].x, t1 = a4[c].y & ~x4[i].y;
           const uint32_t t2 = a4[c].z & ~x4[i].z, t3 = a4[c].w & ~x4[i].w;
-          if ((kk & 12) == 12) {
-            // steps 3 and 7 of 8: direct popcounts
+          if (kk == 8 || kk == 20 || kk == 28) {
+            // steps 2, 5 and 7 of 8: direct popcounts
             acc[c][i] += __popc(t0) + __popc(t1) + __popc(t2) + __popc(t3);
           } else {
             uint32_t o = ones[c][i];
