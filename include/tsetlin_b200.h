@@ -80,6 +80,13 @@ typedef struct tm_train_args {
   int32_t on_device;           /* problems/solutions/codes are device pointers */
   int32_t has_seed;            /* 1: use `seed` instead of the machine's */
   uint64_t seed;
+  /* Train only the units of classes [class_begin, class_end) (0, 0: all).
+   * Units are independent and every draw is keyed, so ranks that each train
+   * a class range and then exchange those classes' automata hold exactly
+   * the single-GPU result (the multi-GPU split of one machine).  No
+   * counterpart in the reference. */
+  uint32_t class_begin;
+  uint32_t class_end;
 } tm_train_args;
 
 /* Reconfigure arguments (capi.c:1590-1673). */

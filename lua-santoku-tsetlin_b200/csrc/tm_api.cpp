@@ -477,6 +477,9 @@ static int max_smem_optin(int dev) {
 
 static int validate_train(tm_machine *m, const tm_train_args *a) {
   if (!m || !a) return fail(TM_ERR_ARG, "null argument");
+  if (a->class_end && (a->class_begin >= a->class_end || a->class_end > m->classes))
+    return fail(TM_ERR_ARG, "train: class range [%u, %u) outside [0, %u)", a->class_begin,
+                a->class_end, m->classes);
   if (!m->has_state || !m->d_cnt)
     return fail(TM_ERR_STATE, "can't train a model loaded without state");
   if (a->samples >= (1ull << 31)) return fail(TM_ERR_ARG, "train: too many samples");
@@ -754,7 +757,9 @@ static int run_epochs(std::vector<TrainJob> &jobs, uint32_t e0, uint32_t e1, tm_
     t.epochs = std::min<uint32_t>(J.a->iterations, e1);
     t.epoch_base = 0;
     if (t.n == 0 || t.epochs <= e0) continue;
-    for (uint32_t h = 0; h < m->classes; h++) {
+    const uint32_t hb = J.a->class_end ? J.a->class_begin : 0;
+    const uint32_t he = J.a->class_end ? std::min(J.a->class_end, m->classes) : m->classes;
+    for (uint32_t h = hb; h < he; h++) {
       const ClassDev &c = J.cls[h];
       Wpmax = std::max(Wpmax, c.Wp);
       smax = std::max(smax, c.s_picks);
@@ -803,7 +808,10 @@ static int run_epochs(std::vector<TrainJob> &jobs, uint32_t e0, uint32_t e1, tm_
   if (rc) return rc;
   m0->stats.train_launches++;
   for (auto &J : jobs)
-    m0->stats.train_unit_steps += (uint64_t)J.m->classes * J.m->clause_chunks * J.a->samples *
+    m0->stats.train_unit_steps += (uint64_t)(J.a->class_end ? std::min(J.a->class_end, J.m->classes) -
+                                                                  J.a->class_begin
+                                                            : J.m->classes) *
+                                  J.m->clause_chunks * J.a->samples *
                                   (std::min<uint32_t>(J.a->iterations, e1) > e0
                                        ? std::min<uint32_t>(J.a->iterations, e1) - e0 : 0);
   if (m0->timing) m0->stats.train_kernel_ms += ms;

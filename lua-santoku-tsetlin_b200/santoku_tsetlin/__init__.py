@@ -82,6 +82,8 @@ class _TrainArgs(ctypes.Structure):
         ("on_device", ctypes.c_int32),
         ("has_seed", ctypes.c_int32),
         ("seed", ctypes.c_uint64),
+        ("class_begin", ctypes.c_uint32),
+        ("class_end", ctypes.c_uint32),
     ]
 
 
@@ -313,6 +315,9 @@ class Machine:
         if "seed" in tbl and tbl["seed"] is not None:
             a.has_seed = 1
             a.seed = int(tbl["seed"])
+        if tbl.get("class_range") is not None:
+            # train only these classes' units (multi.train_sharded)
+            a.class_begin, a.class_end = (int(v) for v in tbl["class_range"])
         return a, (prob, sol, cod, dof)
 
     def train(self, tbl):

@@ -5,6 +5,10 @@ data-path collective:
 
 * training: machines (search trials) or replicas are partitioned across
   ranks by cost (`partition_lpt`); nothing is exchanged while they train;
+* training one machine on several GPUs: each rank trains a contiguous class
+  range (its units; every draw is keyed, so the units do not depend on
+  each other) and the ranks then all-gather those classes' automata, after
+  which every rank holds exactly the single-GPU result -- `train_sharded`;
 * predict of one machine too large for a GPU: each rank holds a contiguous
   range of classes and computes their per-class vote sums
   (`Machine.predict_scores`); one all-gather of those sums, then the
@@ -76,3 +80,48 @@ def gather_predict(local_scores, classes, kind="classifier", group=None, device=
         return np.argmax(full, axis=1).astype(np.int64), full
     bits = full > 0
     return np.packbits(bits, axis=1, bitorder="little").ravel(), full
+
+
+def train_sharded(machine, tbl, group=None, device=None):
+    """Train one machine across the ranks of `group`: rank r trains the
+    units of its class range (`class_range`) -- nothing is exchanged while
+    training -- then one all-gather of each range's action and count-plane
+    bytes (the reference's per-class byte blocks, contiguous for a dense
+    machine) leaves the full trained machine on every rank, bit-identical to
+    training it on one GPU.  `device`: where the exchanged tensors live (a
+    CUDA device for NCCL, None for gloo)."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group) if dist.is_initialized() else 1
+    rank = dist.get_rank(group) if dist.is_initialized() else 0
+    info = machine.info()
+    if info["individualized"]:
+        raise ValueError("train_sharded: individualized machines have uneven class blocks")
+    classes = info["classes"]
+    lo, hi = class_range(classes, world, rank)
+    t = dict(tbl)
+    t["class_range"] = (lo, hi)
+    machine.train(t)
+    if world == 1:
+        return machine
+    acts, state = machine.export_state()
+    pa = len(acts) // classes
+    ps = 0 if state is None else len(state) // classes
+    ranges = [class_range(classes, world, r) for r in range(world)]
+    width = max(h - l for l, h in ranges)
+    mine = np.zeros(width * (pa + ps), dtype=np.uint8)
+    mine[:(hi - lo) * pa] = acts[lo * pa:hi * pa]
+    if ps:
+        mine[width * pa:width * pa + (hi - lo) * ps] = state[lo * ps:hi * ps]
+    local = torch.from_numpy(mine)
+    if device is not None:
+        local = local.to(device)
+    parts = [torch.empty_like(local) for _ in range(world)]
+    dist.all_gather(parts, local, group=group)
+    for (l, h), part in zip(ranges, parts):
+        b = part.cpu().numpy()
+        acts[l * pa:h * pa] = b[:(h - l) * pa]
+        if ps:
+            state[l * ps:h * ps] = b[width * pa:width * pa + (h - l) * ps]
+    machine.import_state(acts, state)
+    return machine
