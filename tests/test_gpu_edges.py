@@ -2,7 +2,8 @@
 (bit-exact state, vote sums and outputs): the smallest machine (one class,
 one feature, 2-bit automata), include_bits equal to state_bits, a tolerance
 of 1 and one far above the literal count, an encoder whose hidden width is
-not a multiple of 8 (padding bits of the last code byte), empty
+not a multiple of 8 (the reference leaves the padding bits of the last code
+byte stale, capi.c:957-990, so codes are compared within `hidden`), empty
 predicts, and a predict larger than one tile row in every dimension."""
 import os
 import sys
