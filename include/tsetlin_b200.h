@@ -292,7 +292,9 @@ int tm_set_autotune(tm_machine *m, int32_t mode);
  * clauses evaluated per warp in a single-CTA variant with 8 state bits: 1,
  * 2 or 4 -- 256 / cpw threads per unit); mode -1 returns to the automatic
  * choice.  A train call that the pinned variant cannot run fails with
- * TM_ERR_ARG.  For tests and measurements; no counterpart in the reference. */
+ * TM_ERR_ARG.  The environment variable TSETLIN_B200_VARIANT=mode:cpw, read
+ * when a machine is created, pins the same way.  For tests and
+ * measurements; no counterpart in the reference. */
 int tm_force_variant(tm_machine *m, int32_t mode, int32_t cpw);
 
 /* on != 0 starts timing (events around every train / predict kernel). */

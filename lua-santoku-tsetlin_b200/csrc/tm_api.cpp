@@ -262,6 +262,15 @@ extern "C" int tm_create(const tm_params *p, tm_machine **out) {
     m->no_warp = w && w[0] == '1';
     const char *t = getenv("TSETLIN_B200_AUTOTUNE");
     m->autotune = t && t[0] >= '0' && t[0] <= '2' ? t[0] - '0' : 1;
+    // TSETLIN_B200_VARIANT=mode:cpw pins the train-kernel variant, as
+    // tm_force_variant does (for measurements from the command line)
+    const char *v = getenv("TSETLIN_B200_VARIANT");
+    int vm = -1, vc = 1;
+    if (v && sscanf(v, "%d:%d", &vm, &vc) >= 1 && vm >= 0 && vm <= TM_MODE_WARP &&
+        (vc == 1 || vc == 2 || vc == 4)) {
+      m->force_mode = vm;
+      m->force_cpw = vc;
+    }
   }
   if (m->individualized) {
     // capi.c:528-606 leaves features, input_bits, input_chunks and tail_mask
