@@ -88,3 +88,84 @@ def test_partition_and_ranges():
         lo, hi = multi.class_range(10, 3, r)
         covered += list(range(lo, hi))
     assert covered == list(range(10))
+
+
+class _OracleRangeMachine:
+    """Stand-in for a device machine in `multi.train_sharded` (test
+    infrastructure): training a class range is the oracle's full training
+    with every class outside the range put back to its initial state --
+    units are independent, so that is what class-range training leaves."""
+
+    def __init__(self, O, cfg, x, lab, n):
+        self.m = O.Machine(**cfg)
+        self.x, self.lab, self.n = x, lab, n
+        self.a0, self.s0 = self.m.actions(), self.m.state()
+
+    def info(self):
+        return dict(self.m.info)
+
+    def train(self, tbl):
+        lo, hi = tbl["class_range"]
+        self.m.train(self.x, self.n, tbl["iterations"], labels=self.lab, seed=5)
+        a, s = self.m.actions(), self.m.state()
+        C = self.m.info["classes"]
+        pa, ps = len(a) // C, len(s) // C
+        for h in range(C):
+            if not lo <= h < hi:
+                a[h * pa:(h + 1) * pa] = self.a0[h * pa:(h + 1) * pa]
+                s[h * ps:(h + 1) * ps] = self.s0[h * ps:(h + 1) * ps]
+        self.m.load_state(a, s)
+
+    def export_state(self):
+        return self.m.actions(), self.m.state()
+
+    def import_state(self, a, s):
+        self.m.load_state(a, s)
+
+
+def _sharded_worker(rank, world, port, out):
+    import sys
+    import torch.distributed as dist
+    here = os.path.dirname(os.path.abspath(__file__))
+    root = os.path.dirname(here)
+    sys.path.insert(0, os.path.join(root, "lua-santoku-tsetlin_b200"))
+    sys.path.insert(0, os.path.join(root, "oracle"))
+    import oracle as O
+    from santoku_tsetlin import multi
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        rng = np.random.default_rng(8)
+        F, n, classes = 30, 50, 5
+        cfg = dict(type="classifier", classes=classes, features=F, clauses=16,
+                   clause_tolerance=6, clause_maximum=12, specificity=4.0)
+        b = rng.random((n, F)) < 0.3
+        x = np.packbits(np.concatenate([b, ~b], axis=1), axis=1, bitorder="little").ravel()
+        lab = rng.integers(0, classes, size=n).astype(np.int64)
+        sm = _OracleRangeMachine(O, cfg, x, lab, n)
+        multi.train_sharded(sm, dict(iterations=2))
+        full = O.Machine(**cfg)
+        full.train(x, n, 2, labels=lab, seed=5)
+        a, s = sm.export_state()
+        out[rank] = (np.array_equal(a, full.actions()), np.array_equal(s, full.state()))
+    finally:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def test_train_sharded_gathers_every_class(oracle_lib):
+    """World size 2 over gloo: each rank holds every class's automata after
+    `train_sharded`, equal to one process training the whole machine."""
+    world = 2
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    out = ctx.Manager().dict()
+    procs = [ctx.Process(target=_sharded_worker, args=(r, world, port, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=240)
+        assert p.exitcode == 0
+    for r in range(world):
+        assert out[r] == (True, True)
