@@ -663,39 +663,47 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
           // (capi.c:97-122).  L only changes when the clause is updated, so
           // it is recounted only after feedback to the clause (`dirty`).
           uint32_t *slot_parts = parts + (a & 1) * 64;
+          {
+            // each word of the sample row is loaded once for all CPW clauses
+            uint32_t l[CPW], f[CPW];
 #pragma unroll
-          for (int q = 0; q < CPW; q++) {
-            const uint32_t *act_q = act_j + q * Wp;
-            uint32_t l = 0, f = 0;
+            for (int q = 0; q < CPW; q++) l[q] = f[q] = 0;
             const uint32_t Q = Wp >> 2, qlast = (W - 1) >> 2;
 #pragma unroll 4
             for (uint32_t qi = gl; qi < Q; qi += GS) {
-              uint4 a4 = *(const uint4 *)(act_q + 4 * qi);
               const uint4 x4 = *(const uint4 *)(xr + 4 * qi);
-              if (qi == qlast) {  // evaluation mask on word W-1 (capi.c:104-106)
-                const uint32_t k = (W - 1) & 3;
-                if (k == 0) a4.x &= C.emask;
-                if (k == 1) a4.y &= C.emask;
-                if (k == 2) a4.z &= C.emask;
-                if (k == 3) a4.w &= C.emask;
+#pragma unroll
+              for (int q = 0; q < CPW; q++) {
+                uint4 a4 = *(const uint4 *)(act_j + q * Wp + 4 * qi);
+                if (qi == qlast) {  // evaluation mask on word W-1 (capi.c:104-106)
+                  const uint32_t k = (W - 1) & 3;
+                  if (k == 0) a4.x &= C.emask;
+                  if (k == 1) a4.y &= C.emask;
+                  if (k == 2) a4.z &= C.emask;
+                  if (k == 3) a4.w &= C.emask;
+                }
+                f[q] += __popc(a4.x & ~x4.x) + __popc(a4.y & ~x4.y) + __popc(a4.z & ~x4.z) +
+                        __popc(a4.w & ~x4.w);
+                if (dirty[q]) l[q] += __popc(a4.x) + __popc(a4.y) + __popc(a4.z) + __popc(a4.w);
               }
-              f += __popc(a4.x & ~x4.x) + __popc(a4.y & ~x4.y) + __popc(a4.z & ~x4.z) +
-                   __popc(a4.w & ~x4.w);
-              if (dirty[q]) l += __popc(a4.x) + __popc(a4.y) + __popc(a4.z) + __popc(a4.w);
             }
-            if (dirty[q]) {
-              l = __reduce_add_sync(0xFFFFFFFFu, l);
-            } else {
-              l = (warp % NW == 0) ? lit_cache[q] : 0u;
-            }
-            f = __reduce_add_sync(0xFFFFFFFFu, f);
-            if (lane == 0) {
-              const uint32_t at = (j + q) * 8 + (warp % NW) * 2;
-              slot_parts[at] = l;
-              slot_parts[at + 1] = f;
-              if constexpr (PAIR) {
-                peer_parts[(a & 1) * 64 + at] = l;
-                peer_parts[(a & 1) * 64 + at + 1] = f;
+#pragma unroll
+            for (int q = 0; q < CPW; q++) {
+              uint32_t lq;
+              if (dirty[q]) {
+                lq = __reduce_add_sync(0xFFFFFFFFu, l[q]);
+              } else {
+                lq = (warp % NW == 0) ? lit_cache[q] : 0u;
+              }
+              const uint32_t fq = __reduce_add_sync(0xFFFFFFFFu, f[q]);
+              if (lane == 0) {
+                const uint32_t at = (j + q) * 8 + (warp % NW) * 2;
+                slot_parts[at] = lq;
+                slot_parts[at + 1] = fq;
+                if constexpr (PAIR) {
+                  peer_parts[(a & 1) * 64 + at] = lq;
+                  peer_parts[(a & 1) * 64 + at + 1] = fq;
+                }
               }
             }
           }
@@ -829,7 +837,7 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
                     *(uint2 *)(l0 + w0) = make_uint2(0, 0);
                     *(uint2 *)(l0 + lay.ib_words + w0) = make_uint2(0, 0);
                     ld_pair<BM>(act_c, cnt_c, Wp, m, w0, pq, aq);
-  #pragma unroll
+#pragma unroll
                     for (int k = 0; k < 2; k++) {
                       const uint32_t am = word_mask(w0 + k, W, C.amask);
                       rg_sub_pow2<BM>(pq[k], aq[k], m, 0, k ? m0.y : m0.x, am);
@@ -846,7 +854,7 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
                   const bool need = (t1 && incx) || ((~x2.x & vm0) | (~x2.y & vm1)) != 0;
                   if (need) {
                     ld_pair<BM>(act_c, cnt_c, Wp, m, w0, pq, aq);
-  #pragma unroll
+#pragma unroll
                     for (int k = 0; k < 2; k++) {
                       const uint32_t x = k ? x2.y : x2.x, vm = k ? vm1 : vm0;
                       const uint32_t am = word_mask(w0 + k, W, C.amask);
