@@ -202,6 +202,18 @@ int tm_get_info(const tm_machine *m, uint64_t *out);
 int tm_export_state(tm_machine *m, uint8_t *actions, uint8_t *state);
 int tm_import_state(tm_machine *m, const uint8_t *actions, const uint8_t *state);
 
+/* The slice of tm_export_state's two buffers that classes [class_begin,
+ * class_end) occupy (their clause rows, in the same byte layout), copied
+ * out of or into the machine.  `on_device` = 1: actions / state are device
+ * pointers on the machine's device and the copies stay on the device.  The
+ * unit of the multi-GPU exchange after a class-sharded training (each rank
+ * trains a class range, then all ranks all-gather these slices device to
+ * device).  No counterpart in the reference. */
+int tm_export_classes(tm_machine *m, uint32_t class_begin, uint32_t class_end, uint8_t *actions,
+                      uint8_t *state, int32_t on_device);
+int tm_import_classes(tm_machine *m, uint32_t class_begin, uint32_t class_end,
+                      const uint8_t *actions, const uint8_t *state, int32_t on_device);
+
 /* ---- evaluator metrics and input packing (device) --------------------- */
 /* evaluator.class_accuracy(predicted, expected, n_samples, n_classes):
  * evaluator/capi.c:119-202.  out[3 + 3 * n_classes] = macro precision,
@@ -296,6 +308,13 @@ int tm_set_autotune(tm_machine *m, int32_t mode);
  * when a machine is created, pins the same way.  For tests and
  * measurements; no counterpart in the reference. */
 int tm_force_variant(tm_machine *m, int32_t mode, int32_t cpw);
+
+/* Failure injection for tests of the error paths: after `after` more
+ * successful device allocations, the next one the library makes fails as if
+ * the GPU were out of memory (the call reports TM_ERR_OOM); then the
+ * injection disarms itself.  after < 0 disarms it.  No counterpart in the
+ * reference. */
+int tm_debug_fail_alloc(int64_t after);
 
 /* on != 0 starts timing (events around every train / predict kernel). */
 int tm_stats_enable(tm_machine *m, int32_t on);

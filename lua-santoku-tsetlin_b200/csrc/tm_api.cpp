@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <map>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -38,8 +39,31 @@ static int fail(int code, const char *fmt, ...) {
   do {                                                                                \
     cudaError_t e_ = (call);                                                          \
     if (e_ != cudaSuccess)                                                            \
-      return fail(TM_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));      \
+      return fail(e_ == cudaErrorMemoryAllocation ? TM_ERR_OOM : TM_ERR_CUDA,         \
+                  "%s failed: %s", #call, cudaGetErrorString(e_));                    \
   } while (0)
+
+// Every device allocation of the library goes through here.  A failure
+// injected by tm_debug_fail_alloc makes the chosen allocation report
+// cudaErrorMemoryAllocation without calling cudaMalloc, so the error paths
+// of create / train / predict can be tested without exhausting a GPU.
+static std::atomic<int64_t> g_fail_alloc{-1};
+
+cudaError_t tmb_dev_malloc(void **p, size_t n) {
+  int64_t c = g_fail_alloc.load();
+  while (c >= 0 && !g_fail_alloc.compare_exchange_weak(c, c - 1)) {
+  }
+  if (c == 0) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMalloc(p, n);
+}
+
+extern "C" int tm_debug_fail_alloc(int64_t after) {
+  g_fail_alloc.store(after < 0 ? -1 : after);
+  return TM_OK;
+}
 
 extern "C" const char *tm_last_error(void) { return g_err.c_str(); }
 extern "C" uint32_t tm_align(void) { return 8; }
@@ -68,7 +92,7 @@ struct DevBuf {
     p = nullptr;
     cap = 0;
     size_t want = n < 256 ? 256 : n;
-    cudaError_t e = cudaMalloc(&p, want);
+    cudaError_t e = tmb_dev_malloc(&p, want);
     if (e == cudaSuccess) cap = want;
     return e;
   }
@@ -107,6 +131,8 @@ struct tm_machine {
   bool pair = false;      // TSETLIN_B200_PAIR=1: split units too large for one SM over a
                           // 2-CTA cluster instead of keeping their automata in global memory
   bool no_warp = false;   // TSETLIN_B200_NO_WARP=1: never train a unit with one warp
+  uint32_t row_wait = TM_WAIT_LIMIT;  // TSETLIN_B200_ROW_WAIT: try-wait iterations per
+                                      // sample row (tests shorten it to see TM_ERR_DEVICE)
   int force_mode = -1;    // >= 0: train with this variant (tm_force_variant)
   int force_cpw = 1;
   int autotune = 1;       // 0 heuristic variant choice, 1 tuned (cached per shape),
@@ -188,16 +214,16 @@ static void free_device(tm_machine *m) {
 
 static int alloc_device(tm_machine *m, bool with_state) {
   free_device(m);
-  CK(cudaMalloc(&m->d_act, std::max<uint64_t>(m->act_words, 4) * 4));
+  CK(tmb_dev_malloc((void **)&m->d_act, std::max<uint64_t>(m->act_words, 4) * 4));
   CK(cudaMemsetAsync(m->d_act, 0, std::max<uint64_t>(m->act_words, 4) * 4, m->st));
   if (with_state) {
-    CK(cudaMalloc(&m->d_cnt, std::max<uint64_t>(m->cnt_words, 4) * 4));
+    CK(tmb_dev_malloc((void **)&m->d_cnt, std::max<uint64_t>(m->cnt_words, 4) * 4));
     CK(cudaMemsetAsync(m->d_cnt, 0, std::max<uint64_t>(m->cnt_words, 4) * 4, m->st));
   }
-  CK(cudaMalloc(&m->d_cls, std::max<size_t>(m->classes, 1) * sizeof(ClassDev)));
+  CK(tmb_dev_malloc((void **)&m->d_cls, std::max<size_t>(m->classes, 1) * sizeof(ClassDev)));
   CK(cudaMemcpyAsync(m->d_cls, m->cls.data(), m->classes * sizeof(ClassDev),
                      cudaMemcpyHostToDevice, m->st));
-  CK(cudaMalloc(&m->d_lits, std::max<uint64_t>((uint64_t)m->classes * m->clauses, 1) * 4));
+  CK(tmb_dev_malloc((void **)&m->d_lits, std::max<uint64_t>((uint64_t)m->classes * m->clauses, 1) * 4));
   m->lits_valid = false;
   m->has_state = with_state;
   return TM_OK;
@@ -264,6 +290,11 @@ extern "C" int tm_create(const tm_params *p, tm_machine **out) {
     m->autotune = t && t[0] >= '0' && t[0] <= '2' ? t[0] - '0' : 1;
     // TSETLIN_B200_VARIANT=mode:cpw pins the train-kernel variant, as
     // tm_force_variant does (for measurements from the command line)
+    // TSETLIN_B200_ROW_WAIT=k: a thread gives up on a sample row after k
+    // try-waits and the train call reports TM_ERR_DEVICE (0: at once).  For
+    // tests of the device error path; copies in flight are still drained.
+    const char *rw = getenv("TSETLIN_B200_ROW_WAIT");
+    if (rw && rw[0] >= '0' && rw[0] <= '9') m->row_wait = (uint32_t)strtoul(rw, nullptr, 10);
     const char *v = getenv("TSETLIN_B200_VARIANT");
     int vm = -1, vc = 1;
     if (v && sscanf(v, "%d:%d", &vm, &vc) >= 1 && vm >= 0 && vm <= TM_MODE_WARP &&
@@ -469,6 +500,7 @@ static TrainSmem plan_smem(uint32_t Wpmax, uint32_t Bmax, uint32_t smax, int mod
   L.ovf_off = take(TM_IB_SLOTS * L.ovf_cap * 4);
   L.misc_off = take(32 * 4);
   L.total = o;
+  L.wait_limit = TM_WAIT_LIMIT;
   return L;
 }
 
@@ -503,8 +535,10 @@ static int validate_train(tm_machine *m, const tm_train_args *a) {
 }
 
 // ---------------------------------------------------------------------------
-// Train kernel variants.  All end in the same automaton state (every draw is
-// keyed, §draw contract), so the choice is a matter of speed only: a
+// Train kernel variants.  All end in the same automaton state (every random
+// draw is a Philox output keyed by seed, epoch, sample and unit, so no draw
+// depends on which thread or variant takes it), so the choice is a matter of
+// speed only: a
 // heuristic by resident CTAs per SM, or an autotuner that times the
 // feasible variants on a short trial of the actual launch and caches the
 // fastest per launch shape for the life of the process.
@@ -591,6 +625,8 @@ static int launch_plan(const TrainPlan &p, const TrainShape &sh, const std::vect
   CK(cudaMemsetAsync(base + off_c, 0, 8, st));
   uint32_t *counter = (uint32_t *)(base + off_c);
   uint32_t *err = counter + 1;
+  TrainSmem lay = p.lay;
+  lay.wait_limit = m0->row_wait;
   if (ms) CK(cudaEventRecord(m0->ev0, st));
   if (p.mode == TM_MODE_WARP)
     CK(launch_train_warp((const TrainDev *)base, (const WorkItem *)(base + off_w),
@@ -598,7 +634,7 @@ static int launch_plan(const TrainPlan &p, const TrainShape &sh, const std::vect
                          sh.smax, p.grid, st));
   else
     CK(launch_train((const TrainDev *)base, (const WorkItem *)(base + off_w),
-                    (uint32_t)work.size(), counter, e0, e1, p.lay, p.mode, sh.Bmin, sh.Bmax,
+                    (uint32_t)work.size(), counter, e0, e1, lay, p.mode, sh.Bmin, sh.Bmax,
                     p.cpw, p.grid, err, st));
   if (ms) CK(cudaEventRecord(m0->ev1, st));
   note_launch(m0, 1);
@@ -1101,15 +1137,21 @@ static int predict_common(tm_machine *m, const uint8_t *problems, const int64_t 
 
 int tmb_fail(int code, const char *msg) { return fail(code, "%s", msg); }
 
-int tmb_machine_view(tm_machine *m, MachineView *v) {
+int tmb_machine_view(tm_machine *m, MachineView *v, const char *who) {
   if (!m || !v) return fail(TM_ERR_ARG, "null argument");
-  if (m->individualized) return fail(TM_ERR_ARG, "serving takes dense (non-individualized) machines");
+  if (m->individualized)
+    return fail(TM_ERR_ARG, "%s takes dense (non-individualized) machines",
+                who ? who : "this call");
   DevGuard g(m->device);
+  // A dense machine's resident class table never changes after it is laid
+  // out, so nothing is uploaded here.  The literal counts are recomputed
+  // only after the automata changed (train, restore, import), and only then
+  // is the machine's stream drained so that callers on other streams see
+  // them: a view of an unchanged machine costs no copy and no wait.
+  const bool fresh = !m->lits_valid;
   int rc = ensure_lits(m);
   if (rc) return rc;
-  rc = upload_cls(m, m->d_cls, m->cls);
-  if (rc) return rc;
-  CK(cudaStreamSynchronize(m->st));
+  if (fresh) CK(cudaStreamSynchronize(m->st));
   v->act = m->d_act;
   v->lits = m->d_lits;
   v->cls = m->d_cls;
@@ -1211,6 +1253,65 @@ extern "C" int tm_import_state(tm_machine *m, const uint8_t *actions, const uint
   }
   CK(cudaStreamSynchronize(m->st));
   return TM_OK;
+}
+
+// Classes [lo, hi) of the actions (counts = false) or count planes, in the
+// reference byte layout, to or from `buf` (host, or device memory of the
+// machine's device when on_device).  Class h's rows start where the classes
+// before it end, so the range is one contiguous byte slice of the full
+// layout; for a dense machine it is also one strided device block.
+static int copy_classes(tm_machine *m, uint32_t lo, uint32_t hi, bool to_buf, uint8_t *buf,
+                        bool counts, bool on_device) {
+  const uint32_t planes = counts ? m->B - 1 : 1;
+  const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice
+                                        : (to_buf ? cudaMemcpyDeviceToHost : cudaMemcpyHostToDevice);
+  uint64_t bo = 0;
+  for (uint32_t h = lo; h < hi;) {
+    // dense machines: every class from h on in one copy
+    const uint32_t h1 = m->individualized ? h + 1 : hi;
+    const ClassDev &c = m->cls[h];
+    const uint64_t rows = (uint64_t)(h1 - h) * m->clauses * planes;
+    uint32_t *dev = counts ? m->d_cnt + c.cnt_off : m->d_act + c.act_off;
+    const size_t width = m->n_chunks[h];
+    if (to_buf)
+      CK(cudaMemcpy2DAsync(buf + bo, width, dev, (size_t)c.Wp * 4, width, rows, kind, m->st));
+    else
+      CK(cudaMemcpy2DAsync(dev, (size_t)c.Wp * 4, buf + bo, width, width, rows, kind, m->st));
+    bo += rows * width;
+    h = h1;
+  }
+  return TM_OK;
+}
+
+static int classes_io(tm_machine *m, uint32_t lo, uint32_t hi, bool to_buf, uint8_t *actions,
+                      uint8_t *state, int32_t on_device) {
+  if (!m) return fail(TM_ERR_ARG, "null machine");
+  if (lo > hi || hi > m->classes)
+    return fail(TM_ERR_ARG, "class range [%u, %u) outside [0, %u)", lo, hi, m->classes);
+  if (state && !m->d_cnt) return fail(TM_ERR_STATE, "machine has no state");
+  DevGuard g(m->device);
+  if (actions) {
+    int rc = copy_classes(m, lo, hi, to_buf, actions, false, on_device != 0);
+    if (rc) return rc;
+    if (!to_buf) m->lits_valid = false;
+  }
+  if (state) {
+    int rc = copy_classes(m, lo, hi, to_buf, state, true, on_device != 0);
+    if (rc) return rc;
+  }
+  CK(cudaStreamSynchronize(m->st));
+  return TM_OK;
+}
+
+extern "C" int tm_export_classes(tm_machine *m, uint32_t class_begin, uint32_t class_end,
+                                 uint8_t *actions, uint8_t *state, int32_t on_device) {
+  return classes_io(m, class_begin, class_end, true, actions, state, on_device);
+}
+
+extern "C" int tm_import_classes(tm_machine *m, uint32_t class_begin, uint32_t class_end,
+                                 const uint8_t *actions, const uint8_t *state, int32_t on_device) {
+  return classes_io(m, class_begin, class_end, false, (uint8_t *)actions, (uint8_t *)state,
+                    on_device);
 }
 
 // capi.c:1564-1576

@@ -69,7 +69,13 @@ struct TrainSmem {
   uint32_t ovf_off, ovf_cap;        // TM_IB_SLOTS slots: overflow entries
   uint32_t misc_off;
   uint32_t total;
+  // try-wait iterations a thread spends on a sample row before it reports
+  // the copy as lost (TM_ERR_DEVICE); the drain of copies still in flight
+  // at exit always uses the full limit
+  uint32_t wait_limit;
 };
+
+constexpr uint32_t TM_WAIT_LIMIT = 1u << 22;
 
 constexpr int TM_TRAIN_THREADS = 256;  // 8 warps: warp j owns clause j of the unit
 constexpr int TM_RING = 3;             // sample ring depth
@@ -136,6 +142,9 @@ struct MachineView {
 }  // namespace tmb
 
 struct tm_machine;
-// Fills `v` (computing literal counts if needed).  Dense machines only.
-int tmb_machine_view(tm_machine *m, tmb::MachineView *v);
+// Fills `v` (computing literal counts if needed).  Dense machines only;
+// `who` names the caller in the error message.
+int tmb_machine_view(tm_machine *m, tmb::MachineView *v, const char *who);
 int tmb_fail(int code, const char *msg);
+// cudaMalloc behind the failure injection of tm_debug_fail_alloc
+cudaError_t tmb_dev_malloc(void **p, size_t n);

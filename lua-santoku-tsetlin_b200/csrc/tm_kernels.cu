@@ -72,9 +72,10 @@ __device__ __forceinline__ void tma_row(uint64_t *bar, void *dst, const void *sr
       : "memory");
 }
 // Bounded wait for the phase with the given parity; false on time-out.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity,
+                                          uint32_t limit = TM_WAIT_LIMIT) {
   const uint32_t a = smem_u32(bar);
-  for (uint32_t it = 0; it < (1u << 22); it++) {
+  for (uint32_t it = 0; it < limit; it++) {
     uint32_t done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
@@ -644,7 +645,7 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
         // ---- sequential per-sample steps ---------------------------------
         for (uint32_t a = 0; a < nact; a++) {
           const uint32_t k = gs + a, sl = k % TM_RING;
-          if (!mbar_wait(&bars[sl], (k / TM_RING) & 1u)) {
+          if (!mbar_wait(&bars[sl], (k / TM_RING) & 1u, lay.wait_limit)) {
             misc[20] = 1;
             if constexpr (PAIR) peer_misc[20] = 1;
             atomicOr(err, 1u);
@@ -709,7 +710,12 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
           }
           unit_sync<PAIR>();
           if (misc[20]) {
+            // rows gs + a .. issued - 1 are still to be drained: row gs + a
+            // first (its phase may or may not have completed -- waiting on
+            // a completed phase returns at once), then the ones issued
+            // ahead of it, each in its own ring slot
             aborted = true;
+            gs += a;
             break;
           }
           if (tid == 0 && a + TM_RING - 1 < nact) {
@@ -915,7 +921,7 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
           // the next sample's evaluation reads clauses this step updated
           __syncthreads();
         }
-        gs += nact;
+        if (!aborted) gs += nact;
         unit_sync<PAIR>();
       }
     }

@@ -52,27 +52,30 @@ extern "C" int tm_predict_noalloc(tm_machine *m, const uint8_t *problems, uint64
   if (n == 0) return TM_OK;
   if (!problems) return tmb_fail(TM_ERR_ARG, "predict_noalloc: problems missing");
   tmb::MachineView v{};
-  int rc = tmb_machine_view(m, &v);  // dense machines only; no allocation
+  int rc = tmb_machine_view(m, &v, "predict_noalloc");  // no allocation
   if (rc) return rc;
   if (v.type == TM_CLASSIFIER && !out_classes)
     return tmb_fail(TM_ERR_ARG, "predict_noalloc: out_classes missing");
   if (v.type == TM_ENCODER && !out_codes)
     return tmb_fail(TM_ERR_ARG, "predict_noalloc: out_codes missing");
+  // Bound n before any size is multiplied out: a sample needs Wp words of
+  // padded row and `classes` vote sums, plus up to 256 bytes of alignment
+  // for the whole request.
+  const uint64_t per_sample = (uint64_t)v.Wp * 4 + (uint64_t)v.classes * 4;
+  if (n > (TM_NOALLOC_SCRATCH_BYTES - 256) / per_sample)
+    return tmb_fail(TM_ERR_ARG,
+                    "predict_noalloc: request needs more than the 8 MiB scratch; split it or use "
+                    "tm_predict");
   int prev = -1;
-  cudaGetDevice(&prev);
+  if (cudaGetDevice(&prev) != cudaSuccess)
+    return tmb_fail(TM_ERR_CUDA, "predict_noalloc: cannot query the current device");
   if (prev != v.device && cudaSetDevice(v.device) != cudaSuccess)
     return tmb_fail(TM_ERR_CUDA, "predict_noalloc: cannot select the machine's device");
   // scratch: [padded rows, n * Wp words][vote sums, n * classes int32]
   const uint64_t xbytes = (n * v.Wp * 4 + 255) & ~255ull;
   const uint64_t sbytes = n * v.classes * 4;
   uint8_t *scratch = nullptr;
-  if (xbytes + sbytes > TM_NOALLOC_SCRATCH_BYTES) {
-    rc = tmb_fail(TM_ERR_ARG,
-                  "predict_noalloc: request needs more than the 8 MiB scratch; split it or use "
-                  "tm_predict");
-  } else {
-    rc = noalloc_scratch(v.device, &scratch);
-  }
+  rc = noalloc_scratch(v.device, &scratch);
   if (!rc) {
     uint32_t *x = (uint32_t *)scratch;
     int32_t *sums = (int32_t *)(scratch + xbytes);
@@ -88,6 +91,6 @@ extern "C" int tm_predict_noalloc(tm_machine *m, const uint8_t *problems, uint64
     if (e == cudaSuccess) e = cudaStreamSynchronize(v.st);
     if (e != cudaSuccess) rc = tmb_fail(TM_ERR_CUDA, cudaGetErrorString(e));
   }
-  if (prev >= 0 && prev != v.device) cudaSetDevice(prev);
+  if (prev != v.device) cudaSetDevice(prev);
   return rc;
 }

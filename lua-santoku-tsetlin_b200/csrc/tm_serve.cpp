@@ -198,7 +198,7 @@ extern "C" int tm_serve_open(const tm_server_config *cfg, tm_machine *const *mac
   cudaSetDevice(s->cfg.device);
   for (uint32_t i = 0; i < count; i++) {
     MachineView v{};
-    int rc = tmb_machine_view(machines[i], &v);
+    int rc = tmb_machine_view(machines[i], &v, "serving");
     if (rc) {
       delete s;
       return rc;
@@ -229,10 +229,10 @@ extern "C" int tm_serve_open(const tm_server_config *cfg, tm_machine *const *mac
               cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming) == cudaSuccess &&
               cudaHostAlloc(&sl.h_in, s->cap_in, cudaHostAllocDefault) == cudaSuccess &&
               cudaHostAlloc(&sl.h_out, s->cap_out, cudaHostAllocDefault) == cudaSuccess &&
-              cudaMalloc(&sl.d_raw, s->cap_in) == cudaSuccess &&
-              cudaMalloc(&sl.d_out, s->cap_out) == cudaSuccess &&
-              cudaMalloc(&sl.d_x, s->cap_x) == cudaSuccess &&
-              cudaMalloc(&sl.d_sums, s->cap_sums) == cudaSuccess;
+              tmb_dev_malloc((void **)&sl.d_raw, s->cap_in) == cudaSuccess &&
+              tmb_dev_malloc((void **)&sl.d_out, s->cap_out) == cudaSuccess &&
+              tmb_dev_malloc((void **)&sl.d_x, s->cap_x) == cudaSuccess &&
+              tmb_dev_malloc((void **)&sl.d_sums, s->cap_sums) == cudaSuccess;
     if (!ok) {
       free_server(s);
       return tmb_fail(TM_ERR_OOM, "serve_open: device allocation failed");

@@ -36,7 +36,7 @@ struct DevScratch {
     if (p) cudaFree(p);
     p = nullptr;
     cap = 0;
-    cudaError_t e = cudaMalloc(&p, n);
+    cudaError_t e = tmb_dev_malloc(&p, n);
     if (e == cudaSuccess) cap = n;
     return e;
   }

@@ -132,8 +132,8 @@ EXPORTS = (
     "tm_load",
     "tm_checkpoint", "tm_restore", "tm_reconfigure", "tm_restrict", "tm_type",
     "tm_destroy", "tm_last_error", "tm_align", "tm_get_info", "tm_export_state",
-    "tm_import_state", "tm_class_accuracy", "tm_encoding_accuracy", "tm_bits_to_cvec", "tm_bits_to_cvec_ind",
-    "tm_predict_noalloc", "tm_int_peaks", "tm_set_autotune", "tm_force_variant", "tm_stats_enable", "tm_get_stats", "tm_reset_stats", "tm_serve_open", "tm_serve_submit", "tm_serve_poll",
+    "tm_import_state", "tm_export_classes", "tm_import_classes", "tm_class_accuracy", "tm_encoding_accuracy", "tm_bits_to_cvec", "tm_bits_to_cvec_ind",
+    "tm_predict_noalloc", "tm_int_peaks", "tm_debug_fail_alloc", "tm_set_autotune", "tm_force_variant", "tm_stats_enable", "tm_get_stats", "tm_reset_stats", "tm_serve_open", "tm_serve_submit", "tm_serve_poll",
     "tm_serve_latency_us", "tm_serve_close",
 )
 
@@ -174,8 +174,11 @@ def lib():
     L.tm_get_info.argtypes = [vp, vp]
     L.tm_export_state.argtypes = [vp, vp, vp]
     L.tm_import_state.argtypes = [vp, vp, vp]
+    L.tm_export_classes.argtypes = [vp, u32, u32, vp, vp, i32]
+    L.tm_import_classes.argtypes = [vp, u32, u32, vp, vp, i32]
     L.tm_predict_noalloc.argtypes = [vp, vp, u64, vp, vp]
     L.tm_int_peaks.argtypes = [i32, vp]
+    L.tm_debug_fail_alloc.argtypes = [ctypes.c_int64]
     L.tm_set_autotune.argtypes = [vp, i32]
     L.tm_force_variant.argtypes = [vp, i32, i32]
     L.tm_class_accuracy.argtypes = [vp, vp, u64, u32, i32, i32, vp]
@@ -487,6 +490,39 @@ class Machine:
         a = _Buf(actions, np.uint8)
         s = _Buf(state, np.uint8)
         _check(lib().tm_import_state(self.handle, a.ptr, s.ptr))
+
+    def class_bytes(self, lo, hi):
+        """Bytes of classes [lo, hi) in the action and count-plane layouts
+        of export_state."""
+        info = self.info()
+        per = info["action_chunks"] // max(1, info["classes"])
+        if info["individualized"]:
+            raise TsetlinError("class_bytes: individualized machines have uneven class blocks")
+        a = (hi - lo) * per
+        return a, a * (info["state_bits"] - 1)
+
+    def export_classes(self, lo, hi, out):
+        """Copy classes [lo, hi) (actions, then count planes) into `out`, a
+        uint8 buffer of sum(class_bytes(lo, hi)) bytes: a CUDA tensor on this
+        machine's device (copied on the device) or host memory."""
+        a, s = self.class_bytes(lo, hi)
+        b = _Buf(out, np.uint8)
+        if b.nbytes < a + s:
+            raise TsetlinError("export_classes: buffer too small")
+        base = b.ptr or 0
+        _check(lib().tm_export_classes(self.handle, lo, hi, base if a else None,
+                                       base + a if s else None, 1 if b.device else 0))
+        return out
+
+    def import_classes(self, lo, hi, buf):
+        """Inverse of export_classes."""
+        a, s = self.class_bytes(lo, hi)
+        b = _Buf(buf, np.uint8)
+        if b.nbytes < a + s:
+            raise TsetlinError("import_classes: buffer too small")
+        base = b.ptr or 0
+        _check(lib().tm_import_classes(self.handle, lo, hi, base if a else None,
+                                       base + a if s else None, 1 if b.device else 0))
 
 
 def _params(type_, tbl):

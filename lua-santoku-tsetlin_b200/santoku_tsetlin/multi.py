@@ -86,10 +86,12 @@ def train_sharded(machine, tbl, group=None, device=None):
     """Train one machine across the ranks of `group`: rank r trains the
     units of its class range (`class_range`) -- nothing is exchanged while
     training -- then one all-gather of each range's action and count-plane
-    bytes (the reference's per-class byte blocks, contiguous for a dense
-    machine) leaves the full trained machine on every rank, bit-identical to
-    training it on one GPU.  `device`: where the exchanged tensors live (a
-    CUDA device for NCCL, None for gloo)."""
+    bytes (the reference's per-class byte blocks, `Machine.export_classes`)
+    leaves the full trained machine on every rank, bit-identical to training
+    it on one GPU.  `device`: a CUDA device for NCCL, where the slices are
+    exported, exchanged and imported device to device; None for gloo (host
+    buffers).  A rank whose range is empty (more ranks than classes) trains
+    nothing but joins the exchange, so no rank waits for it."""
     import torch
     import torch.distributed as dist
     world = dist.get_world_size(group) if dist.is_initialized() else 1
@@ -99,29 +101,22 @@ def train_sharded(machine, tbl, group=None, device=None):
         raise ValueError("train_sharded: individualized machines have uneven class blocks")
     classes = info["classes"]
     lo, hi = class_range(classes, world, rank)
-    t = dict(tbl)
-    t["class_range"] = (lo, hi)
-    machine.train(t)
+    if hi > lo:
+        t = dict(tbl)
+        t["class_range"] = (lo, hi)
+        machine.train(t)
     if world == 1:
         return machine
-    acts, state = machine.export_state()
-    pa = len(acts) // classes
-    ps = 0 if state is None else len(state) // classes
     ranges = [class_range(classes, world, r) for r in range(world)]
     width = max(h - l for l, h in ranges)
-    mine = np.zeros(width * (pa + ps), dtype=np.uint8)
-    mine[:(hi - lo) * pa] = acts[lo * pa:hi * pa]
-    if ps:
-        mine[width * pa:width * pa + (hi - lo) * ps] = state[lo * ps:hi * ps]
-    local = torch.from_numpy(mine)
-    if device is not None:
-        local = local.to(device)
+    slot = sum(machine.class_bytes(0, width))
+    local = torch.zeros(slot, dtype=torch.uint8, device=device)
+    if hi > lo:
+        machine.export_classes(lo, hi, local)
     parts = [torch.empty_like(local) for _ in range(world)]
     dist.all_gather(parts, local, group=group)
-    for (l, h), part in zip(ranges, parts):
-        b = part.cpu().numpy()
-        acts[l * pa:h * pa] = b[:(h - l) * pa]
-        if ps:
-            state[l * ps:h * ps] = b[width * pa:width * pa + (h - l) * ps]
-    machine.import_state(acts, state)
+    for r, ((l, h), part) in enumerate(zip(ranges, parts)):
+        if r != rank and h > l:
+            a, st = machine.class_bytes(l, h)
+            machine.import_classes(l, h, part[:a + st])
     return machine

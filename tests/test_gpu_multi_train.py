@@ -91,3 +91,34 @@ def test_class_sharded_training_equals_single_process(tm):
     for rank in (0, 1):
         assert got[rank][0] == want, got[rank][0]
         assert got[rank][1] == want_pred
+
+
+@pytest.mark.parametrize("on_device", [True, False])
+def test_class_slices_round_trip(tm, on_device):
+    """export_classes / import_classes move exactly the slice of the
+    reference byte layout that a class range occupies, device to device (the
+    NCCL exchange of train_sharded) or through host memory (gloo)."""
+    import torch
+    x, y = _data()
+    t = tm.create("classifier", dict(CFG))
+    t.train(dict(samples=len(y), problems=x, solutions=y, iterations=2))
+    ta, ts = t.export_state()
+    C = CFG["classes"]
+    pa, ps = len(ta) // C, len(ts) // C
+    u = tm.create("classifier", dict(CFG, seed=99))
+    for lo, hi in ((0, 2), (2, 5)):
+        a, s = t.class_bytes(lo, hi)
+        assert (a, s) == ((hi - lo) * pa, (hi - lo) * ps)
+        buf = torch.zeros(a + s + 5, dtype=torch.uint8, device="cuda" if on_device else "cpu")
+        t.export_classes(lo, hi, buf)
+        got = buf.cpu().numpy()
+        assert np.array_equal(got[:a], ta[lo * pa:hi * pa])
+        assert np.array_equal(got[a:a + s], ts[lo * ps:hi * ps])
+        u.import_classes(lo, hi, buf)
+    ua, us = u.export_state()
+    assert np.array_equal(ua, ta) and np.array_equal(us, ts)
+    assert np.array_equal(u.predict(x, 64), t.predict(x, 64))
+    with pytest.raises(tm.TsetlinError):
+        t.export_classes(3, 9, torch.zeros(1 << 20, dtype=torch.uint8))
+    t.destroy()
+    u.destroy()

@@ -467,3 +467,39 @@ def test_every_train_variant_matches_oracle(tm, features):
     with pytest.raises(tm.TsetlinError):  # the warp kernel has one clause layout
         t.train(train_table(kind, inp, 1))
     t.destroy()
+
+
+@pytest.fixture(scope="module")
+def c1_multiwave():
+    """The large sparse classifier's rows (16,384 features flip-packed to
+    1,024 words, Zipf data) with 240 clauses per class: 600 units of 8
+    clauses, more than one wave of resident CTAs, trained 1 epoch on 2,000
+    samples -- the production scheduling path (cost-ordered work list,
+    atomic work counter, a CTA taking several units with its row ring's
+    phase carried from one unit to the next)."""
+    from santoku_tsetlin import datagen
+    x, y = datagen.sparse_classifier(2300, classes=20, features=16384, seed=77)
+    cfg = dict(type="classifier", classes=20, features=16384, clauses=240, clause_tolerance=64,
+               clause_maximum=64, specificity=25.0, target=200)
+    inp = dict(n=2000, x=x[:2000].ravel(), labels=y[:2000], xt=x[2000:].ravel(), nt=300)
+    m = _oracle_pair("classifier", cfg, inp, 1, seed=41)
+    return cfg, inp, (m.actions(), m.state(), m.predict(inp["xt"], 300, scores=True)[1])
+
+
+@pytest.mark.parametrize("mode,cpw", [(-1, 1), (1, 1), (1, 2), (1, 4), (2, 1)],
+                         ids=["auto", "global1", "global2", "global4", "pair"])
+def test_multiwave_wide_rows_match_oracle(tm, c1_multiwave, mode, cpw):
+    cfg, inp, (wa, ws, wsc) = c1_multiwave
+    kind, tbl = ref_table(cfg, seed=41)
+    t = tm.create(kind, tbl)
+    if mode >= 0:
+        t.force_variant(mode, cpw)
+    t.stats_enable(True)
+    t.train(train_table(kind, inp, 1))
+    st = t.stats()
+    assert st["train_unit_steps"] == 600 * 2000
+    a, s = t.export_state()
+    assert np.array_equal(a, wa), (mode, cpw)
+    assert np.array_equal(s, ws), (mode, cpw)
+    assert np.array_equal(t.predict_scores(inp["xt"], 300), wsc)
+    t.destroy()

@@ -122,8 +122,31 @@ class _OracleRangeMachine:
     def import_state(self, a, s):
         self.m.load_state(a, s)
 
+    # the class-slice interface of santoku_tsetlin.Machine, on host tensors
+    def class_bytes(self, lo, hi):
+        C = self.m.info["classes"]
+        pa, ps = len(self.a0) // C, len(self.s0) // C
+        return (hi - lo) * pa, (hi - lo) * ps
 
-def _sharded_worker(rank, world, port, out):
+    def export_classes(self, lo, hi, out):
+        a, s = self.export_state()
+        na, ns = self.class_bytes(lo, hi)
+        pa, ps = self.class_bytes(0, 1)
+        out[:na] = __import__("torch").from_numpy(a[lo * pa:lo * pa + na].copy())
+        out[na:na + ns] = __import__("torch").from_numpy(s[lo * ps:lo * ps + ns].copy())
+        return out
+
+    def import_classes(self, lo, hi, buf):
+        a, s = self.export_state()
+        na, ns = self.class_bytes(lo, hi)
+        pa, ps = self.class_bytes(0, 1)
+        b = buf.numpy()
+        a[lo * pa:lo * pa + na] = b[:na]
+        s[lo * ps:lo * ps + ns] = b[na:na + ns]
+        self.import_state(a, s)
+
+
+def _sharded_worker(rank, world, port, out, classes):
     import sys
     import torch.distributed as dist
     here = os.path.dirname(os.path.abspath(__file__))
@@ -137,7 +160,7 @@ def _sharded_worker(rank, world, port, out):
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         rng = np.random.default_rng(8)
-        F, n, classes = 30, 50, 5
+        F, n = 30, 50
         cfg = dict(type="classifier", classes=classes, features=F, clauses=16,
                    clause_tolerance=6, clause_maximum=12, specificity=4.0)
         b = rng.random((n, F)) < 0.3
@@ -154,14 +177,17 @@ def _sharded_worker(rank, world, port, out):
         dist.destroy_process_group()
 
 
-def test_train_sharded_gathers_every_class(oracle_lib):
-    """World size 2 over gloo: each rank holds every class's automata after
-    `train_sharded`, equal to one process training the whole machine."""
-    world = 2
+@pytest.mark.parametrize("world,classes", [(2, 5), (3, 2)])
+def test_train_sharded_gathers_every_class(oracle_lib, world, classes):
+    """gloo ranks on CPU: each rank holds every class's automata after
+    `train_sharded`, equal to one process training the whole machine --
+    also with more ranks than classes, where a rank trains nothing but must
+    still join the exchange (otherwise the others would wait for it)."""
     port = _free_port()
     ctx = mp.get_context("spawn")
     out = ctx.Manager().dict()
-    procs = [ctx.Process(target=_sharded_worker, args=(r, world, port, out)) for r in range(world)]
+    procs = [ctx.Process(target=_sharded_worker, args=(r, world, port, out, classes))
+             for r in range(world)]
     for p in procs:
         p.start()
     for p in procs:

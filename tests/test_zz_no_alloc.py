@@ -75,3 +75,33 @@ def test_noalloc_refuses_oversized_request(tm):
     rc = lib.tm_predict_noalloc(t.handle, xd.data_ptr(), nq, out.data_ptr(), None)
     assert rc < 0
     assert b"8 MiB" in lib.tm_last_error()
+
+
+@pytest.mark.parametrize("nq", [2 ** 31, 2 ** 62, 2 ** 64 - 1])
+def test_noalloc_refuses_huge_n_without_touching_memory(tm, nq):
+    # n so large that n * row bytes wraps 64 bits: refused before any size is
+    # multiplied out, so the small buffers below are never read or written
+    import torch
+    t = _trained(tm, "classifier", features=300, classes=11, n=64, seed=6)
+    xd = torch.zeros(256, dtype=torch.uint8, device="cuda")
+    out = torch.zeros(4, dtype=torch.int64, device="cuda")
+    lib = tm.lib()
+    rc = lib.tm_predict_noalloc(t.handle, xd.data_ptr(), nq, out.data_ptr(), None)
+    assert rc == -1  # TM_ERR_ARG
+    assert b"8 MiB" in lib.tm_last_error()
+    assert int(out.abs().sum().item()) == 0
+
+
+def test_noalloc_refuses_individualized_with_its_own_name(tm):
+    t = tm.create("classifier", dict(classes=2, clauses=8, clause_tolerance=8, clause_maximum=8,
+                                     specificity=4.0, individualized=True,
+                                     feat_offsets=[0, 3, 7]))
+    lib = tm.lib()
+    rc = lib.tm_predict_noalloc(t.handle, None, 0, None, None)
+    assert rc == 0  # n == 0 is a no-op
+    import torch
+    xd = torch.zeros(16, dtype=torch.uint8, device="cuda")
+    out = torch.zeros(1, dtype=torch.int64, device="cuda")
+    rc = lib.tm_predict_noalloc(t.handle, xd.data_ptr(), 1, out.data_ptr(), None)
+    assert rc == -1
+    assert b"predict_noalloc" in lib.tm_last_error()
