@@ -1096,7 +1096,7 @@ static int predict_common(tm_machine *m, const uint8_t *problems, const int64_t 
   CK(launch_predict(m->d_act, m->d_lits, m->d_cls, nullptr, m->classes, m->clauses, m->tol,
                     m->x.as<uint32_t>(), (uint32_t)n, m->sums.as<int32_t>(), m->st));
   if (m->timing) CK(cudaEventRecord(m->ev1, m->st));
-  note_launch(m, 1);
+  note_launch(m, n <= TM_SMALL_N_MAX ? (n + 15) / 16 : 1);
   m->stats.predict_launches++;
   // outputs
   int64_t *dcls = nullptr, *dsc = nullptr;

@@ -129,6 +129,33 @@ cudaError_t launch_finalize(const int32_t *sums, uint32_t n, uint32_t classes, i
                             cudaStream_t st);
 
 
+// One predict job of a multi-job launch (k_predict_multi): a machine's
+// resident automata scored against n padded sample rows.  Its tiles are
+// blocks tile0 .. tile0 + stiles * classes * tpc - 1 of the launch.
+struct PredictJob {
+  const uint32_t *act;
+  const int32_t *lits;
+  const ClassDev *cls;
+  const uint32_t *x;
+  int32_t *sums;          // n x classes, accumulated (zeroed by the caller)
+  const uint32_t *gate;   // optional: the job runs only while *gate != 0
+  uint32_t clauses, tpc, tol, n, classes;
+  uint32_t tile0, stiles;
+  uint32_t pad;
+};
+// tiles of one predict job (64 samples x 64 clauses each)
+uint32_t predict_job_tiles(uint32_t n, uint32_t classes, uint32_t clauses, uint32_t *stiles,
+                           uint32_t *tpc);
+cudaError_t launch_predict_multi(const PredictJob *jobs_dev, uint32_t njobs, uint32_t total_tiles,
+                                 cudaStream_t st);
+// Predicts of at most this many samples read each clause row once with one
+// warp per row (k_predict_small) instead of the 64 x 64 tiles.
+constexpr uint32_t TM_SMALL_N_MAX = 32;
+// k_lits with an optional gate (skipped while *gate == 0)
+cudaError_t launch_lits_gated(const uint32_t *act, const ClassDev *cls, uint32_t classes,
+                              uint32_t clauses, int32_t *lits, const uint32_t *gate,
+                              cudaStream_t st);
+
 // Read-only view of a resident dense machine for the server (tm_serve.cpp).
 struct MachineView {
   const uint32_t *act;

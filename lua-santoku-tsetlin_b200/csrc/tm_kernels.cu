@@ -1318,7 +1318,9 @@ cudaError_t launch_train(const TrainDev *machines, const WorkItem *work, uint32_
 // Literal counts (capi.c:103-108): one warp per clause row.
 // ---------------------------------------------------------------------------
 __global__ void k_lits(const uint32_t *__restrict__ act, const ClassDev *__restrict__ cls,
-                       uint32_t clauses, int32_t *__restrict__ lits) {
+                       uint32_t clauses, int32_t *__restrict__ lits,
+                       const uint32_t *__restrict__ gate) {
+  if (gate && *gate == 0) return;
   const ClassDev C = cls[blockIdx.y];
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
@@ -1335,11 +1337,17 @@ __global__ void k_lits(const uint32_t *__restrict__ act, const ClassDev *__restr
   }
 }
 
+cudaError_t launch_lits_gated(const uint32_t *act, const ClassDev *cls, uint32_t classes,
+                              uint32_t clauses, int32_t *lits, const uint32_t *gate,
+                              cudaStream_t st) {
+  dim3 grid((clauses + 7) / 8 < 64 ? (clauses + 7) / 8 : 64, classes);
+  k_lits<<<grid, 256, 0, st>>>(act, cls, clauses, lits, gate);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_lits(const uint32_t *act, const ClassDev *cls, uint32_t classes,
                         uint32_t clauses, int32_t *lits, cudaStream_t st) {
-  dim3 grid((clauses + 7) / 8 < 64 ? (clauses + 7) / 8 : 64, classes);
-  k_lits<<<grid, 256, 0, st>>>(act, cls, clauses, lits);
-  return cudaGetLastError();
+  return launch_lits_gated(act, cls, classes, clauses, lits, nullptr, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -1367,19 +1375,17 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-__global__ void __launch_bounds__(256, 2)
-    k_predict(const uint32_t *__restrict__ act, const int32_t *__restrict__ lits,
-              const ClassDev *__restrict__ cls, uint32_t clauses, uint32_t tiles_per_class,
-              uint32_t tol, const uint32_t *__restrict__ x, uint32_t n, uint32_t classes,
-              int32_t *__restrict__ sums) {
+// One (64 samples) x (64 clauses of class h) tile: samples s0.., clauses c0..
+__device__ __forceinline__ void predict_tile(const uint32_t *__restrict__ act,
+                                             const int32_t *__restrict__ lits, const ClassDev &C,
+                                             uint32_t h, uint32_t c0, uint32_t s0,
+                                             uint32_t clauses, uint32_t tol,
+                                             const uint32_t *__restrict__ x, uint32_t n,
+                                             uint32_t classes, int32_t *__restrict__ sums) {
   // two buffers: the next 32-word chunk streams in while this one is used
   __shared__ __align__(16) uint32_t As[2][PT_C * PT_LD];
   __shared__ __align__(16) uint32_t Xs[2][PT_S * PT_LD];
   __shared__ int32_t red[16][PT_S + 1];
-  const uint32_t h = blockIdx.y / tiles_per_class;
-  const uint32_t c0 = (blockIdx.y % tiles_per_class) * PT_C;
-  const uint32_t s0 = blockIdx.x * PT_S;
-  const ClassDev C = cls[h];
   const uint32_t tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   // Failed-literal counts popc(a & ~x) per (clause, sample).  Five of every
   // eight 4-word steps go through carry-save adders: `ones` and `twos` hold
@@ -1493,15 +1499,162 @@ __global__ void __launch_bounds__(256, 2)
   }
 }
 
+
+__global__ void __launch_bounds__(256, 2)
+    k_predict(const uint32_t *__restrict__ act, const int32_t *__restrict__ lits,
+              const ClassDev *__restrict__ cls, uint32_t clauses, uint32_t tiles_per_class,
+              uint32_t tol, const uint32_t *__restrict__ x, uint32_t n, uint32_t classes,
+              int32_t *__restrict__ sums) {
+  const uint32_t h = blockIdx.y / tiles_per_class;
+  const ClassDev C = cls[h];
+  predict_tile(act, lits, C, h, (blockIdx.y % tiles_per_class) * PT_C, blockIdx.x * PT_S, clauses,
+               tol, x, n, classes, sums);
+}
+
+// Many predict jobs (machines and sample sets of any size) in one launch:
+// block b runs tile b - jobs[j].tile0 of the job j whose tiles contain b
+// (jobs in ascending tile0); a job whose gate reads 0 is skipped.
+__global__ void __launch_bounds__(256, 2)
+    k_predict_multi(const PredictJob *__restrict__ jobs, uint32_t njobs) {
+  uint32_t lo = 0, hi = njobs;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (jobs[mid].tile0 <= blockIdx.x) lo = mid;
+    else hi = mid;
+  }
+  const PredictJob J = jobs[lo];
+  if (J.gate && *J.gate == 0) return;
+  const uint32_t t = blockIdx.x - J.tile0;
+  const uint32_t st = t % J.stiles, ct = t / J.stiles;
+  const uint32_t h = ct / J.tpc;
+  const ClassDev C = J.cls[h];
+  predict_tile(J.act, J.lits, C, h, (ct % J.tpc) * PT_C, st * PT_S, J.clauses, J.tol, J.x, J.n,
+               J.classes, J.sums);
+}
+
+// ---------------------------------------------------------------------------
+// Small-batch predict (at most 16 samples per launch): one warp per clause
+// row.  The row streams once through the warp in 128-bit loads that do not
+// allocate in L1 (every action word is read once per launch: the HBM-bound
+// regime of a serving request), and each word is tested against all the
+// launch's samples, whose rows every CTA re-reads through L1.  Lane s keeps
+// sample s's vote sum over the warp's clauses (capi.c:110-118 votes, signed
+// by clause parity as in capi.c:148-161) and adds it to sums once.  The
+// same integer votes as k_predict, so the same sums bit for bit.
+// Grid: (clause blocks of TM_SMALL_CPB clauses, classes).
+// ---------------------------------------------------------------------------
+constexpr uint32_t TM_SMALL_CPB = 64;
+
+__device__ __forceinline__ uint4 ld_stream16(const void *p) {
+  uint4 v;
+  asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "l"(p));
+  return v;
+}
+
+template <int NS>
+__global__ void __launch_bounds__(256)
+    k_predict_small(const uint32_t *__restrict__ act, const int32_t *__restrict__ lits,
+                    const ClassDev *__restrict__ cls, uint32_t clauses, uint32_t tol,
+                    const uint32_t *__restrict__ x, uint32_t s0, uint32_t ns, uint32_t classes,
+                    int32_t *__restrict__ sums) {
+  const uint32_t h = blockIdx.y;
+  const ClassDev C = cls[h];
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t cb = blockIdx.x * TM_SMALL_CPB;
+  const uint32_t ce = cb + TM_SMALL_CPB < clauses ? cb + TM_SMALL_CPB : clauses;
+  const uint32_t Q = C.Wp >> 2, qlast = (C.W - 1) >> 2, klast = (C.W - 1) & 3;
+  const uint4 *xr = (const uint4 *)(x + C.x_off + (uint64_t)s0 * C.Wp);
+  int32_t part = 0;  // lane s < ns: sample s0 + s
+  for (uint32_t c = cb + warp; c < ce; c += 8) {
+    const uint4 *ar = (const uint4 *)(act + C.act_off + (uint64_t)c * C.Wp);
+    uint32_t f[NS];
+#pragma unroll
+    for (int s = 0; s < NS; s++) f[s] = 0;
+#pragma unroll 2
+    for (uint32_t q = lane; q < Q; q += 32) {
+      uint4 a = ld_stream16(ar + q);
+      if (q == qlast) {  // evaluation mask on word W-1 (capi.c:104-106)
+        if (klast == 0) a.x &= C.emask;
+        if (klast == 1) a.y &= C.emask;
+        if (klast == 2) a.z &= C.emask;
+        if (klast == 3) a.w &= C.emask;
+      }
+#pragma unroll
+      for (int s = 0; s < NS; s++) {
+        if ((uint32_t)s < ns) {
+          const uint4 v = __ldg(xr + (uint64_t)s * Q + q);
+          f[s] += __popc(a.x & ~v.x) + __popc(a.y & ~v.y) + __popc(a.z & ~v.z) +
+                  __popc(a.w & ~v.w);
+        }
+      }
+    }
+    const int32_t L = lits[(uint64_t)h * clauses + c];
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+      if ((uint32_t)s < ns) {
+        const int32_t F = (int32_t)__reduce_add_sync(0xFFFFFFFFu, f[s]);
+        if (lane == (uint32_t)s) {
+          int32_t vote;
+          if (L == 0)
+            vote = (int32_t)tol;
+          else {
+            vote = (L < (int32_t)tol ? L : (int32_t)tol) - F;
+            vote = vote < 0 ? 0 : vote;
+          }
+          part += (c & 1) ? -vote : vote;
+        }
+      }
+    }
+  }
+  if (lane < ns && part != 0) atomicAdd(&sums[(uint64_t)(s0 + lane) * classes + h], part);
+}
+
+template <int NS>
+static void small_launch(dim3 grid, cudaStream_t st, const uint32_t *act, const int32_t *lits,
+                         const ClassDev *cls, uint32_t clauses, uint32_t tol, const uint32_t *x,
+                         uint32_t s0, uint32_t ns, uint32_t classes, int32_t *sums) {
+  k_predict_small<NS><<<grid, 256, 0, st>>>(act, lits, cls, clauses, tol, x, s0, ns, classes, sums);
+}
+
 cudaError_t launch_predict(const uint32_t *act, const int32_t *lits, const ClassDev *cls,
                            const ClassDev *cls_host, uint32_t classes, uint32_t clauses,
                            uint32_t tol, const uint32_t *x, uint32_t n, int32_t *sums,
                            cudaStream_t st) {
   (void)cls_host;
   if (!n) return cudaSuccess;
+  if (n <= TM_SMALL_N_MAX) {
+    const dim3 grid((clauses + TM_SMALL_CPB - 1) / TM_SMALL_CPB, classes);
+    for (uint32_t s0 = 0; s0 < n; s0 += 16) {
+      const uint32_t ns = n - s0 < 16 ? n - s0 : 16;
+      if (ns <= 1) small_launch<1>(grid, st, act, lits, cls, clauses, tol, x, s0, ns, classes, sums);
+      else if (ns <= 2) small_launch<2>(grid, st, act, lits, cls, clauses, tol, x, s0, ns, classes, sums);
+      else if (ns <= 4) small_launch<4>(grid, st, act, lits, cls, clauses, tol, x, s0, ns, classes, sums);
+      else if (ns <= 8) small_launch<8>(grid, st, act, lits, cls, clauses, tol, x, s0, ns, classes, sums);
+      else small_launch<16>(grid, st, act, lits, cls, clauses, tol, x, s0, ns, classes, sums);
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }
   const uint32_t tpc = (clauses + PT_C - 1) / PT_C;
   dim3 grid((n + PT_S - 1) / PT_S, classes * tpc);
   k_predict<<<grid, 256, 0, st>>>(act, lits, cls, clauses, tpc, tol, x, n, classes, sums);
+  return cudaGetLastError();
+}
+
+uint32_t predict_job_tiles(uint32_t n, uint32_t classes, uint32_t clauses, uint32_t *stiles,
+                           uint32_t *tpc) {
+  *stiles = (n + PT_S - 1) / PT_S;
+  *tpc = (clauses + PT_C - 1) / PT_C;
+  return *stiles * classes * *tpc;
+}
+
+cudaError_t launch_predict_multi(const PredictJob *jobs_dev, uint32_t njobs, uint32_t total_tiles,
+                                 cudaStream_t st) {
+  if (!njobs || !total_tiles) return cudaSuccess;
+  k_predict_multi<<<total_tiles, 256, 0, st>>>(jobs_dev, njobs);
   return cudaGetLastError();
 }
 

@@ -503,3 +503,49 @@ def test_multiwave_wide_rows_match_oracle(tm, c1_multiwave, mode, cpw):
     assert np.array_equal(s, ws), (mode, cpw)
     assert np.array_equal(t.predict_scores(inp["xt"], 300), wsc)
     t.destroy()
+
+
+@pytest.mark.parametrize("kind,classes,F,clauses,ind", [
+    ("classifier", 20, 16384, 136, False),   # the large sparse classifier's rows
+    ("encoder", 24, 4096, 40, False),
+    ("classifier", 3, 0, 24, True),          # individualized: a row width per class
+])
+def test_small_batch_predict_matches_oracle(tm, kind, classes, F, clauses, ind):
+    """Predicts of 1 to 32 samples take the warp-per-clause kernel (each
+    clause row read once), 33 and more the tiled one: both give the
+    oracle's vote sums bit for bit, at every size across the switch."""
+    rng = np.random.default_rng(classes + clauses)
+    cfg = dict(type=kind, classes=classes, clauses=clauses, clause_tolerance=48,
+               clause_maximum=64, specificity=25.0)
+    if ind:
+        fo = np.array([0, 700, 1900, 5000], dtype=np.int64)
+        cfg.update(individualized=True, feat_offsets=fo)
+    else:
+        cfg["features"] = F
+    m = O.Machine(**cfg)
+    nbytes = m.info["action_chunks"]
+    acts = np.packbits(rng.random(nbytes * 8) < 0.01, bitorder="little")
+    m.load_state(actions=acts)
+    kind2, tbl = ref_table(cfg)
+    t = tm.create(kind2, tbl)
+    t.import_state(actions=acts)
+    for n in (1, 2, 3, 5, 8, 13, 16, 17, 31, 32, 33, 70):
+        if ind:
+            blocks, dof = [], [0]
+            for h in range(classes):
+                k = int(fo[h + 1] - fo[h])
+                b = rng.random((n, k)) < 0.05
+                blocks.append(np.packbits(np.concatenate([b, ~b], axis=1), axis=1,
+                                          bitorder="little").ravel())
+                dof.append(dof[-1] + blocks[-1].size)
+            x = np.concatenate(blocks)
+            dof = np.array(dof[:-1], dtype=np.int64)
+            want = m.predict(x, n, dim_offsets=dof, scores=True)[1]
+            assert np.array_equal(t.predict_scores(x, dof, n), want), n
+        else:
+            b = rng.random((n, F)) < 0.02
+            x = np.packbits(np.concatenate([b, ~b], axis=1), axis=1, bitorder="little").ravel()
+            want_out, want = m.predict(x, n, scores=True)
+            assert np.array_equal(t.predict_scores(x, n), want), n
+            assert np.array_equal(t.predict(x, n), want_out.ravel()), n
+    t.destroy()
