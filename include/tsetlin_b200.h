@@ -129,6 +129,55 @@ typedef int (*tm_batch_epoch_cb)(void *user, uint32_t epoch, int32_t *stop, uint
 int tm_train_batch_each(tm_machine *const *machines, const tm_train_args *args, uint32_t count,
                         tm_batch_epoch_cb each, void *user);
 
+/* ---- device-resident search round ----------------------------------------
+ * One round of the reference's hyper-parameter search for `count` machines
+ * at once: every trial trains with train_tm's per-epoch logic
+ * (optimize.lua:586-653) -- after each epoch the machine is scored on a
+ * holdout, a score above best + tolerance is kept (and, with patience > 0,
+ * the actions are checkpointed), `patience` epochs without one stop the
+ * machine, and at the end a machine with a checkpoint is restored to it
+ * and scored again.  The search metric is computed on the device: the
+ * reference's usual search_metric, evaluator.class_accuracy(...).f1
+ * (evaluator/capi.c:119-202), the fraction of correct classes, or
+ * encoding_accuracy(...).mean_hamming for encoders (:497-574).  Each epoch
+ * of all machines is one CUDA graph replay and one host synchronisation.
+ * Every machine ends exactly as tm_train with the same `each` logic would
+ * leave it.  No single counterpart in the reference. */
+#define TM_METRIC_F1 0        /* classifier: macro F1 of class_accuracy */
+#define TM_METRIC_ACCURACY 1  /* classifier: correct / test_samples */
+#define TM_METRIC_HAMMING 2   /* encoder: mean_hamming of encoding_accuracy */
+
+/* After each epoch: scores[i] is machine i's score this epoch (NaN if it
+ * did not train), training[i] whether it trains on; set stop[i] = 1 to stop
+ * machine i, return non-zero to stop all. */
+typedef int (*tm_search_epoch_cb)(void *user, uint32_t epoch, const double *scores,
+                                  const int32_t *training, int32_t *stop, uint32_t count);
+
+typedef struct tm_search_args {
+  uint64_t test_samples;
+  const uint8_t *test_problems;       /* classifier problems / encoder sentences */
+  const int64_t *test_solutions;      /* classifier labels */
+  const uint8_t *test_codes;          /* encoder codes */
+  const int64_t *test_dim_offsets;    /* individualized machines */
+  const uint8_t *const *test_each;    /* optional: machine i's own holdout rows (machines whose
+                                         literal layouts differ), else test_problems for all */
+  int32_t on_device;                  /* test buffers are device pointers */
+  int32_t metric;                     /* TM_METRIC_* */
+  uint32_t patience;                  /* search_patience; 0: no early stop, no checkpoint */
+  double tolerance;                   /* search_tolerance */
+  tm_search_epoch_cb each;            /* optional */
+  void *each_user;
+  /* outputs (host arrays, each may be NULL) */
+  double *scores;          /* [count * max iterations] per-epoch scores, NaN where untrained */
+  double *final_scores;    /* [count] score of the machine as it ends */
+  double *best_scores;     /* [count] */
+  uint32_t *epochs_run;    /* [count] */
+  uint32_t *best_epochs;   /* [count] 1-based epoch of the best score */
+} tm_search_args;
+
+int tm_train_batch_search(tm_machine *const *machines, const tm_train_args *args, uint32_t count,
+                          const tm_search_args *search);
+
 /* machine:predict(problems, n) / (problems, dim_offsets, n): capi.c:1088-1110.
  * Classifier: out_classes[n] (int64, argmax, ties to the lowest class).
  * Encoder: out_codes[n * ceil(hidden/8)]. */
@@ -289,6 +338,11 @@ typedef struct tm_stats {
                                  cluster, 3 one warp per unit (rows of at most 64 words) */
   int32_t train_autotuned;    /* 1 if the autotuner chose that variant */
   int32_t train_cpw;          /* clauses per warp of that variant */
+  int32_t pad_;
+  uint64_t train_active_pairs; /* (unit, sample) steps trained after negative sampling */
+  double search_epoch_ms;     /* device-resident search rounds: summed epoch graph time */
+  uint64_t search_epochs;     /* epoch graph replays */
+  double search_train_ms;     /* the train kernel's share of those replays */
 } tm_stats;
 /* Train-kernel variant choice.  All variants end in the same automaton
  * state; they differ in speed.  mode 0: heuristic (resident CTAs per SM);

@@ -144,6 +144,9 @@ struct tm_machine {
   // Separate, so that a predict inside an `each` callback does not replace
   // the rows the next epoch trains on.
   DevBuf x, tx, raw, labels, codes, perm, perm_scratch, sums, outc, work, tdev, cls_job, errf;
+  // device-resident search round: checkpoint of the actions, and (owner of
+  // the round) its tables and the staged holdout truth
+  DevBuf ckpt, search, search_truth;
 };
 
 // Kernels launched by a CUB 64-bit radix sort of pairs: upsweep histogram,
@@ -355,7 +358,8 @@ extern "C" void tm_destroy(tm_machine *m) {
   if (m->st) cudaStreamSynchronize(m->st);
   free_device(m);
   for (DevBuf *b : {&m->x, &m->tx, &m->raw, &m->labels, &m->codes, &m->perm, &m->perm_scratch, &m->sums,
-                    &m->outc, &m->work, &m->tdev, &m->cls_job, &m->errf})
+                    &m->outc, &m->work, &m->tdev, &m->cls_job, &m->errf, &m->ckpt, &m->search,
+                    &m->search_truth})
     b->release();
   if (m->ev0) cudaEventDestroy(m->ev0);
   if (m->ev1) cudaEventDestroy(m->ev1);
@@ -622,25 +626,28 @@ static int launch_plan(const TrainPlan &p, const TrainShape &sh, const std::vect
   uint8_t *base = m0->tdev.as<uint8_t>();
   CK(cudaMemcpyAsync(base, td.data(), tb, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(base + off_w, work.data(), wb, cudaMemcpyHostToDevice, st));
-  CK(cudaMemsetAsync(base + off_c, 0, 8, st));
+  // [0] work counter, [2] status bits, [4..5] active (unit, sample) steps
+  CK(cudaMemsetAsync(base + off_c, 0, 32, st));
   uint32_t *counter = (uint32_t *)(base + off_c);
-  uint32_t *err = counter + 1;
+  uint32_t *err = counter + 2;
   TrainSmem lay = p.lay;
   lay.wait_limit = m0->row_wait;
   if (ms) CK(cudaEventRecord(m0->ev0, st));
   if (p.mode == TM_MODE_WARP)
     CK(launch_train_warp((const TrainDev *)base, (const WorkItem *)(base + off_w),
                          (uint32_t)work.size(), counter, e0, e1, sh.Wpmax, sh.Bmin, sh.Bmax,
-                         sh.smax, p.grid, st));
+                         sh.smax, p.grid, st, (unsigned long long *)(err + 2)));
   else
     CK(launch_train((const TrainDev *)base, (const WorkItem *)(base + off_w),
                     (uint32_t)work.size(), counter, e0, e1, lay, p.mode, sh.Bmin, sh.Bmax,
                     p.cpw, p.grid, err, st));
   if (ms) CK(cudaEventRecord(m0->ev1, st));
   note_launch(m0, 1);
-  *herr = 0;
-  CK(cudaMemcpyAsync(herr, err, 4, cudaMemcpyDeviceToHost, st));
+  uint32_t hc[4] = {0, 0, 0, 0};
+  CK(cudaMemcpyAsync(hc, err, 16, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
+  *herr = hc[0];
+  m0->stats.train_active_pairs += (uint64_t)hc[2] | ((uint64_t)hc[3] << 32);
   if (ms) CK(cudaEventElapsedTime(ms, m0->ev0, m0->ev1));
   return TM_OK;
 }
@@ -737,44 +744,14 @@ static int autotune_plan(std::vector<TrainJob> &jobs, const std::vector<TrainDev
   return TM_OK;
 }
 
-// Runs local epochs [e0, e1) of every job in one launch (units of all jobs
-// share the grid).  Permutations are built per job for those epochs.
-static int run_epochs(std::vector<TrainJob> &jobs, uint32_t e0, uint32_t e1, tm_machine *owner) {
-  tm_machine *m0 = owner;
-  cudaStream_t st = m0->st;
-  const int dev = m0->device;
-  // distinct (seed, n) -> permutation block
-  std::map<std::pair<uint64_t, uint64_t>, uint64_t> pidx;
-  uint64_t pwords = 0;
-  std::vector<uint64_t> joff(jobs.size());
-  for (size_t i = 0; i < jobs.size(); i++) {
-    auto key = std::make_pair(jobs[i].seed, (uint64_t)jobs[i].a->samples);
-    auto it = pidx.find(key);
-    if (it == pidx.end()) {
-      pidx[key] = pwords;
-      joff[i] = pwords;
-      pwords += (uint64_t)(e1 - e0) * jobs[i].a->samples;
-    } else {
-      joff[i] = it->second;
-    }
-  }
-  CK(m0->perm.ensure(std::max<uint64_t>(pwords, 4) * 4));
-  uint32_t maxn = 0;
-  for (auto &j : jobs) maxn = std::max<uint32_t>(maxn, (uint32_t)j.a->samples);
-  const size_t psb = perm_scratch_bytes(std::max<uint32_t>(maxn, 1));
-  CK(m0->perm_scratch.ensure(psb));
-  for (auto &kv : pidx) {
-    const uint64_t seed = kv.first.first, n = kv.first.second;
-    for (uint32_t e = e0; e < e1; e++) {
-      // the draw-contract epoch index is local epoch e (epoch_base 0)
-      CK(launch_perm(seed, e, (uint32_t)n, m0->perm.as<uint32_t>() + kv.second + (e - e0) * n,
-                     m0->perm_scratch.p, m0->perm_scratch.cap, st));
-      note_launch(m0, 1 + kSortKernels);
-    }
-  }
-  // machine table + work list
-  std::vector<TrainDev> td(jobs.size());
-  std::vector<WorkItem> work;
+// Machine table and cost-ordered work list of one launch over local epochs
+// [e0, e1); job i's epoch orders start at word joff[i] of the owner's
+// permutation buffer.
+static void build_tables(std::vector<TrainJob> &jobs, uint32_t e0, uint32_t e1, tm_machine *m0,
+                         const std::vector<uint64_t> &joff, std::vector<TrainDev> &td,
+                         std::vector<WorkItem> &work, TrainShape &sh) {
+  td.assign(jobs.size(), TrainDev{});
+  work.clear();
   uint32_t Wpmax = 4, Bmin = 32, Bmax = 2, smax = 0;
   for (size_t i = 0; i < jobs.size(); i++) {
     TrainJob &J = jobs[i];
@@ -818,13 +795,19 @@ static int run_epochs(std::vector<TrainJob> &jobs, uint32_t e0, uint32_t e1, tm_
     Bmax = std::max(Bmax, m->B);
     Bmin = std::min(Bmin, m->B);
   }
-  if (work.empty()) return TM_OK;
   std::stable_sort(work.begin(), work.end(),
                    [](const WorkItem &a, const WorkItem &b) { return a.cost > b.cost; });
-  TrainShape sh{Wpmax, Bmin, Bmax, smax, (uint32_t)work.size(), max_smem_optin(dev),
-                num_sms(dev)};
-  TrainPlan plan;
-  bool tuned = false;
+  const int dev = m0->device;
+  sh = TrainShape{Wpmax, Bmin, Bmax, smax, (uint32_t)work.size(), max_smem_optin(dev),
+                  num_sms(dev)};
+}
+
+// The train-kernel variant of a launch: pinned, tuned (trials at epoch 0,
+// on the freshly reset automata) or by the heuristic.
+static int choose_plan(std::vector<TrainJob> &jobs, const std::vector<TrainDev> &td,
+                       const std::vector<WorkItem> &work, const TrainShape &sh, uint32_t e0,
+                       tm_machine *m0, TrainPlan &plan, bool &tuned) {
+  tuned = false;
   if (m0->force_mode >= 0) {
     if (!plan_mode(m0->force_mode, sh, plan, m0->force_cpw))
       return fail(TM_ERR_ARG, "train: variant %d with %d clauses per warp cannot run this launch",
@@ -843,6 +826,52 @@ static int run_epochs(std::vector<TrainJob> &jobs, uint32_t e0, uint32_t e1, tm_
       if (rc) return rc;
     }
   }
+  return TM_OK;
+}
+
+// Runs local epochs [e0, e1) of every job in one launch (units of all jobs
+// share the grid).  Permutations are built per job for those epochs.
+static int run_epochs(std::vector<TrainJob> &jobs, uint32_t e0, uint32_t e1, tm_machine *owner) {
+  tm_machine *m0 = owner;
+  cudaStream_t st = m0->st;
+  // distinct (seed, n) -> permutation block
+  std::map<std::pair<uint64_t, uint64_t>, uint64_t> pidx;
+  uint64_t pwords = 0;
+  std::vector<uint64_t> joff(jobs.size());
+  for (size_t i = 0; i < jobs.size(); i++) {
+    auto key = std::make_pair(jobs[i].seed, (uint64_t)jobs[i].a->samples);
+    auto it = pidx.find(key);
+    if (it == pidx.end()) {
+      pidx[key] = pwords;
+      joff[i] = pwords;
+      pwords += (uint64_t)(e1 - e0) * jobs[i].a->samples;
+    } else {
+      joff[i] = it->second;
+    }
+  }
+  CK(m0->perm.ensure(std::max<uint64_t>(pwords, 4) * 4));
+  uint32_t maxn = 0;
+  for (auto &j : jobs) maxn = std::max<uint32_t>(maxn, (uint32_t)j.a->samples);
+  const size_t psb = perm_scratch_bytes(std::max<uint32_t>(maxn, 1));
+  CK(m0->perm_scratch.ensure(psb));
+  for (auto &kv : pidx) {
+    const uint64_t seed = kv.first.first, n = kv.first.second;
+    for (uint32_t e = e0; e < e1; e++) {
+      // the draw-contract epoch index is local epoch e (epoch_base 0)
+      CK(launch_perm(seed, e, (uint32_t)n, m0->perm.as<uint32_t>() + kv.second + (e - e0) * n,
+                     m0->perm_scratch.p, m0->perm_scratch.cap, st));
+      note_launch(m0, 1 + kSortKernels);
+    }
+  }
+  std::vector<TrainDev> td;
+  std::vector<WorkItem> work;
+  TrainShape sh{};
+  build_tables(jobs, e0, e1, m0, joff, td, work, sh);
+  if (work.empty()) return TM_OK;
+  TrainPlan plan;
+  bool tuned = false;
+  int prc = choose_plan(jobs, td, work, sh, e0, m0, plan, tuned);
+  if (prc) return prc;
   m0->last_mode = plan.mode;
   m0->stats.train_mode = plan.mode;
   m0->stats.train_autotuned = tuned ? 1 : 0;
@@ -963,10 +992,11 @@ extern "C" int tm_train_batch_each(tm_machine *const *ms, const tm_train_args *a
   return train_batch_impl(ms, args, count, each, user);
 }
 
-static int train_batch_impl(tm_machine *const *ms, const tm_train_args *args, uint32_t count,
-                            tm_batch_epoch_cb each, void *user) {
+// Validates a batch, stages every job's inputs (identical inputs once) and
+// resets every machine's automata (capi.c:1136-1146).
+static int stage_batch(tm_machine *const *ms, const tm_train_args *args, uint32_t count,
+                       std::vector<TrainJob> &jobs) {
   if (!ms || !args) return fail(TM_ERR_ARG, "null argument");
-  if (count == 0) return TM_OK;
   tm_machine *m0 = ms[0];
   for (uint32_t i = 0; i < count; i++) {
     int rc = validate_train(ms[i], &args[i]);
@@ -976,8 +1006,7 @@ static int train_batch_impl(tm_machine *const *ms, const tm_train_args *args, ui
     for (uint32_t k = 0; k < i; k++)
       if (ms[k] == ms[i]) return fail(TM_ERR_ARG, "train_batch: machine listed twice");
   }
-  DevGuard g(m0->device);
-  std::vector<TrainJob> jobs(count);
+  jobs.assign(count, TrainJob{});
   // identical inputs (same pointers, layout and size) are staged once
   std::vector<int> same_x(count, -1);
   for (uint32_t i = 0; i < count; i++) {
@@ -1024,6 +1053,19 @@ static int train_batch_impl(tm_machine *const *ms, const tm_train_args *args, ui
     if (e != cudaSuccess) return fail(TM_ERR_CUDA, "setup: %s", cudaGetErrorString(e));
     note_launch(m0, 1);
   }
+  return TM_OK;
+}
+
+static int train_batch_impl(tm_machine *const *ms, const tm_train_args *args, uint32_t count,
+                            tm_batch_epoch_cb each, void *user) {
+  if (!ms || !args) return fail(TM_ERR_ARG, "null argument");
+  if (count == 0) return TM_OK;
+  if (!ms[0]) return fail(TM_ERR_ARG, "null machine");
+  tm_machine *m0 = ms[0];
+  DevGuard g(m0->device);
+  std::vector<TrainJob> jobs;
+  int src = stage_batch(ms, args, count, jobs);
+  if (src) return src;
   uint32_t E = 0;
   uint64_t maxn = 1;
   for (uint32_t i = 0; i < count; i++) {
@@ -1060,6 +1102,389 @@ static int train_batch_impl(tm_machine *const *ms, const tm_train_args *args, ui
     if (rc) return rc;
   }
   return TM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Device-resident search round: the trials of one round of the reference's
+// search (optimize.lua:424-471), each with train_tm's per-epoch logic
+// (optimize.lua:586-653), for all machines at once.  One epoch is one CUDA
+// graph -- the epoch orders, the fused train kernel over every live
+// machine's units, literal counts, predict of the holdout for every machine
+// (k_predict_multi), the scores and early-stop decisions
+// (k_search_score), the checkpoint copies, the epoch counter and a copy of
+// the per-machine states to pinned host memory -- replayed once per epoch
+// with one host synchronisation.  Every kernel reads the machine's `live`
+// flag, so stopped machines drop out of the replays without a new graph.
+// ---------------------------------------------------------------------------
+static int search_round(tm_machine *const *ms, const tm_train_args *args, uint32_t count,
+                        const tm_search_args *sa) {
+  tm_machine *m0 = ms[0];
+  const int32_t type = m0->type;
+  const uint64_t nt = sa->test_samples;
+  if (nt == 0 || nt >= (1ull << 31)) return fail(TM_ERR_ARG, "search: test_samples out of range");
+  if (!sa->test_problems && !sa->test_each)
+    return fail(TM_ERR_ARG, "search: test problems missing");
+  if (type == TM_CLASSIFIER) {
+    if (sa->metric != TM_METRIC_F1 && sa->metric != TM_METRIC_ACCURACY)
+      return fail(TM_ERR_ARG, "search: classifiers are scored by TM_METRIC_F1 or TM_METRIC_ACCURACY");
+    if (!sa->test_solutions) return fail(TM_ERR_ARG, "search: test solutions missing");
+  } else {
+    if (sa->metric != TM_METRIC_HAMMING)
+      return fail(TM_ERR_ARG, "search: encoders are scored by TM_METRIC_HAMMING");
+    if (!sa->test_codes) return fail(TM_ERR_ARG, "search: test codes missing");
+  }
+  uint32_t E = 0, maxC = 1;
+  for (uint32_t i = 0; i < count; i++) {
+    tm_machine *m = ms[i];
+    if (!m) return fail(TM_ERR_ARG, "null machine");
+    if (m->type != type) return fail(TM_ERR_ARG, "search: classifiers and encoders mixed");
+    if (type == TM_ENCODER && m->classes != m0->classes)
+      return fail(TM_ERR_ARG, "search: encoders of different hidden sizes");
+    if (m->classes > TM_SEARCH_MAX_CLASSES)
+      return fail(TM_ERR_ARG, "search: more than %u classes", TM_SEARCH_MAX_CLASSES);
+    if (m->individualized && !sa->test_dim_offsets)
+      return fail(TM_ERR_ARG, "search: test dim_offsets missing");
+    if (sa->test_each && !sa->test_each[i] && !sa->test_problems)
+      return fail(TM_ERR_ARG, "search: test problems of machine %u missing", i);
+    E = std::max(E, args[i].iterations);
+    maxC = std::max(maxC, m->classes);
+  }
+  std::vector<TrainJob> jobs;
+  int rc = stage_batch(ms, args, count, jobs);
+  if (rc) return rc;
+  cudaStream_t st = m0->st;
+  const uint32_t Es = std::max<uint32_t>(E, 1);
+  // ---- holdout: truth once, padded rows per machine ------------------------
+  const uint64_t tb = type == TM_CLASSIFIER ? nt * 8 : nt * m0->class_chunks;
+  const int64_t *d_lab = nullptr;
+  const uint8_t *d_cod = nullptr;
+  if (sa->on_device) {
+    d_lab = sa->test_solutions;
+    d_cod = sa->test_codes;
+  } else {
+    CK(m0->search_truth.ensure(tb));
+    CK(cudaMemcpyAsync(m0->search_truth.p,
+                       type == TM_CLASSIFIER ? (const void *)sa->test_solutions
+                                             : (const void *)sa->test_codes,
+                       tb, cudaMemcpyHostToDevice, st));
+    if (type == TM_CLASSIFIER) d_lab = m0->search_truth.as<int64_t>();
+    else d_cod = m0->search_truth.as<uint8_t>();
+  }
+  for (uint32_t i = 0; i < count; i++) {
+    tm_machine *m = ms[i];
+    std::vector<ClassDev> tcls;
+    const uint8_t *tp = sa->test_each && sa->test_each[i] ? sa->test_each[i] : sa->test_problems;
+    cudaStream_t keep = m->st;
+    m->st = st;
+    rc = stage_rows(m, m->x, tp, sa->test_dim_offsets, nt, sa->on_device != 0, tcls);
+    if (!rc) rc = upload_cls(m, m->d_cls, tcls);
+    m->st = keep;
+    if (rc) return rc;
+    CK(m->sums.ensure(nt * m->classes * 4));
+    CK(cudaMemsetAsync(m->sums.p, 0, nt * m->classes * 4, st));
+    if (sa->patience) CK(m->ckpt.ensure(std::max<uint64_t>(m->act_words, 4) * 4));
+  }
+  // ---- device tables ---------------------------------------------------------
+  auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
+  const size_t o_scores = al(count * sizeof(SearchState));
+  const size_t o_pj = al(o_scores + (size_t)count * Es * 8);
+  const size_t o_pjf = al(o_pj + count * sizeof(PredictJob));
+  const size_t o_lj = al(o_pjf + count * sizeof(PredictJob));
+  const size_t o_ljf = al(o_lj + count * sizeof(LitsJob));
+  const size_t o_sj = al(o_ljf + count * sizeof(LitsJob));
+  const size_t o_cj = al(o_sj + count * sizeof(ScoreJob));
+  const size_t o_rj = al(o_cj + count * sizeof(CopyJob));
+  const size_t o_ctr = al(o_rj + count * sizeof(CopyJob));
+  CK(m0->search.ensure(o_ctr + 256));
+  uint8_t *base = m0->search.as<uint8_t>();
+  SearchState *d_state = (SearchState *)base;
+  double *d_scores = (double *)(base + o_scores);
+  // [0] epoch, [2] status bits of the train kernel, [4..5] its active steps
+  uint32_t *d_epoch = (uint32_t *)(base + o_ctr), *d_err = d_epoch + 2;
+  std::vector<SearchState> hs(count);
+  std::vector<PredictJob> pj(count), pjf(count);
+  std::vector<LitsJob> lj(count), ljf(count);
+  std::vector<ScoreJob> sj(count);
+  std::vector<CopyJob> cj(count), rj(count);
+  uint32_t tiles = 0;
+  for (uint32_t i = 0; i < count; i++) {
+    tm_machine *m = ms[i];
+    SearchState &S = hs[i];
+    S = SearchState{};
+    S.live = args[i].iterations > 0 && args[i].samples > 0 ? 1u : 0u;
+    S.patience = sa->patience;
+    S.iterations = args[i].iterations;
+    S.best = -INFINITY;
+    S.last = -INFINITY;
+    S.tolerance = sa->tolerance;
+    PredictJob &P = pj[i];
+    P = PredictJob{};
+    P.act = m->d_act;
+    P.lits = m->d_lits;
+    P.cls = m->d_cls;
+    P.x = m->x.as<uint32_t>();
+    P.sums = m->sums.as<int32_t>();
+    P.gate = &d_state[i].live;
+    P.clauses = m->clauses;
+    P.tol = m->tol;
+    P.n = (uint32_t)nt;
+    P.classes = m->classes;
+    P.tile0 = tiles;
+    tiles += predict_job_tiles((uint32_t)nt, m->classes, m->clauses, &P.stiles, &P.tpc);
+    pjf[i] = P;
+    pjf[i].gate = &d_state[i].has_ckpt;
+    lj[i] = LitsJob{m->d_act, m->d_cls, m->d_lits, &d_state[i].live, m->classes, m->clauses};
+    ljf[i] = lj[i];
+    ljf[i].gate = &d_state[i].has_ckpt;
+    sj[i] = ScoreJob{m->sums.as<int32_t>(), d_lab, d_cod, (uint32_t)nt, m->classes,
+                     (uint32_t)type, (uint32_t)sa->metric};
+    const uint64_t aw = (m->act_words + 3) & ~3ull;
+    cj[i] = CopyJob{m->d_act, sa->patience ? m->ckpt.as<uint32_t>() : nullptr, aw,
+                    sa->patience ? &d_state[i].ckpt_now : nullptr};
+    rj[i] = CopyJob{sa->patience ? m->ckpt.as<uint32_t>() : nullptr, m->d_act, aw,
+                    sa->patience ? &d_state[i].has_ckpt : nullptr};
+  }
+  CK(cudaMemcpyAsync(d_state, hs.data(), count * sizeof(SearchState), cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(d_scores, 0xFF, (size_t)count * Es * 8, st));  // NaN
+  CK(cudaMemcpyAsync(base + o_pj, pj.data(), count * sizeof(PredictJob), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(base + o_pjf, pjf.data(), count * sizeof(PredictJob), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(base + o_lj, lj.data(), count * sizeof(LitsJob), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(base + o_ljf, ljf.data(), count * sizeof(LitsJob), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(base + o_sj, sj.data(), count * sizeof(ScoreJob), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(base + o_cj, cj.data(), count * sizeof(CopyJob), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(base + o_rj, rj.data(), count * sizeof(CopyJob), cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(d_epoch, 0, 32, st));
+  // ---- one epoch's train launch ----------------------------------------------
+  std::map<std::pair<uint64_t, uint64_t>, uint64_t> pidx;
+  uint64_t pwords = 0;
+  std::vector<uint64_t> joff(count);
+  uint32_t maxn = 1;
+  for (uint32_t i = 0; i < count; i++) {
+    auto key = std::make_pair(jobs[i].seed, (uint64_t)args[i].samples);
+    auto it = pidx.find(key);
+    if (it == pidx.end()) {
+      pidx[key] = pwords;
+      joff[i] = pwords;
+      pwords += args[i].samples;
+    } else {
+      joff[i] = it->second;
+    }
+    maxn = std::max<uint32_t>(maxn, (uint32_t)args[i].samples);
+  }
+  CK(m0->perm.ensure(std::max<uint64_t>(pwords, 4) * 4));
+  CK(m0->perm_scratch.ensure(perm_scratch_bytes(maxn)));
+  std::vector<TrainDev> td;
+  std::vector<WorkItem> work;
+  TrainShape sh{};
+  build_tables(jobs, 0, 1, m0, joff, td, work, sh);
+  for (uint32_t i = 0; i < count; i++) {
+    td[i].gate = &d_state[i].live;
+    td[i].epoch_dev = d_epoch;
+  }
+  // epoch 0's orders: the tuner's trial launches read them (the graph
+  // rebuilds them for every epoch from the device epoch counter)
+  for (auto &kv : pidx)
+    CK(launch_perm(kv.first.first, 0, (uint32_t)kv.first.second,
+                   m0->perm.as<uint32_t>() + kv.second, m0->perm_scratch.p, m0->perm_scratch.cap,
+                   st, d_epoch));
+  TrainPlan plan;
+  bool tuned = false;
+  if (!work.empty()) {
+    // trial launches of the tuner also read the gates and the epoch counter
+    CK(cudaStreamSynchronize(st));
+    rc = choose_plan(jobs, td, work, sh, 0, m0, plan, tuned);
+    if (rc) return rc;
+    m0->last_mode = plan.mode;
+    m0->stats.train_mode = plan.mode;
+    m0->stats.train_autotuned = tuned ? 1 : 0;
+    m0->stats.train_cpw = plan.cpw;
+  }
+  const size_t tbytes = td.size() * sizeof(TrainDev);
+  const size_t off_w = (tbytes + 255) & ~(size_t)255;
+  const size_t off_c = (off_w + work.size() * sizeof(WorkItem) + 255) & ~(size_t)255;
+  CK(m0->tdev.ensure(off_c + 256));
+  uint8_t *tbase = m0->tdev.as<uint8_t>();
+  CK(cudaMemcpyAsync(tbase, td.data(), tbytes, cudaMemcpyHostToDevice, st));
+  if (!work.empty())
+    CK(cudaMemcpyAsync(tbase + off_w, work.data(), work.size() * sizeof(WorkItem),
+                       cudaMemcpyHostToDevice, st));
+  uint32_t *counter = (uint32_t *)(tbase + off_c);
+  TrainSmem lay = plan.lay;
+  lay.wait_limit = m0->row_wait;
+  // ---- pinned mirror of the states, events around the train kernel -----------
+  SearchState *h_state = nullptr;
+  CK(cudaHostAlloc((void **)&h_state, count * sizeof(SearchState) + 64, cudaHostAllocDefault));
+  uint32_t *h_err = (uint32_t *)(h_state + count);
+  const bool timing = m0->timing && m0->ev0 && m0->ev1;
+  cudaEvent_t tk0 = nullptr, tk1 = nullptr;
+  if (timing && (cudaEventCreate(&tk0) != cudaSuccess || cudaEventCreate(&tk1) != cudaSuccess)) {
+    cudaFreeHost(h_state);
+    return fail(TM_ERR_CUDA, "search: event creation failed");
+  }
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  auto drop = [&]() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+    if (tk0) cudaEventDestroy(tk0);
+    if (tk1) cudaEventDestroy(tk1);
+    tk0 = tk1 = nullptr;
+    if (h_state) cudaFreeHost(h_state);
+    h_state = nullptr;
+  };
+  // ---- capture one epoch ------------------------------------------------------
+  uint64_t launches = 0;
+  cudaError_t ce = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+  if (ce == cudaSuccess) {
+    for (auto &kv : pidx) {
+      if (ce != cudaSuccess) break;
+      ce = launch_perm(kv.first.first, 0, (uint32_t)kv.first.second,
+                       m0->perm.as<uint32_t>() + kv.second, m0->perm_scratch.p,
+                       m0->perm_scratch.cap, st, d_epoch);
+      launches += 1 + kSortKernels;
+    }
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(counter, 0, 4, st);
+    if (ce == cudaSuccess && timing) ce = cudaEventRecord(tk0, st);
+    if (ce == cudaSuccess && !work.empty()) {
+      if (plan.mode == TM_MODE_WARP)
+        ce = launch_train_warp((const TrainDev *)tbase, (const WorkItem *)(tbase + off_w),
+                               (uint32_t)work.size(), counter, 0, 1, sh.Wpmax, sh.Bmin, sh.Bmax,
+                               sh.smax, plan.grid, st, (unsigned long long *)(d_err + 2));
+      else
+        ce = launch_train((const TrainDev *)tbase, (const WorkItem *)(tbase + off_w),
+                          (uint32_t)work.size(), counter, 0, 1, lay, plan.mode, sh.Bmin, sh.Bmax,
+                          plan.cpw, plan.grid, d_err, st);
+      launches++;
+    }
+    if (ce == cudaSuccess && timing) ce = cudaEventRecord(tk1, st);
+    if (ce == cudaSuccess)
+      ce = launch_lits_multi((const LitsJob *)(base + o_lj), count, maxC, st);
+    if (ce == cudaSuccess)
+      ce = launch_predict_multi((const PredictJob *)(base + o_pj), count, tiles, st);
+    if (ce == cudaSuccess)
+      ce = launch_search_score((const ScoreJob *)(base + o_sj), d_state, d_scores, Es, count,
+                               maxC, 0, st);
+    if (ce == cudaSuccess && sa->patience)
+      ce = launch_copy_multi((const CopyJob *)(base + o_cj), count, st);
+    if (ce == cudaSuccess) ce = launch_tick(d_epoch, st);
+    if (ce == cudaSuccess)
+      ce = cudaMemcpyAsync(h_state, d_state, count * sizeof(SearchState), cudaMemcpyDeviceToHost,
+                           st);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(h_err, d_err, 4, cudaMemcpyDeviceToHost, st);
+    launches += 4 + (sa->patience ? 1 : 0);
+    cudaError_t ee = cudaStreamEndCapture(st, &graph);
+    if (ce == cudaSuccess) ce = ee;
+  }
+  if (ce == cudaSuccess) ce = cudaGraphInstantiate(&exec, graph, 0);
+  if (ce != cudaSuccess) {
+    drop();
+    return fail(TM_ERR_CUDA, "search: epoch graph: %s", cudaGetErrorString(ce));
+  }
+  // ---- epochs -----------------------------------------------------------------
+  std::vector<double> last(count);
+  std::vector<int32_t> live(count), stop(count);
+  for (uint32_t e = 0; e < E; e++) {
+    ce = timing ? cudaEventRecord(m0->ev0, st) : cudaSuccess;
+    if (ce == cudaSuccess) ce = cudaGraphLaunch(exec, st);
+    if (ce == cudaSuccess && timing) ce = cudaEventRecord(m0->ev1, st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+    if (ce != cudaSuccess) {
+      drop();
+      return fail(TM_ERR_CUDA, "search: epoch %u: %s", e + 1, cudaGetErrorString(ce));
+    }
+    if (timing) {
+      float ms = 0, tms = 0;
+      if (cudaEventElapsedTime(&ms, m0->ev0, m0->ev1) == cudaSuccess) m0->stats.search_epoch_ms += ms;
+      if (!work.empty() && cudaEventElapsedTime(&tms, tk0, tk1) == cudaSuccess) {
+        m0->stats.search_train_ms += tms;
+        m0->stats.train_kernel_ms += tms;
+      }
+      m0->stats.search_epochs++;
+    }
+    m0->stats.kernel_launches += launches;
+    m0->stats.train_launches += work.empty() ? 0 : 1;
+    if (*h_err) {
+      const uint32_t he = *h_err;
+      drop();
+      return fail(TM_ERR_DEVICE, "train: a sample copy did not complete (status %u)", he);
+    }
+    bool any = false;
+    for (uint32_t i = 0; i < count; i++) {
+      live[i] = (int32_t)h_state[i].live;
+      last[i] = h_state[i].epochs_run == e + 1 ? h_state[i].last : NAN;
+      stop[i] = 0;
+    }
+    if (sa->each) {
+      const int all = sa->each(sa->each_user, e + 1, last.data(), live.data(), stop.data(), count);
+      for (uint32_t i = 0; i < count; i++) {
+        if ((all || stop[i]) && live[i]) {
+          static const uint32_t zero = 0;
+          ce = cudaMemcpyAsync(&d_state[i].live, &zero, 4, cudaMemcpyHostToDevice, st);
+          if (ce != cudaSuccess) {
+            drop();
+            return fail(TM_ERR_CUDA, "search: %s", cudaGetErrorString(ce));
+          }
+          live[i] = 0;
+        }
+      }
+      ce = cudaStreamSynchronize(st);
+      if (ce != cudaSuccess) {
+        drop();
+        return fail(TM_ERR_CUDA, "search: %s", cudaGetErrorString(ce));
+      }
+    }
+    for (uint32_t i = 0; i < count; i++) any = any || live[i];
+    if (!any) break;
+  }
+  drop();
+  // ---- restore each machine's best checkpoint and score it ---------------------
+  if (sa->patience) {
+    CK(launch_copy_multi((const CopyJob *)(base + o_rj), count, st));
+    CK(launch_lits_multi((const LitsJob *)(base + o_ljf), count, maxC, st));
+    CK(launch_predict_multi((const PredictJob *)(base + o_pjf), count, tiles, st));
+    CK(launch_search_score((const ScoreJob *)(base + o_sj), d_state, d_scores, Es, count, maxC, 1,
+                           st));
+    m0->stats.kernel_launches += 4;
+  }
+  std::vector<double> scores((size_t)count * Es);
+  uint32_t hc[4] = {0, 0, 0, 0};
+  CK(cudaMemcpyAsync(hc, d_err, 16, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(hs.data(), d_state, count * sizeof(SearchState), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(scores.data(), d_scores, scores.size() * 8, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  m0->stats.train_active_pairs += (uint64_t)hc[2] | ((uint64_t)hc[3] << 32);
+  for (uint32_t i = 0; i < count; i++) {
+    if (sa->final_scores) sa->final_scores[i] = hs[i].last;
+    if (sa->best_scores) sa->best_scores[i] = hs[i].best;
+    if (sa->epochs_run) sa->epochs_run[i] = hs[i].epochs_run;
+    if (sa->best_epochs) sa->best_epochs[i] = hs[i].best_epoch;
+    if (sa->scores)
+      for (uint32_t e = 0; e < E; e++) sa->scores[(size_t)i * E + e] = scores[(size_t)i * Es + e];
+    tm_machine *m = ms[i];
+    m0->stats.train_unit_steps +=
+        (uint64_t)m->classes * m->clause_chunks * args[i].samples * hs[i].epochs_run;
+    if (m->individualized) {
+      rc = upload_cls(m, m->d_cls, m->cls);
+      if (rc) return rc;
+    }
+  }
+  CK(cudaStreamSynchronize(st));
+  for (uint32_t i = 0; i < count; i++) {
+    rc = finish_train(ms[i]);
+    if (rc) return rc;
+  }
+  return TM_OK;
+}
+
+extern "C" int tm_train_batch_search(tm_machine *const *ms, const tm_train_args *args,
+                                     uint32_t count, const tm_search_args *sa) {
+  if (!ms || !args || !sa) return fail(TM_ERR_ARG, "null argument");
+  if (count == 0) return TM_OK;
+  if (!ms[0]) return fail(TM_ERR_ARG, "null machine");
+  DevGuard g(ms[0]->device);
+  return search_round(ms, args, count, sa);
 }
 
 // ---------------------------------------------------------------------------

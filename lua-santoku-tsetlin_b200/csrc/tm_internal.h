@@ -49,6 +49,8 @@ struct TrainDev {
   uint32_t code_bytes;
   uint32_t epochs;          // epochs this machine trains in this launch group
   uint32_t epoch_base;      // draw-contract epoch index of local epoch 0
+  const uint32_t *gate;     // optional: the machine's units are skipped while *gate == 0
+  const uint32_t *epoch_dev;  // optional: added to epoch_base (a graph replayed per epoch)
 };
 
 struct WorkItem {
@@ -96,7 +98,8 @@ cudaError_t launch_labels(const int64_t *src, int32_t *dst, uint64_t n, cudaStre
 cudaError_t launch_setup(uint32_t *act, uint32_t *cnt, const ClassDev *cls, uint32_t classes,
                          uint32_t clauses, uint32_t B, uint64_t act_words, cudaStream_t st);
 cudaError_t launch_perm(uint64_t seed, uint32_t epoch, uint32_t n, uint32_t *out,
-                        void *scratch, size_t scratch_bytes, cudaStream_t st);
+                        void *scratch, size_t scratch_bytes, cudaStream_t st,
+                        const uint32_t *epoch_dev = nullptr);
 size_t perm_scratch_bytes(uint32_t n);
 // k_train variants: automata in shared memory (one CTA per unit), in global
 // memory (one CTA per unit), or split over a 2-CTA cluster in shared memory.
@@ -117,7 +120,10 @@ int train_warp_occupancy(uint32_t Wpmax, uint32_t Bmin, uint32_t Bmax, uint32_t 
 cudaError_t launch_train_warp(const TrainDev *machines, const WorkItem *work, uint32_t nwork,
                               uint32_t *counter, uint32_t e_begin, uint32_t e_end, uint32_t Wpmax,
                               uint32_t Bmin, uint32_t Bmax, uint32_t smax, int grid,
-                              cudaStream_t st);
+                              cudaStream_t st, unsigned long long *pairs);
+// The fused train kernels report through err[0] (status bits) and
+// err[2..3], a 64-bit count of active (unit, sample) steps -- the samples
+// each unit actually trained on after negative sampling.
 cudaError_t launch_lits(const uint32_t *act, const ClassDev *cls, uint32_t classes,
                         uint32_t clauses, int32_t *lits, cudaStream_t st);
 cudaError_t launch_predict(const uint32_t *act, const int32_t *lits, const ClassDev *cls,
@@ -155,6 +161,58 @@ constexpr uint32_t TM_SMALL_N_MAX = 32;
 cudaError_t launch_lits_gated(const uint32_t *act, const ClassDev *cls, uint32_t classes,
                               uint32_t clauses, int32_t *lits, const uint32_t *gate,
                               cudaStream_t st);
+
+// ---- device-resident search round (tm_train_batch_search) ----------------
+// Per-machine state of the round, kept on the device and read by the host
+// once per epoch.  The epoch logic of the reference's train_tm
+// (optimize.lua:599-625): score, best + tolerance, patience, checkpoint.
+struct SearchState {
+  uint32_t live;        // still training: gates its units, its metric and its checkpoint
+  uint32_t since;       // epochs since the best score improved
+  uint32_t ckpt_now;    // the epoch just scored improved: checkpoint the actions
+  uint32_t has_ckpt;    // a checkpoint exists: restored at the end
+  uint32_t epochs_run;
+  uint32_t best_epoch;  // 1-based epoch of the best score
+  uint32_t patience;    // 0: no early stop and no checkpoint
+  uint32_t iterations;
+  double best;          // -inf before the first epoch
+  double last;          // last score (after the final restore: the restored machine's)
+  double tolerance;
+};
+
+// Scoring of one machine's vote sums against the truth.
+struct ScoreJob {
+  int32_t *sums;           // n x classes vote sums; zeroed once scored
+  const int64_t *labels;   // classifier truth
+  const uint8_t *codes;    // encoder truth codes, ceil(classes / 8) bytes per sample
+  uint32_t n, classes, type, metric;
+};
+
+// Literal counts of one machine (k_lits), skipped while *gate == 0.
+struct LitsJob {
+  const uint32_t *act;
+  const ClassDev *cls;
+  int32_t *lits;
+  const uint32_t *gate;
+  uint32_t classes, clauses;
+};
+
+// A word copy run while *flag != 0 (checkpoint and restore of actions).
+struct CopyJob {
+  const uint32_t *src;
+  uint32_t *dst;
+  uint64_t words;  // a multiple of 4
+  const uint32_t *flag;
+};
+
+constexpr uint32_t TM_SEARCH_MAX_CLASSES = 4000;  // counts of a score in shared memory
+cudaError_t launch_lits_multi(const LitsJob *jobs, uint32_t njobs, uint32_t max_classes,
+                              cudaStream_t st);
+cudaError_t launch_search_score(const ScoreJob *jobs, SearchState *state, double *scores,
+                                uint32_t max_epochs, uint32_t njobs, uint32_t max_classes,
+                                int final_pass, cudaStream_t st);
+cudaError_t launch_copy_multi(const CopyJob *jobs, uint32_t njobs, cudaStream_t st);
+cudaError_t launch_tick(uint32_t *counter, cudaStream_t st);
 
 // Read-only view of a resident dense machine for the server (tm_serve.cpp).
 struct MachineView {

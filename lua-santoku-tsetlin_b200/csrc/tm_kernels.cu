@@ -159,7 +159,10 @@ cudaError_t launch_setup(uint32_t *act, uint32_t *cnt, const ClassDev *cls, uint
 // Epoch order: sort samples by a 64-bit Philox key (stable, ties by index).
 // ---------------------------------------------------------------------------
 __global__ void k_perm_keys(uint64_t seed, uint32_t epoch, uint32_t n, uint64_t *keys,
-                            uint32_t *idx) {
+                            uint32_t *idx, const uint32_t *epoch_dev) {
+  // epoch_dev (optional): the epoch is read from device memory, so that a
+  // captured graph builds the order of whatever epoch it is replayed for
+  if (epoch_dev) epoch += *epoch_dev;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     uint32_t o[4];
     philox(i, epoch, 0u, ST_PERM, seed, o);
@@ -178,7 +181,7 @@ size_t perm_scratch_bytes(uint32_t n) {
 }
 
 cudaError_t launch_perm(uint64_t seed, uint32_t epoch, uint32_t n, uint32_t *out, void *scratch,
-                        size_t scratch_bytes, cudaStream_t st) {
+                        size_t scratch_bytes, cudaStream_t st, const uint32_t *epoch_dev) {
   if (!n) return cudaSuccess;
   size_t temp = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, temp, (uint64_t *)nullptr, (uint64_t *)nullptr,
@@ -193,7 +196,7 @@ cudaError_t launch_perm(uint64_t seed, uint32_t epoch, uint32_t n, uint32_t *out
   void *tmp = p;
   if ((size_t)(p - (uint8_t *)scratch) + temp > scratch_bytes) return cudaErrorInvalidValue;
   const int blocks = (int)std::min<uint32_t>((n + 255) / 256, 148u * 8);
-  k_perm_keys<<<blocks, 256, 0, st>>>(seed, epoch, n, k_in, v_in);
+  k_perm_keys<<<blocks, 256, 0, st>>>(seed, epoch, n, k_in, v_in, epoch_dev);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   return cub::DeviceRadixSort::SortPairs(tmp, temp, k_in, k_out, v_in, out, (int)n, 0, 64, st);
@@ -537,6 +540,7 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
   uint32_t gs = 0;  // rows issued to the ring so far (slot/phase of row k: k % R, k / R)
   uint32_t issued = 0;
   bool aborted = false;
+  uint64_t pairs = 0;  // active (unit, sample) steps of this CTA, reported at exit
 
   while (true) {
     if (tid == 0 && rank == 0) {
@@ -549,6 +553,12 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
     if (u >= nwork) break;
     const WorkItem wi = work[u];
     const TrainDev &M = machines[wi.m];
+    if (M.gate && *M.gate == 0) {
+      // a machine that stopped (search early stop): its units are skipped;
+      // every thread has read misc[0] before thread 0 fetches the next unit
+      unit_sync<PAIR>();
+      continue;
+    }
     const ClassDev C = M.cls[wi.h];
     const uint32_t m = EXACT ? (uint32_t)BM : M.B - 1;
     const uint32_t Wp = C.Wp, W = C.W;
@@ -587,11 +597,12 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
     const uint32_t T = M.T;
     const uint64_t T2 = 2ull * T;
     const uint32_t ep_end = e_end < M.epochs ? e_end : M.epochs;
+    const uint32_t eb = M.epoch_base + (M.epoch_dev ? *M.epoch_dev : 0u);
     const uint32_t row_bytes = Wp * 4;
     const uint32_t *xbase = M.x + C.x_off;
 
     for (uint32_t e = e_begin; e < ep_end && !aborted; e++) {
-      const uint32_t ee = M.epoch_base + e;
+      const uint32_t ee = eb + e;
       const uint32_t *perm = M.perm + (uint64_t)(e - e_begin) * M.n;
       for (uint32_t base = 0; base < M.n && !aborted; base += blockDim.x) {
         // ---- batch phase: skip decisions and chance draws ----------------
@@ -922,6 +933,7 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
           __syncthreads();
         }
         if (!aborted) gs += nact;
+        pairs += nact;
         unit_sync<PAIR>();
       }
     }
@@ -943,6 +955,7 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
     // wait (bounded) for this CTA's copies still in flight before exiting
     for (uint32_t k = gs; k < issued; k++) mbar_wait(&bars[k % TM_RING], (k / TM_RING) & 1u);
   }
+  if (tid == 0 && rank == 0 && pairs) atomicAdd((unsigned long long *)(err + 2), pairs);
   // no CTA of a pair leaves while its peer may still write to its shared memory
   unit_sync<PAIR>();
 }
@@ -963,7 +976,8 @@ template <int BM, bool EXACT = false>
 __global__ void __launch_bounds__(TM_WARP_THREADS)
     k_train_warp(const TrainDev *__restrict__ machines, const WorkItem *__restrict__ work,
                  uint32_t nwork, uint32_t *__restrict__ counter, uint32_t e_begin, uint32_t e_end,
-                 uint32_t slice_words, uint32_t ib_words, uint32_t ovf_cap, uint32_t stride) {
+                 uint32_t slice_words, uint32_t ib_words, uint32_t ovf_cap, uint32_t stride,
+                 unsigned long long *__restrict__ pairs) {
   extern __shared__ __align__(128) uint8_t smem[];
   const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   // stride: words per warp, a multiple of 32 (16-byte alignment of every slice)
@@ -973,6 +987,7 @@ __global__ void __launch_bounds__(TM_WARP_THREADS)
   for (uint32_t i = lane; i < 2 * ib_words; i += 32) lev0[i] = 0;
   if (lane == 0) cnt_ovf[0] = 0;
   __syncwarp();
+  uint64_t npairs = 0;  // active (unit, sample) steps of this warp, reported at exit
   while (true) {
     uint32_t u = 0;
     if (lane == 0) u = atomicAdd(counter, 1u);
@@ -980,6 +995,7 @@ __global__ void __launch_bounds__(TM_WARP_THREADS)
     if (u >= nwork) break;
     const WorkItem wi = work[u];
     const TrainDev &M = machines[wi.m];
+    if (M.gate && *M.gate == 0) continue;  // a stopped machine's unit
     const ClassDev C = M.cls[wi.h];
     const uint32_t m = EXACT ? (uint32_t)BM : M.B - 1;
     const uint32_t Wp = C.Wp, W = C.W;
@@ -993,6 +1009,7 @@ __global__ void __launch_bounds__(TM_WARP_THREADS)
     const uint32_t T = M.T;
     const uint64_t T2 = 2ull * T;
     const uint32_t ep_end = e_end < M.epochs ? e_end : M.epochs;
+    const uint32_t eb = M.epoch_base + (M.epoch_dev ? *M.epoch_dev : 0u);
     const uint32_t *xbase = M.x + C.x_off;
     const uint32_t w0 = lane, w1 = lane + 32;
     const uint32_t vm0 = word_mask(w0, W, C.vmask), vm1 = word_mask(w1, W, C.vmask);
@@ -1002,7 +1019,7 @@ __global__ void __launch_bounds__(TM_WARP_THREADS)
     uint32_t dirty = 0xFFu;
 
     for (uint32_t e = e_begin; e < ep_end; e++) {
-      const uint32_t ee = M.epoch_base + e;
+      const uint32_t ee = eb + e;
       const uint32_t *perm = M.perm + (uint64_t)(e - e_begin) * M.n;
       for (uint32_t base = 0; base < M.n; base += 32) {
         const uint32_t i = base + lane;
@@ -1029,6 +1046,7 @@ __global__ void __launch_bounds__(TM_WARP_THREADS)
           }
         }
         uint32_t bal = __ballot_sync(0xFFFFFFFFu, live);
+        npairs += __popc(bal);
         if (!bal) continue;
         // row of the first surviving sample
         uint32_t src = __ffs(bal) - 1;
@@ -1181,6 +1199,7 @@ __global__ void __launch_bounds__(TM_WARP_THREADS)
     for (uint32_t i = lane; i < 2 * m * Wp; i += 32) ((uint4 *)gcnt)[i] = ((const uint4 *)cnt)[i];
     __syncwarp();
   }
+  if (lane == 0 && pairs && npairs) atomicAdd(pairs, (unsigned long long)npairs);
 }
 
 // shared memory per warp of k_train_warp, in words (a multiple of 32)
@@ -1208,17 +1227,17 @@ int train_warp_occupancy(uint32_t Wpmax, uint32_t Bmin, uint32_t Bmax, uint32_t 
 cudaError_t launch_train_warp(const TrainDev *machines, const WorkItem *work, uint32_t nwork,
                               uint32_t *counter, uint32_t e_begin, uint32_t e_end, uint32_t Wpmax,
                               uint32_t Bmin, uint32_t Bmax, uint32_t smax, int grid,
-                              cudaStream_t st) {
+                              cudaStream_t st, unsigned long long *pairs) {
   const uint32_t ovf_cap = smax / 4 > 0 ? smax / 4 : 1;
   const uint32_t slice = 8 * Bmax * Wpmax;
   const uint32_t stride = warp_slice_words(Wpmax, Bmax, Wpmax, ovf_cap);
   const size_t bytes = (size_t)(TM_WARP_THREADS / 32) * stride * 4;
   if (Bmin == 8 && Bmax == 8)
     k_train_warp<7, true><<<grid, TM_WARP_THREADS, bytes, st>>>(
-        machines, work, nwork, counter, e_begin, e_end, slice, Wpmax, ovf_cap, stride);
+        machines, work, nwork, counter, e_begin, e_end, slice, Wpmax, ovf_cap, stride, pairs);
   else
     k_train_warp<7, false><<<grid, TM_WARP_THREADS, bytes, st>>>(
-        machines, work, nwork, counter, e_begin, e_end, slice, Wpmax, ovf_cap, stride);
+        machines, work, nwork, counter, e_begin, e_end, slice, Wpmax, ovf_cap, stride, pairs);
   return cudaGetLastError();
 }
 

@@ -64,6 +64,25 @@ __global__ void k_class_counts(const int64_t *__restrict__ pred, const int64_t *
   }
 }
 
+}  // namespace
+
+namespace tmb {
+// Precision, recall and F1 of one class from its counts (evaluator
+// capi.c:155-160), with explicit round-to-nearest operations: no fused
+// multiply-add, so each operation rounds as in a plain IEEE evaluation of
+// the formula and the result equals the reference's double arithmetic.
+__device__ __forceinline__ void class_prf(unsigned long long t, unsigned long long f,
+                                          unsigned long long g, double &p, double &r,
+                                          double &f1) {
+  p = (t + f) > 0 ? __ddiv_rn((double)t, (double)(t + f)) : 0.0;
+  r = (t + g) > 0 ? __ddiv_rn((double)t, (double)(t + g)) : 0.0;
+  const double pr = __dadd_rn(p, r);
+  f1 = pr > 0 ? __ddiv_rn(__dmul_rn(__dmul_rn(2.0, p), r), pr) : 0.0;
+}
+}  // namespace tmb
+
+namespace {
+
 // capi.c:155-172 of the evaluator, in its order: out = [precision, recall,
 // f1 (macro), then per class precision, recall, f1]
 __global__ void k_class_finish(const unsigned long long *__restrict__ tp,
@@ -73,13 +92,8 @@ __global__ void k_class_finish(const unsigned long long *__restrict__ tp,
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   double pa = 0.0, ra = 0.0, fa = 0.0;
   for (uint32_t c = 0; c < classes; c++) {
-    const unsigned long long t = tp[c], f = fp[c], g = fn[c];
-    // explicit round-to-nearest operations: no fused multiply-add, so each
-    // operation rounds as in a plain IEEE evaluation of the formula
-    const double p = (t + f) > 0 ? __ddiv_rn((double)t, (double)(t + f)) : 0.0;
-    const double r = (t + g) > 0 ? __ddiv_rn((double)t, (double)(t + g)) : 0.0;
-    const double pr = __dadd_rn(p, r);
-    const double f1 = pr > 0 ? __ddiv_rn(__dmul_rn(__dmul_rn(2.0, p), r), pr) : 0.0;
+    double p, r, f1;
+    tmb::class_prf(tp[c], fp[c], fn[c], p, r, f1);
     out[3 + 3 * c] = p;
     out[3 + 3 * c + 1] = r;
     out[3 + 3 * c + 2] = f1;
@@ -263,6 +277,167 @@ int grid_for(uint64_t work) {
 }
 
 }  // namespace
+
+namespace tmb {
+
+// The score of one machine per CTA: predictions from the vote sums (argmax
+// with ties to the lowest class, capi.c:934-942, or code bits h = sum > 0,
+// capi.c:982-990), the evaluator's counts (class_accuracy,
+// evaluator/capi.c:141-153; encoding_accuracy, :520-535), then the metric
+// and the epoch logic of the reference's train_tm (optimize.lua:599-625):
+// a score above best + tolerance becomes the best (and is checkpointed when
+// patience > 0); `patience` epochs without one, or the last iteration,
+// stop the machine.  final_pass scores the machines holding a checkpoint
+// after the restore and only records the score.
+__global__ void k_search_score(const ScoreJob *__restrict__ jobs, SearchState *__restrict__ state,
+                               double *__restrict__ scores, uint32_t max_epochs, int final_pass) {
+  extern __shared__ uint32_t cnt[];
+  SearchState *S = state + blockIdx.x;
+  if (!(final_pass ? S->has_ckpt : S->live)) return;
+  const ScoreJob J = jobs[blockIdx.x];
+  const uint32_t C = J.classes, tid = threadIdx.x;
+  const uint32_t ncnt = J.type == 0 ? 3 * C : C;
+  for (uint32_t i = tid; i < ncnt; i += blockDim.x) cnt[i] = 0;
+  __syncthreads();
+  if (J.type == 0) {
+    for (uint32_t s = tid; s < J.n; s += blockDim.x) {
+      int32_t *r = J.sums + (uint64_t)s * C;
+      int32_t best = r[0];
+      uint32_t bc = 0;
+      r[0] = 0;
+      for (uint32_t h = 1; h < C; h++) {
+        const int32_t v = r[h];
+        r[h] = 0;
+        if (v > best) {
+          best = v;
+          bc = h;
+        }
+      }
+      const uint32_t yt = (uint32_t)J.labels[s];
+      if (yt >= C) continue;
+      if (bc == yt) {
+        atomicAdd(&cnt[yt], 1u);
+      } else {
+        atomicAdd(&cnt[C + bc], 1u);
+        atomicAdd(&cnt[2 * C + yt], 1u);
+      }
+    }
+  } else {
+    const uint32_t nb = (C + 7) >> 3;
+    for (uint32_t s = tid; s < J.n; s += blockDim.x) {
+      int32_t *r = J.sums + (uint64_t)s * C;
+      const uint8_t *code = J.codes + (uint64_t)s * nb;
+      for (uint32_t h = 0; h < C; h++) {
+        const uint32_t p = r[h] > 0 ? 1u : 0u;
+        r[h] = 0;
+        if (p != ((code[h >> 3] >> (h & 7)) & 1u)) atomicAdd(&cnt[h], 1u);
+      }
+    }
+  }
+  __syncthreads();
+  if (tid != 0) return;
+  double score;
+  if (J.type == 0 && J.metric == 0) {  // macro F1 (evaluator capi.c:155-172)
+    double fa = 0.0;
+    for (uint32_t c = 0; c < C; c++) {
+      double p, r, f1;
+      class_prf(cnt[c], cnt[C + c], cnt[2 * C + c], p, r, f1);
+      fa = __dadd_rn(fa, f1);
+    }
+    score = __ddiv_rn(fa, (double)C);
+  } else if (J.type == 0) {  // accuracy: correct / n
+    unsigned long long t = 0;
+    for (uint32_t c = 0; c < C; c++) t += cnt[c];
+    score = J.n ? __ddiv_rn((double)t, (double)J.n) : 0.0;
+  } else {  // mean_hamming = 1 - mean bit error rate (evaluator capi.c:557-566)
+    unsigned long long t = 0;
+    for (uint32_t h = 0; h < C; h++) t += cnt[h];
+    score = __dsub_rn(1.0, __ddiv_rn((double)t, (double)((uint64_t)J.n * C)));
+  }
+  if (final_pass) {
+    S->last = score;
+    return;
+  }
+  const uint32_t e = S->epochs_run;
+  if (scores && e < max_epochs) scores[(uint64_t)blockIdx.x * max_epochs + e] = score;
+  S->epochs_run = e + 1;
+  S->last = score;
+  if (score > __dadd_rn(S->best, S->tolerance)) {
+    S->best = score;
+    S->since = 0;
+    S->best_epoch = e + 1;
+    S->ckpt_now = S->patience ? 1u : 0u;
+    if (S->patience) S->has_ckpt = 1;
+  } else {
+    S->since++;
+    S->ckpt_now = 0;
+  }
+  if ((S->patience && S->since >= S->patience) || e + 1 >= S->iterations) S->live = 0;
+}
+
+cudaError_t launch_search_score(const ScoreJob *jobs, SearchState *state, double *scores,
+                                uint32_t max_epochs, uint32_t njobs, uint32_t max_classes,
+                                int final_pass, cudaStream_t st) {
+  if (!njobs) return cudaSuccess;
+  const size_t smem = (size_t)3 * max_classes * 4;
+  k_search_score<<<njobs, 256, smem, st>>>(jobs, state, scores, max_epochs, final_pass);
+  return cudaGetLastError();
+}
+
+// capi.c:103-108 literal counts for many machines: grid (64, classes, job)
+__global__ void k_lits_multi(const LitsJob *__restrict__ jobs) {
+  const LitsJob J = jobs[blockIdx.z];
+  if (J.gate && *J.gate == 0) return;
+  if (blockIdx.y >= J.classes) return;
+  const ClassDev C = J.cls[blockIdx.y];
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t c = warp; c < J.clauses; c += nw) {
+    const uint32_t *row = J.act + C.act_off + (uint64_t)c * C.Wp;
+    uint32_t l = 0;
+    for (uint32_t w = lane; w < C.W; w += 32) {
+      uint32_t a = row[w];
+      if (w + 1 == C.W) a &= C.emask;
+      l += __popc(a);
+    }
+    l = __reduce_add_sync(0xFFFFFFFFu, l);
+    if (lane == 0) J.lits[(uint64_t)blockIdx.y * J.clauses + c] = (int32_t)l;
+  }
+}
+
+cudaError_t launch_lits_multi(const LitsJob *jobs, uint32_t njobs, uint32_t max_classes,
+                              cudaStream_t st) {
+  if (!njobs || !max_classes) return cudaSuccess;
+  k_lits_multi<<<dim3(64, max_classes, njobs), 256, 0, st>>>(jobs);
+  return cudaGetLastError();
+}
+
+// grid (blocks, job): 16-byte copies while the job's flag is set
+__global__ void k_copy_multi(const CopyJob *__restrict__ jobs) {
+  const CopyJob J = jobs[blockIdx.y];
+  if (!J.flag || *J.flag == 0) return;
+  const uint64_t n4 = J.words >> 2;
+  const uint4 *src = (const uint4 *)J.src;
+  uint4 *dst = (uint4 *)J.dst;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    dst[i] = src[i];
+}
+
+cudaError_t launch_copy_multi(const CopyJob *jobs, uint32_t njobs, cudaStream_t st) {
+  if (!njobs) return cudaSuccess;
+  k_copy_multi<<<dim3(32, njobs), 256, 0, st>>>(jobs);
+  return cudaGetLastError();
+}
+
+__global__ void k_tick(uint32_t *counter) { *counter += 1; }
+
+cudaError_t launch_tick(uint32_t *counter, cudaStream_t st) {
+  k_tick<<<1, 1, 0, st>>>(counter);
+  return cudaGetLastError();
+}
+
+}  // namespace tmb
 
 #define CKU(call)                                                                \
   do {                                                                           \

@@ -65,6 +65,11 @@ class _Params(ctypes.Structure):
 
 
 EPOCH_CB = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_uint32)
+SEARCH_EPOCH_CB = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_uint32,
+                                   ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_int32),
+                                   ctypes.POINTER(ctypes.c_int32), ctypes.c_uint32)
+METRICS = {"f1": 0, "accuracy": 1, "mean_hamming": 2}
 BATCH_EPOCH_CB = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_uint32,
                                   ctypes.POINTER(ctypes.c_int32), ctypes.c_uint32)
 
@@ -98,6 +103,28 @@ class _Reconfig(ctypes.Structure):
     ]
 
 
+class _SearchArgs(ctypes.Structure):
+    _fields_ = [
+        ("test_samples", ctypes.c_uint64),
+        ("test_problems", ctypes.c_void_p),
+        ("test_solutions", ctypes.c_void_p),
+        ("test_codes", ctypes.c_void_p),
+        ("test_dim_offsets", ctypes.c_void_p),
+        ("test_each", ctypes.c_void_p),
+        ("on_device", ctypes.c_int32),
+        ("metric", ctypes.c_int32),
+        ("patience", ctypes.c_uint32),
+        ("tolerance", ctypes.c_double),
+        ("each", SEARCH_EPOCH_CB),
+        ("each_user", ctypes.c_void_p),
+        ("scores", ctypes.c_void_p),
+        ("final_scores", ctypes.c_void_p),
+        ("best_scores", ctypes.c_void_p),
+        ("epochs_run", ctypes.c_void_p),
+        ("best_epochs", ctypes.c_void_p),
+    ]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [
         ("train_launches", ctypes.c_uint64),
@@ -109,6 +136,11 @@ class Stats(ctypes.Structure):
         ("train_mode", ctypes.c_int32),
         ("train_autotuned", ctypes.c_int32),
         ("train_cpw", ctypes.c_int32),
+        ("pad_", ctypes.c_int32),
+        ("train_active_pairs", ctypes.c_uint64),
+        ("search_epoch_ms", ctypes.c_double),
+        ("search_epochs", ctypes.c_uint64),
+        ("search_train_ms", ctypes.c_double),
     ]
 
     def as_dict(self):
@@ -154,6 +186,8 @@ def lib():
     L.tm_train_batch.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(_TrainArgs), u32]
     L.tm_train_batch_each.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(_TrainArgs), u32,
                                       BATCH_EPOCH_CB, vp]
+    L.tm_train_batch_search.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(_TrainArgs), u32,
+                                        ctypes.POINTER(_SearchArgs)]
     L.tm_predict.argtypes = [vp, vp, vp, u64, vp, vp, i32]
     L.tm_predict_scores.argtypes = [vp, vp, vp, u64, vp, i32]
     L.tm_persist.argtypes = [vp, ctypes.c_char_p]
@@ -627,6 +661,100 @@ def train_batch(machines, tbls, each=None):
         _check(lib().tm_train_batch_each(hs, arr, len(machines), cb, None))
         del cb
     del keeps
+
+
+def train_batch_search(machines, tbls, test, patience=0, tolerance=1e-8, metric=None,
+                       each=None):
+    """One device-resident round of the reference's search
+    (optimize.lua:424-471 with train_tm's epoch logic, :586-653): every
+    machine trains on its table, is scored on `test` after each epoch on the
+    GPU (metric "f1" -- evaluator.class_accuracy(...).f1, the reference's
+    usual search_metric --, "accuracy", or "mean_hamming" for encoders),
+    keeps a checkpoint of its best epoch when patience > 0, stops after
+    `patience` epochs without improving by more than `tolerance`, and ends
+    restored to its best checkpoint.  One CUDA graph replay per epoch.
+    `test`: {"samples", "problems", "solutions"} or {"samples", "sentences",
+    "codes"} (+ "dim_offsets"); "problems_each" (one holdout per machine, for
+    machines whose literal layouts differ) replaces "problems".
+    `each(epoch, scores, training)` may return False (stop all) or
+    per-machine stop flags.  Returns per-machine numpy arrays: scores
+    [machines, epochs] (NaN where untrained), final, best, epochs,
+    best_epoch."""
+    if len(machines) != len(tbls):
+        raise TsetlinError("train_batch_search: one table per machine")
+    count = len(machines)
+    if count == 0:
+        return {}
+    arr = (_TrainArgs * count)()
+    keeps = []
+    for i, (m, t) in enumerate(zip(machines, tbls)):
+        if t.get("each") is not None:
+            raise TsetlinError("train_batch_search: per-epoch callbacks go in `each`")
+        a, keep = m._train_args(t)
+        arr[i] = a
+        keeps.append(keep)
+    enc = machines[0].info()["type"] == ENCODER
+    if metric is None:
+        metric = "mean_hamming" if enc else "f1"
+    if metric not in METRICS:
+        raise TsetlinError("train_batch_search: metric is one of %s" % sorted(METRICS))
+    n = int(test["samples"])
+    each_x = test.get("problems_each")
+    x = _Buf(test.get("sentences" if enc else "problems"), np.uint8)
+    xs = [_Buf(v, np.uint8) for v in each_x] if each_x is not None else []
+    if each_x is not None and len(xs) != count:
+        raise TsetlinError("train_batch_search: one holdout per machine in problems_each")
+    truth = _Buf(test["codes"], np.uint8) if enc else _Buf(test["solutions"], np.int64)
+    dof = _Buf(test.get("dim_offsets"), np.int64)
+    on_dev = xs[0].device if xs else x.device
+    if on_dev != truth.device or any(b.device != on_dev for b in xs):
+        raise TsetlinError("train_batch_search: test inputs on different devices")
+    tx_arr = (ctypes.c_void_p * count)(*[b.ptr for b in xs]) if xs else None
+    E = max(int(t["iterations"]) for t in tbls)
+    out = {"scores": np.full((count, max(E, 1)), np.nan), "final": np.zeros(count),
+           "best": np.zeros(count), "epochs": np.zeros(count, dtype=np.uint32),
+           "best_epoch": np.zeros(count, dtype=np.uint32)}
+    sa = _SearchArgs()
+    sa.test_samples = n
+    sa.test_problems = x.ptr
+    sa.test_solutions = None if enc else truth.ptr
+    sa.test_codes = truth.ptr if enc else None
+    sa.test_dim_offsets = dof.ptr
+    sa.test_each = ctypes.cast(tx_arr, ctypes.c_void_p) if tx_arr is not None else None
+    sa.on_device = 1 if on_dev else 0
+    sa.metric = METRICS[metric]
+    sa.patience = int(patience or 0)
+    sa.tolerance = float(tolerance)
+    sa.scores = out["scores"].ctypes.data
+    sa.final_scores = out["final"].ctypes.data
+    sa.best_scores = out["best"].ctypes.data
+    sa.epochs_run = out["epochs"].ctypes.data
+    sa.best_epochs = out["best_epoch"].ctypes.data
+    cb = None
+    if each is not None:
+        def _cb(_user, epoch, scores, training, stop, cnt):
+            try:
+                sc = np.ctypeslib.as_array(scores, shape=(cnt,)).copy()
+                tr = np.ctypeslib.as_array(training, shape=(cnt,)).astype(bool)
+                r = each(int(epoch), sc, tr)
+            except Exception as e:  # noqa: BLE001
+                sys.stderr.write("Error in callback: %s\n" % (e,))
+                return 1
+            if r is False:
+                return 1
+            if r is not None:
+                for i, flag in enumerate(r):
+                    if i < cnt and flag:
+                        stop[i] = 1
+            return 0
+        cb = SEARCH_EPOCH_CB(_cb)
+        sa.each = cb
+    hs = (ctypes.c_void_p * count)(*[m.handle.value for m in machines])
+    _check(lib().tm_train_batch_search(hs, arr, count, ctypes.byref(sa)))
+    del keeps, cb, xs, tx_arr
+    if E:
+        out["scores"] = out["scores"][:, :E]
+    return out
 
 
 # ---------------------------------------------------------------------------

@@ -18,6 +18,16 @@ Each trial's machine trains exactly as it would alone (the keyed draws make
 machines independent), so the per-trial epochs, scores and chosen
 parameters are the same as the sequential form.
 
+`search_metric` may also name a metric the GPU computes itself -- a table
+{"metric": "f1" | "accuracy" | "mean_hamming", "samples": n, "problems" /
+"sentences": holdout, "solutions" / "codes": truth} standing for the
+reference's usual `function (t) ... class_accuracy(t:predict(...)).f1`.
+A batched round then runs device-resident (`train_batch_search`): each
+epoch of all trials -- training, holdout predict, scores, patience,
+checkpoints -- is one CUDA graph replay, and no per-trial data leaves the
+GPU until the round ends.  Scores and chosen parameters are the same as
+with the equivalent callable.
+
 The reference's generator for sampling (santoku's num.random /
 rand.fast_normal) is not available; a seeded numpy Generator stands in.
 The landmark-encoding options of the encoder search (HLTH) are out of
@@ -27,7 +37,7 @@ import math
 
 import numpy as np
 
-from . import create, train_batch
+from . import class_accuracy, create, encoding_accuracy, train_batch, train_batch_search
 
 PARAM_NAMES = ("clauses", "clause_tolerance", "clause_maximum", "target", "specificity",
                "include_bits")
@@ -276,6 +286,32 @@ def train_tm_batch(typ, machines, args, plist, iterations, patience, tolerance, 
     return [tr.finish() for tr in trs]
 
 
+def device_metric_fn(typ, spec):
+    """The host form of a device metric table: predict the holdout and score
+    it with the GPU evaluator (used for single trials and the final
+    training; equal to what the device-resident round computes)."""
+    n = int(spec["samples"])
+    name = spec.get("metric", "mean_hamming" if typ == "encoder" else "f1")
+    dof = spec.get("dim_offsets")
+    rest = [dof, n] if dof is not None else [n]
+
+    def fn(t, _enc_info=None):
+        if typ == "encoder":
+            acc = encoding_accuracy(t.predict(spec["sentences"], *rest), spec["codes"], n,
+                                    t.info()["classes"])
+            return acc["mean_hamming"], acc
+        pred = t.predict(spec["problems"], *rest)
+        if name == "accuracy":
+            pv = pred.cpu().numpy() if hasattr(pred, "cpu") else pred
+            yv = spec["solutions"]
+            yv = yv.cpu().numpy() if hasattr(yv, "cpu") else np.asarray(yv)
+            acc = float((pv == yv).sum()) / n
+            return acc, {"accuracy": acc}
+        acc = class_accuracy(pred, spec["solutions"], n, t.info()["classes"])
+        return acc["f1"], acc
+    return fn
+
+
 def _machine_table(typ, args, params, reusable):
     t = {"clauses": params["clauses"], "clause_tolerance": params["clause_tolerance"],
          "clause_maximum": params["clause_maximum"], "target": params["target"],
@@ -299,7 +335,8 @@ def _optimize_tm(args, typ):
     tolerance = args.get("search_tolerance", 1e-8)
     iters = args.get("search_iterations", 10)
     final_iters = args.get("final_iterations", iters * 10)
-    metric_fn = args["search_metric"]
+    metric_spec = args["search_metric"] if isinstance(args["search_metric"], dict) else None
+    metric_fn = device_metric_fn(typ, metric_spec) if metric_spec else args["search_metric"]
     each_cb = args.get("each")
     samplers = build_samplers(args, PARAM_NAMES, args.get("search_dev", 0.2), rng)
 
@@ -321,8 +358,19 @@ def _optimize_tm(args, typ):
     def round_fn(plist, infos):
         plist = [fix(p) for p in plist]
         ms = [create(typ, _machine_table(typ, args, p, True)) for p in plist]
-        res = train_tm_batch(typ, ms, args, plist, iters, patience if patience > 0 else None,
-                             tolerance, metric_fn, each_cb, infos)
+        if metric_spec is not None and each_cb is None:
+            # device-resident round: per-epoch scores never leave the GPU
+            test = {k: v for k, v in metric_spec.items() if k != "metric"}
+            r = train_batch_search(ms, [_train_table(typ, args, iters)] * len(ms), test,
+                                   patience=patience if patience > 0 else 0,
+                                   tolerance=tolerance, metric=metric_spec.get("metric"))
+            res = [(float(r["final"][k]), {"score": float(r["final"][k]),
+                                           "epochs": int(r["epochs"][k])})
+                   for k in range(len(ms))]
+        else:
+            res = train_tm_batch(typ, ms, args, plist, iters,
+                                 patience if patience > 0 else None, tolerance, metric_fn,
+                                 each_cb, infos)
         for m in ms:
             m.destroy()
         return [(score, metrics, None) for score, metrics in res]

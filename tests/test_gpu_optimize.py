@@ -24,7 +24,8 @@ def _setup(tm):
         return acc["f1"], acc
 
     return dict(features=784, classes=10, samples=1200, problems=x[:1200].ravel(),
-                solutions=y[:1200], search_metric=metric)
+                solutions=y[:1200], search_metric=metric,
+                holdout=dict(samples=len(yv), problems=xv, solutions=yv))
 
 
 def test_batched_round_equals_sequential(tm):
@@ -50,3 +51,28 @@ def test_batched_round_equals_sequential(tm):
     assert sorted(events[True]) == sorted(events[False])
     assert results[True] == results[False]
     assert any(e[0] for e in events[True])  # the final training ran
+
+
+def test_device_metric_search_equals_callable(tm):
+    """A search whose metric is a device metric table runs its batched
+    rounds device-resident (train_batch_search) and chooses the same
+    parameters, with the same final score, as the same search driven by the
+    equivalent callable metric."""
+    from santoku_tsetlin import optimize
+    base = _setup(tm)
+    results = {}
+    for kind in ("callable", "device"):
+        args = dict(base, clauses={"def": 16, "min": 8, "max": 64, "round": 8},
+                    clause_tolerance={"def": 16, "min": 8, "max": 64, "int": True},
+                    clause_maximum={"def": 16, "min": 8, "max": 64, "int": True},
+                    target={"def": 8, "min": 4, "max": 32, "int": True},
+                    specificity={"def": 10, "min": 4, "max": 40},
+                    include_bits=1, search_rounds=2, search_trials=4, search_iterations=4,
+                    search_patience=2, final_iterations=3, final_patience=0, batched=True,
+                    search_seed=11)
+        if kind == "device":
+            args["search_metric"] = dict(base["holdout"], metric="f1")
+        final, metrics, best = optimize.classifier(args)
+        results[kind] = (best, metrics["f1"])
+        final.destroy()
+    assert results["device"] == results["callable"]
