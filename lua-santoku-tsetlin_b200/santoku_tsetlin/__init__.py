@@ -159,6 +159,7 @@ class _ServerConfig(ctypes.Structure):
 _lib = None
 EXPORTS = (
     "tm_params_init", "tm_create", "tm_train", "tm_train_batch", "tm_train_batch_each",
+    "tm_train_batch_search",
     "tm_predict",
     "tm_predict_scores", "tm_persist", "tm_persist_buf", "tm_save", "tm_save_buf", "tm_free",
     "tm_load",
