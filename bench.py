@@ -1,28 +1,46 @@
 #!/usr/bin/env python
 """Benchmark of the Tsetlin-machine hot path on B200.
 
-Metric: "TM train+predict samples/s" -- one step is one training epoch of a
-machine from its initial state (`train{iterations = 1}`, capi.c:1484) plus
-predict over the held-out set (capi.c:1088), the unit of work the
-reference's search driver repeats per trial epoch (optimize.lua:586-653).
+Metric: "TM train+predict samples/s (batched vs plain, equal accuracy)".
 
-Default workload (N = 1): the large sparse classifier -- 20 classes, 16,384
-features (flip-packed to 32,768 literal bits, 4 KB per sample), 2,048
-clauses per class, specificity 25, target 200, clause_tolerance 64,
-clause_maximum 64, 8-bit state; 100,000 train and 20,000 test samples of
-Zipf(1.1) features at ~1.5 % density with per-class boosted subsets
-(synthetic, seeded; datagen.sparse_classifier).
+Default workload (N = 1): the batched hyper-parameter search -- 64
+classifiers of uneven size (clauses per class log-uniform over 64..4,096,
+specificity U[2, 40], target U[20, 400], negated literals on or off) on
+plain-classifier data (10 classes, 784 features, class prototypes with 10 %
+bit flips) scaled to 60,000 train and 15,000 holdout samples.  A search
+round trains all 64 for 10 epochs and scores each on the holdout after
+every epoch (the reference's search loop, optimize.lua:424-471, with
+train_tm's epoch logic, :586-653; search metric = macro F1 of
+evaluator.class_accuracy).  One step is one epoch of the round: all 64
+machines train one epoch over the 60,000 samples, then predict and score
+the 15,000 holdout samples -- `tm_train_batch_search`, one CUDA graph
+replay per epoch.  `value` counts machine-samples (train + holdout) per
+second over K consecutive epochs; rounds restart after 10 epochs and their
+set-up (machine creation, staging, graph capture) is inside the timed
+region.  `plain` is the same round run the reference's way: one machine at
+a time, one launch per epoch, the metric on the host between epochs.
+`accuracy` checks that both forms end every machine with the same score
+(they are bit-identical).
+
+Other workloads (--workload): c1 / c0 / c2 -- one machine, one step = one
+training epoch from the initial state + predict of the test set; serve --
+resident machines under Poisson requests.
 
 Arms:
   default           the CUDA library through the C ABI (santoku_tsetlin)
   --impl reference  the reference's CPU implementation of the same step on
                     this host's cores: the reference's own capi.c/automata.h
                     (oracle/_ref) where it was built, else the C restatement
-                    (oracle/), on a bounded sample of units, scaled.
+                    (oracle/), on a bounded sample of units and samples,
+                    scaled.
 
-Under torchrun each rank trains its own replica of the machine (independent
-units, no data-path collective): weak scaling; `value` = all ranks' samples
-over the max-over-ranks device time.
+Under torchrun the search's machines are partitioned across ranks by cost
+(LPT; no data-path collective) -- the 64-machine round is fixed work
+(strong scaling); the single-machine workloads train one machine split by
+class ranges (multi.train_sharded: every rank trains its classes, then one
+all-gather of their automata, device to device over NCCL) and each rank
+predicts its share of the test set.  `value` = the job's samples over the
+max-over-ranks time.
 """
 import argparse
 import json
@@ -178,9 +196,72 @@ def measured_peaks():
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: the reference's path on a bounded sample of units
+# common
 # ---------------------------------------------------------------------------
-def cpu_step(w, d, threads, budget_units=None):
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def balanced_chunks(classes, threads, at_most):
+    """8-clause chunks per class for a CPU sample whose unit count
+    (classes x chunks) is a multiple of the thread count when possible, so
+    that OpenMP's static schedule gives every thread the same units."""
+    k = max(1, -(-threads // classes))
+    while (classes * k) % threads and k < at_most:
+        k += 1
+    return max(1, min(k, at_most))
+
+
+# Warp-instructions the fused train kernels issue per active (unit, sample)
+# step -- a sample the unit trains on after negative sampling -- counted by
+# ncu (smsp__inst_executed.sum of one launch divided by the launch's active
+# steps, which the library counts itself), per (workload, mode, clauses per
+# warp).  The int_issue roofline below is that count x the live active steps
+# / the train kernel's live time, against 4 warp-instructions per clock per
+# SM.  Capture commands:
+#   TSETLIN_B200_VARIANT=<mode>:<cpw> ncu --clock-control none -k regex:k_train -c 1 \
+#       --metrics smsp__inst_executed.sum python bench.py --profile-launch search
+#   ncu --clock-control none -k regex:k_train -c 1 --metrics smsp__inst_executed.sum \
+#       python bench.py --profile-launch c1_small
+INSTR_PER_PAIR = {}
+
+
+def issue_roofline(key, pairs, kernel_ms, sm_mhz, extra=None):
+    peak = 148 * 4 * sm_mhz * 1e6
+    ipp = INSTR_PER_PAIR.get(key)
+    r = {"bound": "int_issue", "unit": "warp-instr/s", "peak": peak,
+         "peak_source": "148 SMs x 4 warp-instructions per clock x median SM clock under load",
+         "variant": list(key[1:]), "active_pairs": int(pairs), "train_kernel_ms": kernel_ms,
+         "instr_per_active_pair": ipp}
+    if ipp and kernel_ms > 0:
+        r["achieved"] = ipp * pairs / (kernel_ms / 1e3)
+        r["frac"] = r["achieved"] / peak
+    else:
+        r["achieved"] = r["frac"] = None
+    if extra:
+        r.update(extra)
+    return r
+
+
+# ---------------------------------------------------------------------------
+# single-machine workloads (c1 / c0 / c2)
+# ---------------------------------------------------------------------------
+def cpu_step(w, d, threads):
     """One step of the workload on the CPU, on a machine with the same rows
     but fewer clauses per class (units are independent 8-clause chunks, so
     per-unit work is unchanged), scaled to the full clause count.  Predict is
@@ -188,10 +269,8 @@ def cpu_step(w, d, threads, budget_units=None):
     import oracle as O
     which = "ref" if O.ref_available() else "oracle"
     threads = threads or os.cpu_count()
-    units_per_class = max(1, min(w["clauses"] // 8, (2 * threads + w["classes"] - 1) // w["classes"]))
-    if budget_units:
-        units_per_class = max(1, min(units_per_class, budget_units // w["classes"]))
-    clauses = 8 * units_per_class
+    chunks = balanced_chunks(w["classes"], threads, w["clauses"] // 8)
+    clauses = 8 * chunks
     cfg = dict(type=w["kind"], classes=w["classes"], features=w["features"], clauses=clauses,
                clause_tolerance=w["clause_tolerance"], clause_maximum=w["clause_maximum"],
                specificity=w["specificity"], target=w["target"])
@@ -208,57 +287,16 @@ def cpu_step(w, d, threads, budget_units=None):
     t0 = time.perf_counter()
     m.predict(xt.ravel(), nt, threads=threads)
     t_pred = time.perf_counter() - t0
-    scale_units = (w["clauses"] // 8) / units_per_class
+    scale_units = (w["clauses"] // 8) / chunks
     step_s = t_train * scale_units + t_pred * scale_units * (w["n_test"] / nt)
     samples = w["n_train"] + w["n_test"]
-    sample = ("1 train epoch of %d of %d clauses per class (%d of %d units) over all %d "
-              "samples + predict of %d of %d test samples; times scaled by units and samples"
-              % (clauses, w["clauses"], units_per_class * w["classes"],
-                 (w["clauses"] // 8) * w["classes"], n, nt, w["n_test"]))
+    sample = ("1 train epoch of %d of %d clauses per class (%d of %d units, a multiple of the "
+              "%d threads) over all %d samples + predict of %d of %d test samples; times "
+              "scaled by units and samples"
+              % (clauses, w["clauses"], chunks * w["classes"],
+                 (w["clauses"] // 8) * w["classes"], threads, n, nt, w["n_test"]))
     return dict(value=samples / step_s, step_s=step_s, kind="reference" if which == "ref" else "port",
                 cores=threads, sample=sample, measured_s=t_train + t_pred)
-
-
-# ---------------------------------------------------------------------------
-# arms
-# ---------------------------------------------------------------------------
-def dist_init():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if ws > 1:
-        import datetime
-        import torch
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    return ws, rank, local
-
-
-def run_reference(args, w):
-    ws, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
-    if rank != 0:
-        return
-    d = make_data(w)
-    threads = os.cpu_count()
-    for _ in range(args.warmup if args.warmup < 1 else 1):
-        pass
-    vals = []
-    for _ in range(max(1, min(args.steps, 3))):
-        r = cpu_step(w, d, threads)
-        vals.append(r)
-    v = float(np.median([r["value"] for r in vals]))
-    step_s = float(np.median([r["step_s"] for r in vals]))
-    out = {
-        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws,
-        "steps": len(vals), "warmup": 0, "ms_per_step": step_s * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": config_of(w, ws),
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": vals[0]["cores"],
-                         "kind": vals[0]["kind"], "sample": vals[0]["sample"]},
-        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
-    print(json.dumps(out), flush=True)
 
 
 def config_of(w, ws):
@@ -269,9 +307,33 @@ def config_of(w, ws):
         "specificity": w["specificity"], "target": w["target"], "state_bits": 8,
         "n_train": w["n_train"], "n_test": w["n_test"],
         "step": "train{iterations=1} from the initial state + predict(test)",
-        "parallelism": "replicas" if ws > 1 else "single",
+        "parallelism": "class-sharded" if ws > 1 else "single",
         "l2": "inputs larger than L2 (train set and automata exceed 126 MB)",
     }
+
+
+def run_reference(args, w):
+    ws, rank = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    d = make_data(w)
+    threads = os.cpu_count()
+    vals = []
+    for _ in range(max(1, min(args.steps, 3))):
+        vals.append(cpu_step(w, d, threads))
+    v = float(np.median([r["value"] for r in vals]))
+    step_s = float(np.median([r["step_s"] for r in vals]))
+    out = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws,
+        "steps": len(vals), "warmup": 0, "ms_per_step": step_s * 1e3, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": config_of(w, ws),
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": vals[0]["cores"],
+                         "kind": vals[0]["kind"], "sample": vals[0]["sample"]},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "measured_s": float(sum(r["measured_s"] for r in vals)),
+    }
+    print(json.dumps(out), flush=True)
 
 
 def train_algorithmic_bytes(w, resident_units):
@@ -288,37 +350,41 @@ def train_algorithmic_bytes(w, resident_units):
 def run_ours(args, w):
     import torch
     import santoku_tsetlin as tm
+    from santoku_tsetlin import multi
     ws, rank, local = dist_init()
     dev = torch.device("cuda", local if ws > 1 else 0)
     torch.cuda.set_device(dev)
-    d = make_data(w, rank)
+    d = make_data(w, 0)
     n, nt = w["n_train"], w["n_test"]
+    # class-sharded: every rank predicts its share of the test set
+    lo_s, hi_s = multi.class_range(nt, ws, rank)
     lab_key = "y" if w["kind"] == "classifier" else "codes"
     # device-resident inputs (value) and pinned host inputs (e2e)
     x_dev = torch.from_numpy(np.ascontiguousarray(d["x"][:n])).to(dev)
     lab_dev = torch.from_numpy(np.ascontiguousarray(d[lab_key][:n])).to(dev)
-    xt_dev = torch.from_numpy(np.ascontiguousarray(d["x"][n:n + nt])).to(dev)
+    xt_dev = torch.from_numpy(np.ascontiguousarray(d["x"][n + lo_s:n + hi_s])).to(dev)
     x_host = torch.from_numpy(np.ascontiguousarray(d["x"][:n])).pin_memory()
     lab_host = torch.from_numpy(np.ascontiguousarray(d[lab_key][:n])).pin_memory()
-    xt_host = torch.from_numpy(np.ascontiguousarray(d["x"][n:n + nt])).pin_memory()
-    t = tm.create(w["kind"], create_table(w, seed=rank))
+    xt_host = torch.from_numpy(np.ascontiguousarray(d["x"][n + lo_s:n + hi_s])).pin_memory()
+    t = tm.create(w["kind"], create_table(w, seed=0))
     t.stats_enable(True)
 
+    def train(tbl):
+        if ws > 1:
+            multi.train_sharded(t, tbl, device=dev)
+        else:
+            t.train(tbl)
+
     def step_dev():
-        t.train(train_table(w, x_dev, lab_dev))
-        return t.predict(xt_dev, nt)
+        train(train_table(w, x_dev, lab_dev))
+        return t.predict(xt_dev, hi_s - lo_s)
 
     def step_host():
-        t.train(train_table(w, x_host.numpy(), lab_host.numpy()))
-        return t.predict(xt_host.numpy(), nt)
-
-    def barrier():
-        if ws > 1:
-            import torch.distributed as dist
-            dist.barrier()
+        train(train_table(w, x_host.numpy(), lab_host.numpy()))
+        return t.predict(xt_host.numpy(), hi_s - lo_s)
 
     def timed(fn, k):
-        barrier()
+        barrier(ws)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -326,8 +392,7 @@ def run_ours(args, w):
             fn()
         e1.record()
         torch.cuda.synchronize()
-        barrier()
-        from santoku_tsetlin import multi
+        barrier(ws)
         return multi.max_over_ranks(e0.elapsed_time(e1), device=dev)
 
     for _ in range(args.warmup):
@@ -338,60 +403,52 @@ def run_ours(args, w):
     ms = timed(step_dev, args.steps)
     ck = clocks.stop()
     st = t.stats()
-    # end to end through the public API from pinned host buffers
     step_host()
-    ms_e2e = timed(step_host, max(1, min(args.steps, 3)))
     k_e2e = max(1, min(args.steps, 3))
-    samples = (n + nt) * ws
+    ms_e2e = timed(step_host, k_e2e)
+    samples = n + nt
     value = samples * args.steps / (ms / 1e3)
     e2e_value = samples * k_e2e / (ms_e2e / 1e3)
     peaks, peak_kind = measured_peaks()
-    # roofline of the dominant kernel (the fused train kernel), timed with CUDA
-    # events on the library's stream
-    occ_units = 2 * 148
-    alg = train_algorithmic_bytes(w, occ_units)
-    # DRAM bytes of one k_train launch from an ncu capture of the same kernel
-    # on the large sparse classifier's rows with 280 units and 40,000 samples
-    # (profiles/k_train_c1_small_ncu.md: 1.856 GB read + 8.695 GB written),
-    # scaled by units x samples to this launch.
-    traffic = None
-    if w["name"] == "large-sparse-classifier":
-        per_unit_sample = (1.855563e9 + 8.695468e9) / (280 * 40000)
-        traffic = per_unit_sample * (w["classes"] * w["clauses"] // 8) * w["n_train"]
     avg_ms = st["train_kernel_ms"] / max(1, st["train_launches"])
-    achieved = alg / (avg_ms / 1e3) / 1e9
+    alg = train_algorithmic_bytes(w, max(1, st["train_resident"]))
     wp = ((2 * w["features"] + 31) // 32 + 3) // 4 * 4
+    sm_mhz = (ck or {}).get("sm_mhz") or 1965.0
+    key = (args.workload, st["train_mode"], st["train_cpw"])
+    roof = issue_roofline(key, st["train_active_pairs"] / max(1, st["train_launches"]), avg_ms,
+                          sm_mhz, extra={
+                              "kernel": "k_train_warp" if st["train_mode"] == 3 else "k_train",
+                              "hbm": {"algorithmic_bytes_per_launch": alg,
+                                      "achieved_gbs": alg / (avg_ms / 1e3) / 1e9,
+                                      "peak_gbs": peaks["hbm_gbs"], "peak_source": peak_kind,
+                                      "resident_units": st["train_resident"]},
+                              "avg_launch_ms": avg_ms, "traffic": None})
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "scaling": "strong", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": config_of(w, ws),
         "e2e": {"value": e2e_value, "unit": UNIT,
                 "h2d_bytes_per_step": int(n * d["x"].shape[1] + d[lab_key][:n].nbytes +
-                                          nt * d["x"].shape[1]),
-                "d2h_bytes_per_step": int(nt * (8 if w["kind"] == "classifier"
-                                                else (w["classes"] + 7) // 8))},
+                                          (hi_s - lo_s) * d["x"].shape[1]),
+                "d2h_bytes_per_step": int((hi_s - lo_s) * (8 if w["kind"] == "classifier"
+                                                           else (w["classes"] + 7) // 8))},
         "gpu_launches": int(st["kernel_launches"]),
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
-                     "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
-                     "kernel": "k_train", "peak_source": peak_kind,
-                     "frac_of_nominal": achieved / 8000.0, "nominal_peak": 8000.0,
-                     "algorithmic_bytes_per_launch": alg, "avg_launch_ms": avg_ms},
+        "roofline": roof,
         "kernels": {
             "train_ms_per_step": st["train_kernel_ms"] / args.steps,
             "predict_ms_per_step": st["predict_kernel_ms"] / args.steps,
             "train_unit_steps": st["train_unit_steps"],
+            "train_active_pairs": st["train_active_pairs"],
             "literal_evals_per_s_train_upper": st["train_unit_steps"] * 8 * 32 * wp /
                                                (st["train_kernel_ms"] / 1e3 + 1e-12),
-            "predict_literal_evals_per_s": nt * w["classes"] * w["clauses"] * 2 * w["features"] /
-                                           (st["predict_kernel_ms"] / max(1, st["predict_launches"]) / 1e3 + 1e-12),
+            "predict_literal_evals_per_s": (hi_s - lo_s) * w["classes"] * w["clauses"] * 2 *
+                                           w["features"] /
+                                           (st["predict_kernel_ms"] / max(1, st["predict_launches"])
+                                            / 1e3 + 1e-12),
         },
     }
     if rank == 0:
-        # integer-pipe roofline of clause evaluation (after the timed region):
-        # per 32 words k_predict's inner loop issues 62 logic ops (5 carry-save
-        # steps of 4 AND-NOT + 6 LOP3, 3 direct steps of 4 AND-NOT) and 17
-        # POPC (5 + 12); POPC and the logic ops issue on separate pipes
         pk = tm.int_peaks(dev.index if dev.index is not None else 0)
         wops = out["kernels"]["predict_literal_evals_per_s"] / 32
         bound = min(32 * pk["lop3"] / 62, 32 * pk["popc"] / 17)
@@ -413,103 +470,292 @@ def run_ours(args, w):
 
 
 # ---------------------------------------------------------------------------
-# batched hyper-parameter search: 64 machines, batched vs one per launch
+# batched hyper-parameter search (default): 64 machines, device-resident
+# rounds vs the plain one-machine-per-launch form
 # ---------------------------------------------------------------------------
-def run_search(args):
+SEARCH = dict(machines=64, n_train=60000, n_test=15000, epochs=10, classes=10, features=784)
+
+
+def search_data():
+    from santoku_tsetlin import datagen
+    n = SEARCH["n_train"] + SEARCH["n_test"]
+    cache = "/tmp/tsetlin_b200_search_%d.npz" % n
+    if os.path.exists(cache):
+        z = np.load(cache)
+        return {True: (z["x1"], z["xt1"]), False: (z["x0"], z["xt0"]), "y": z["y"], "yt": z["yt"]}
+    protos = np.random.default_rng(7919 + 1).random((SEARCH["classes"], SEARCH["features"])) < 0.2
+    out = {}
+    for negated in (True, False):
+        x, y, _ = datagen.prototype_classifier(n, classes=SEARCH["classes"],
+                                               features=SEARCH["features"], seed=1,
+                                               negated=negated, prototypes=protos)
+        out[negated] = (np.ascontiguousarray(x[:SEARCH["n_train"]]),
+                        np.ascontiguousarray(x[SEARCH["n_train"]:]))
+    out["y"] = np.ascontiguousarray(y[:SEARCH["n_train"]])
+    out["yt"] = np.ascontiguousarray(y[SEARCH["n_train"]:])
+    try:
+        np.savez(cache, x1=out[True][0], xt1=out[True][1], x0=out[False][0],
+                 xt0=out[False][1], y=out["y"], yt=out["yt"])
+    except OSError:
+        pass
+    return out
+
+
+def search_params(ws=1, rank=0):
+    from santoku_tsetlin import datagen, multi
+    allp = datagen.search_machines(SEARCH["machines"])
+    parts = multi.partition_lpt([p["clauses"] * (p["features"] + 31) // 32 for p in allp], ws)
+    return allp, [allp[i] for i in parts[rank]]
+
+
+def search_config(ws, allp, n_train):
+    return {
+        "workload": "batched-search", "machines": len(allp), "classes": SEARCH["classes"],
+        "features": SEARCH["features"],
+        "clauses_per_class": [p["clauses"] for p in allp],
+        "units": sum(SEARCH["classes"] * p["clauses"] // 8 for p in allp),
+        "negated": [p["negated"] for p in allp],
+        "specificity_range": [2, 40], "target_range": [20, 400], "clause_tolerance": 64,
+        "clause_maximum": 64, "state_bits": 8, "n_train": n_train, "n_test": SEARCH["n_test"],
+        "epochs_per_round": SEARCH["epochs"], "search_metric": "macro F1 (class_accuracy)",
+        "step": "one epoch of the device-resident round: every machine trains one epoch over "
+                "the train set, then predicts and scores the holdout (one CUDA graph replay)",
+        "parallelism": "machines partitioned across ranks (LPT)" if ws > 1 else "single",
+        "l2": "inputs larger than L2 (the 64 machines' automata, 1.2 GB, exceed 126 MB)",
+    }
+
+
+def make_search_machines(tm, params):
+    return [tm.create("classifier", dict(
+        classes=SEARCH["classes"], features=p["features"], clauses=p["clauses"],
+        clause_tolerance=p["clause_tolerance"], clause_maximum=p["clause_maximum"],
+        specificity=p["specificity"], target=p["target"], seed=p["seed"], reusable=True))
+        for p in params]
+
+
+def run_search_bench(args):
     import torch
     import santoku_tsetlin as tm
-    from santoku_tsetlin import datagen, multi
+    from santoku_tsetlin import multi
     ws, rank, local = dist_init()
-    count, n_train, n_test = args.machines, 60000, 6000
-    epochs = args.epochs or 2
-    all_params = datagen.search_machines(count)
-    # machines are independent: LPT partition by units across ranks (strong
-    # scaling: the 64-machine round is fixed)
-    parts = multi.partition_lpt([p["clauses"] * (p["features"] + 31) // 32 for p in all_params], ws)
-    params = [all_params[i] for i in parts[rank]]
-    count_local = len(params)
-    protos = np.random.default_rng(7919 + 1).random((10, 784)) < 0.2
-    xs = {}
-    for negated in (True, False):
-        x, y, _ = datagen.prototype_classifier(n_train + n_test, classes=10, features=784,
-                                               seed=1, negated=negated, prototypes=protos)
-        xs[negated] = (np.ascontiguousarray(x[:n_train]), np.ascontiguousarray(x[n_train:]))
-    yv = y
-    y_tr, y_te = np.ascontiguousarray(yv[:n_train]), yv[n_train:]
     dev = torch.device("cuda", local if ws > 1 else 0)
     torch.cuda.set_device(dev)
-    xd = {k: (torch.from_numpy(v[0]).to(dev), torch.from_numpy(v[1]).to(dev)) for k, v in xs.items()}
-    yd = torch.from_numpy(y_tr).to(dev)
+    n_train = args.search_train or SEARCH["n_train"]
+    allp, params = search_params(ws, rank)
+    d = search_data()
+    nt, E = SEARCH["n_test"], SEARCH["epochs"]
+    xd = {k: (torch.from_numpy(d[k][0][:n_train]).to(dev), torch.from_numpy(d[k][1]).to(dev))
+          for k in (True, False)}
+    yd = torch.from_numpy(d["y"][:n_train]).to(dev)
+    ytd = torch.from_numpy(d["yt"]).to(dev)
 
-    def make():
-        out = []
-        for p in params:
-            out.append(tm.create("classifier", dict(
-                classes=10, features=p["features"], clauses=p["clauses"],
-                clause_tolerance=p["clause_tolerance"], clause_maximum=p["clause_maximum"],
-                specificity=p["specificity"], target=p["target"], seed=p["seed"],
-                reusable=True)))
-        return out
+    def round_(iters, host=False, stats=None):
+        """One device-resident round of `iters` epochs of every local
+        machine (fresh machines, as the search creates them per trial)."""
+        ms = make_search_machines(tm, params)
+        if stats is not None and ms:
+            ms[0].stats_enable(True)  # the round's statistics gather on its first machine
+        tabs = [{"samples": n_train,
+                 "problems": d[p["negated"]][0][:n_train] if host else xd[p["negated"]][0],
+                 "solutions": d["y"][:n_train] if host else yd, "iterations": iters}
+                for p in params]
+        test = {"samples": nt, "solutions": d["yt"] if host else ytd,
+                "problems_each": [d[p["negated"]][1] if host else xd[p["negated"]][1]
+                                  for p in params]}
+        r = tm.train_batch_search(ms, tabs, test, patience=0, metric="f1") if ms else None
+        if stats is not None and ms:
+            stats.append(ms[0].stats())
+        for m in ms:
+            m.destroy()
+        return r
 
-    def tables():
-        return [{"samples": n_train, "problems": xd[p["negated"]][0], "solutions": yd,
-                 "iterations": epochs} for p in params]
-
-    def timed(fn):
-        if ws > 1:
-            import torch.distributed as dist
-            dist.barrier()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        fn()
-        e1.record()
-        torch.cuda.synchronize()
-        return multi.max_over_ranks(e0.elapsed_time(e1), device=dev)
-
-    warm = make()
-    tm.train_batch(warm[:4], tables()[:4])
-    for m in warm:
-        m.destroy()
-    batched = make()
-    clocks = ClockSampler(0)
+    if args.profile_launch:
+        # one round of one epoch: the launch an ncu capture profiles
+        st = []
+        round_(1, stats=st)
+        print(json.dumps({"profile_launch": "search", "mode": st[0]["train_mode"],
+                          "cpw": st[0]["train_cpw"],
+                          "active_pairs": st[0]["train_active_pairs"]}), flush=True)
+        return
+    # ---- warm-up: W epochs (tuning, first-touch allocations) ---------------
+    round_(max(1, args.warmup))
+    torch.cuda.synchronize()
+    # ---- timed: K epochs of device-resident rounds ---------------------------
+    K = args.steps
+    stats = []
+    clocks = ClockSampler(dev.index if dev.index is not None else 0)
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     clocks.start()
-    ms_b = timed(lambda: tm.train_batch(batched, tables()) if batched else None)
+    e0.record()
+    done = 0
+    while done < K:
+        it = min(E, K - done)
+        round_(it, stats=stats)
+        done += it
+    e1.record()
+    torch.cuda.synchronize()
     ck = clocks.stop()
-    plain = make()
-    tabs = tables()
-    ms_p = timed(lambda: [m.train(t) for m, t in zip(plain, tabs)])
-    same = all(np.array_equal(a.export_state()[0], b.export_state()[0])
-               for a, b in zip(batched[:8], plain[:8]))
-    acc_b = [float((m.predict(xd[p["negated"]][1], n_test).cpu().numpy() == y_te).mean())
-             for m, p in zip(batched, params)]
-    acc_p = [float((m.predict(xd[p["negated"]][1], n_test).cpu().numpy() == y_te).mean())
-             for m, p in zip(plain, params)]
-    samples = count * n_train * epochs
-    units = sum(10 * p["clauses"] // 8 for p in all_params)
+    barrier(ws)
+    ms_b = multi.max_over_ranks(e0.elapsed_time(e1), device=dev)
+    train_ms = sum(x["search_train_ms"] for x in stats)
+    graph_ms = sum(x["search_epoch_ms"] for x in stats)
+    pairs = sum(x["train_active_pairs"] for x in stats)
+    launches = sum(x["kernel_launches"] for x in stats)
+    modes = sorted({(x["train_mode"], x["train_cpw"]) for x in stats})
+    value = len(allp) * (n_train + nt) * K / (ms_b / 1e3)
+
+    # ---- plain: one machine at a time, one launch per epoch, host metric ---
+    pe = min(args.plain_epochs, E)
+    plain_final = {}
+    barrier(ws)
+    torch.cuda.synchronize()
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record()
+    for i, p in enumerate(params):
+        m = make_search_machines(tm, [p])[0]
+        scores = []
+
+        def each(epoch, m=m, xt=xd[p["negated"]][1], scores=scores):
+            scores.append(tm.class_accuracy(m.predict(xt, nt), ytd, nt, SEARCH["classes"])["f1"])
+            return True
+        m.train({"samples": n_train, "problems": xd[p["negated"]][0], "solutions": yd,
+                 "iterations": pe, "each": each})
+        plain_final[i] = scores[-1]
+        m.destroy()
+    p1.record()
+    torch.cuda.synchronize()
+    barrier(ws)
+    ms_p = multi.max_over_ranks(p0.elapsed_time(p1), device=dev)
+    plain_value = len(allp) * (n_train + nt) * pe / (ms_p / 1e3)
+
+    # ---- end to end from host buffers: one round of the plain form's epochs
+    # (so the two forms' final scores must agree machine by machine) ---------
+    barrier(ws)
+    torch.cuda.synchronize()
+    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    q0.record()
+    r = round_(pe, host=True)
+    q1.record()
+    torch.cuda.synchronize()
+    barrier(ws)
+    ms_e = multi.max_over_ranks(q0.elapsed_time(q1), device=dev)
+    e2e_value = len(allp) * (n_train + nt) * pe / (ms_e / 1e3)
+    batched_final = {i: float(r["final"][i]) for i in range(len(params))} if r else {}
+    same = all(batched_final[i] == plain_final[i] for i in range(len(params)))
+    # bytes copied per round: each machine's train rows and holdout (the
+    # library stages identical inputs once: one copy per literal layout)
+    # and the labels; back: the per-machine states once per epoch
+    h2d = sum(d[neg][0][:n_train].nbytes + d[neg][1].nbytes
+              for neg in {p["negated"] for p in params}) + d["y"][:n_train].nbytes + \
+        d["yt"].nbytes
+    sm_mhz = (ck or {}).get("sm_mhz") or 1965.0
+    key = ("search",) + (modes[-1] if len(modes) == 1 else (-1, -1))
+    roof = issue_roofline(key, pairs, train_ms, sm_mhz, extra={
+        "kernel": "k_train_warp" if key[1] == 3 else "k_train",
+        "epoch_graph_ms": graph_ms, "train_share_of_graph": train_ms / graph_ms if graph_ms else None,
+        "resident_units": stats[0]["train_resident"] if stats else None, "traffic": None})
+    peaks, peak_kind = measured_peaks()
     out = {
-        "metric": "TM batched search train samples/s", "value": samples / (ms_b / 1e3),
-        "unit": "samples/s", "n_gpus": ws, "steps": 1, "warmup": 1, "ms_per_step": ms_b,
+        "metric": METRIC + " (batched vs plain, equal accuracy)", "value": value, "unit": UNIT,
+        "n_gpus": ws, "steps": K, "warmup": args.warmup, "ms_per_step": ms_b / K,
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u32",
-        "data": "synthetic",
-        "config": {"workload": "batched-search", "machines": count, "units": units,
-                   "n_train": n_train, "epochs": epochs,
-                   "clauses_per_class": [p["clauses"] for p in all_params],
-                   "parallelism": "machines partitioned across ranks (LPT)" if ws > 1 else "single",
-                   "step": "%d machines x %d epochs in one tm_train_batch" % (count, epochs)},
-        "plain": {"value": samples / (ms_p / 1e3), "ms": ms_p,
-                  "form": "one tm_train call (one launch group) per machine, in sequence"},
-        "batched_over_plain": ms_p / ms_b,
-        "bit_identical_first_8": bool(same),
-        "accuracy": {"batched_mean": float(np.mean(acc_b)), "plain_mean": float(np.mean(acc_p))},
+        "data": "synthetic", "config": search_config(ws, allp, n_train),
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d / pe),
+                "d2h_bytes_per_step": int(len(params) * 64),
+                "form": "train_batch_search from host numpy buffers, one round of %d epochs; "
+                        "the round's copies spread over its epochs" % pe},
+        "gpu_launches": int(launches),
+        "plain": {"value": plain_value, "ms": ms_p, "epochs": pe,
+                  "form": "one tm_train per machine in turn with an `each` callback that "
+                          "predicts and scores the holdout (one launch per epoch per machine: "
+                          "the reference's train_tm flow)"},
+        "batched_over_plain": value / plain_value,
+        "accuracy": {"equal": bool(same), "epochs": pe,
+                     "batched_mean_f1": float(np.mean(list(batched_final.values()))),
+                     "plain_mean_f1": float(np.mean(list(plain_final.values())))},
+        "roofline": roof,
+        "hbm_peak": {"value": peaks["hbm_gbs"], "unit": "GB/s", "source": peak_kind},
     }
     if ck:
         out["clocks"] = ck
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cb = cpu_search_step(allp, d, os.cpu_count(), n_sample=args.cpu_samples)
+        out["cpu_baseline"] = {"value": cb["value"], "unit": UNIT, "cores": cb["cores"],
+                               "kind": cb["kind"], "sample": cb["sample"]}
     if rank == 0:
         print(json.dumps(out), flush=True)
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def cpu_search_step(allp, d, threads, n_sample=6000):
+    """One epoch of the 64-machine round on the CPU: each machine, with
+    enough 8-clause chunks per class for its units to be a multiple of the
+    thread count (units are independent, so per-unit work is the full
+    machine's), trains one epoch over `n_sample` of the train samples and
+    predicts `n_sample` / 4 holdout samples; times scaled by the machine's
+    units and by samples."""
+    import oracle as O
+    which = "ref" if O.ref_available() else "oracle"
+    total_s, measured = 0.0, 0.0
+    n_pred = max(1, n_sample // 4)
+    n_train, nt = SEARCH["n_train"], SEARCH["n_test"]
+    for p in allp:
+        chunks = balanced_chunks(SEARCH["classes"], threads, p["clauses"] // 8)
+        cfg = dict(type="classifier", classes=SEARCH["classes"], features=p["features"],
+                   clauses=8 * chunks, clause_tolerance=p["clause_tolerance"],
+                   clause_maximum=p["clause_maximum"], specificity=p["specificity"],
+                   target=p["target"])
+        m = O.Machine(which=which, **cfg)
+        x, xt = d[p["negated"]]
+        t0 = time.perf_counter()
+        m.train(x[:n_sample].ravel(), n_sample, 1, labels=d["y"][:n_sample], seed=p["seed"],
+                mode=O.REFSTRUCT if which == "ref" else O.PHILOX, threads=threads)
+        t1 = time.perf_counter()
+        m.predict(xt[:n_pred].ravel(), n_pred, threads=threads)
+        t2 = time.perf_counter()
+        scale = (p["clauses"] // 8) / chunks
+        total_s += (t1 - t0) * scale * (n_train / n_sample) + (t2 - t1) * scale * (nt / n_pred)
+        measured += t2 - t0
+    samples = len(allp) * (n_train + nt)
+    sample = ("one epoch of each of the %d machines with a thread-balanced %d-%d units each "
+              "over %d of %d train samples, predict of %d of %d holdout samples; scaled by "
+              "units and samples" % (len(allp), SEARCH["classes"],
+                                     SEARCH["classes"] * balanced_chunks(SEARCH["classes"], threads, 512),
+                                     n_sample, n_train, n_pred, nt))
+    return dict(value=samples / total_s, step_s=total_s, measured_s=measured,
+                kind="reference" if which == "ref" else "port", cores=threads, sample=sample)
+
+
+def run_search_reference(args):
+    ws, rank = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    allp, _ = search_params(1, 0)
+    d = search_data()
+    threads = os.cpu_count()
+    vals = []
+    for _ in range(max(1, args.steps)):
+        vals.append(cpu_search_step(allp, d, threads, n_sample=args.cpu_samples))
+        if sum(v["measured_s"] for v in vals) > args.cpu_budget:
+            break
+    v = float(np.median([r["value"] for r in vals]))
+    step_s = float(np.median([r["step_s"] for r in vals]))
+    out = {
+        "impl": "reference", "metric": METRIC + " (batched vs plain, equal accuracy)",
+        "value": v, "unit": UNIT, "n_gpus": ws, "steps": len(vals), "warmup": 0,
+        "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": search_config(ws, allp, SEARCH["n_train"]),
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": vals[0]["cores"],
+                         "kind": vals[0]["kind"], "sample": vals[0]["sample"]},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "measured_s": float(sum(r["measured_s"] for r in vals)),
+    }
+    print(json.dumps(out), flush=True)
 
 
 # ---------------------------------------------------------------------------
@@ -620,21 +866,35 @@ def serve_at(args, L, tm, machines, pools, rng, rate, requests=None):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=12)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS) + ["search", "serve"])
+    ap.add_argument("--workload", default="search", choices=sorted(WORKLOADS) + ["search", "serve"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--machines", type=int, default=64, help="search: machines")
-    ap.add_argument("--epochs", type=int, default=0, help="search: epochs (default 2)")
+    ap.add_argument("--plain-epochs", type=int, default=10,
+                    help="search: epochs of the plain form and of the e2e round")
+    ap.add_argument("--search-train", type=int, default=0,
+                    help="search: train samples (default 60,000; fewer for profiler captures)")
+    ap.add_argument("--cpu-samples", type=int, default=6000,
+                    help="search: train samples of the CPU reference's sampled epoch")
+    ap.add_argument("--cpu-budget", type=float, default=150.0,
+                    help="search --impl reference: stop after this many measured CPU seconds")
+    ap.add_argument("--profile-launch", default="", choices=["", "search"] + sorted(WORKLOADS),
+                    help="run only the train launch a profiler capture looks at")
     ap.add_argument("--requests", type=int, default=2000, help="serve: requests")
     ap.add_argument("--rate", type=float, default=5000.0, help="serve: arrivals per second")
     ap.add_argument("--hbm-budget", type=int, default=2048, help="serve: staging MB")
     ap.add_argument("--sustainable-rate", type=float, default=150.0,
                     help="serve: second, sustainable arrival rate")
     args = ap.parse_args()
-    if args.workload == "search":
-        run_search(args)
+    if args.profile_launch and args.profile_launch != "search":
+        run_profile_launch(args, WORKLOADS[args.profile_launch])
+        return
+    if args.workload == "search" or args.profile_launch == "search":
+        if args.impl == "reference":
+            run_search_reference(args)
+        else:
+            run_search_bench(args)
         return
     if args.workload == "serve":
         run_serve(args)
@@ -644,6 +904,28 @@ def main():
         run_reference(args, w)
     else:
         run_ours(args, w)
+
+
+def run_profile_launch(args, w):
+    """One train launch of a single-machine workload (1 epoch), printing
+    the library's count of its active steps: the launch a profiler capture
+    looks at."""
+    import torch
+    import santoku_tsetlin as tm
+    d = make_data(w, 0)
+    n = w["n_train"]
+    lab_key = "y" if w["kind"] == "classifier" else "codes"
+    x = torch.from_numpy(np.ascontiguousarray(d["x"][:n])).cuda()
+    lab = torch.from_numpy(np.ascontiguousarray(d[lab_key][:n])).cuda()
+    t = tm.create(w["kind"], create_table(w, seed=0))
+    t.set_autotune(0)
+    t.stats_enable(True)
+    t.train(train_table(w, x, lab))
+    st = t.stats()
+    print(json.dumps({"profile_launch": w["name"], "mode": st["train_mode"], "cpw": st["train_cpw"],
+                      "active_pairs": st["train_active_pairs"],
+                      "train_kernel_ms": st["train_kernel_ms"]}), flush=True)
+    t.destroy()
 
 
 if __name__ == "__main__":

@@ -343,6 +343,7 @@ typedef struct tm_stats {
   double search_epoch_ms;     /* device-resident search rounds: summed epoch graph time */
   uint64_t search_epochs;     /* epoch graph replays */
   double search_train_ms;     /* the train kernel's share of those replays */
+  uint64_t train_resident;    /* units resident at once in the last train launch */
 } tm_stats;
 /* Train-kernel variant choice.  All variants end in the same automaton
  * state; they differ in speed.  mode 0: heuristic (resident CTAs per SM);

@@ -612,6 +612,14 @@ static int heuristic_plan(const TrainShape &sh, const tm_machine *m0, TrainPlan 
               sh.Bmax);
 }
 
+// Units a launch of `p` holds at once: a warp per unit (4 per CTA), a CTA
+// per unit, or a 2-CTA cluster per unit.
+static uint64_t resident_units(const TrainPlan &p) {
+  if (p.mode == TM_MODE_WARP) return (uint64_t)p.grid * 4;
+  if (p.mode == TM_MODE_PAIR) return (uint64_t)p.grid / 2;
+  return (uint64_t)p.grid;
+}
+
 // Uploads the machine table and work list and launches `p` over epochs
 // [e0, e1).  `ms` (optional) receives the kernel's device time.
 static int launch_plan(const TrainPlan &p, const TrainShape &sh, const std::vector<TrainDev> &td,
@@ -876,6 +884,7 @@ static int run_epochs(std::vector<TrainJob> &jobs, uint32_t e0, uint32_t e1, tm_
   m0->stats.train_mode = plan.mode;
   m0->stats.train_autotuned = tuned ? 1 : 0;
   m0->stats.train_cpw = plan.cpw;
+  m0->stats.train_resident = resident_units(plan);
   float ms = 0;
   uint32_t herr = 0;
   int rc = launch_plan(plan, sh, td, work, e0, e1, m0, m0->timing ? &ms : nullptr, &herr);
@@ -1298,6 +1307,7 @@ static int search_round(tm_machine *const *ms, const tm_train_args *args, uint32
     m0->stats.train_mode = plan.mode;
     m0->stats.train_autotuned = tuned ? 1 : 0;
     m0->stats.train_cpw = plan.cpw;
+    m0->stats.train_resident = resident_units(plan);
   }
   const size_t tbytes = td.size() * sizeof(TrainDev);
   const size_t off_w = (tbytes + 255) & ~(size_t)255;

@@ -141,6 +141,7 @@ class Stats(ctypes.Structure):
         ("search_epoch_ms", ctypes.c_double),
         ("search_epochs", ctypes.c_uint64),
         ("search_train_ms", ctypes.c_double),
+        ("train_resident", ctypes.c_uint64),
     ]
 
     def as_dict(self):
