@@ -35,6 +35,7 @@ extern "C" {
 #define TM_ERR_OOM (-4)      /* allocation failed (host or device) */
 #define TM_ERR_IO (-5)       /* file or stream error */
 #define TM_ERR_DEVICE (-6)   /* a kernel reported an error status */
+#define TM_ERR_BUSY (-7)     /* the server's queue is full: retry later */
 
 #define TM_CLASSIFIER 0
 #define TM_ENCODER 1
@@ -379,31 +380,41 @@ int tm_reset_stats(tm_machine *m);
 /* ---- serving: resident machines, continuous batching ------------------- */
 /* No counterpart in the reference (its predict is one synchronous call per
  * batch, capi.c:1088-1110).  A server keeps machines resident, accepts
- * predict requests at any time, packs queued requests into shared device
- * launches as slots and its device-memory budget allow, and completes each
- * request with exactly the result tm_predict gives for it alone. */
+ * predict requests at any time, and packs queued requests -- for any of its
+ * machines, in arrival order -- into shared device launches as launch slots
+ * and its device-memory budget allow; each request completes with exactly
+ * the result tm_predict gives for it alone. */
 typedef struct tm_server tm_server;
 
 typedef struct tm_server_config {
-  uint64_t hbm_budget_bytes;   /* request staging memory (inputs + outputs) */
-  uint32_t max_inflight;       /* requests on the device at once */
-  uint32_t max_batch_samples;  /* samples packed into one launch */
+  uint64_t hbm_budget_bytes;   /* staging memory of the launch slots (inputs + outputs) */
+  uint32_t max_inflight;       /* launch slots on the device at once */
+  uint32_t max_batch_samples;  /* samples packed into one launch slot */
   int32_t device;
+  int32_t reserved;
+  uint64_t max_queued_samples; /* samples waiting for a slot before submit refuses
+                                  (TM_ERR_BUSY); 0: 64 x max_batch_samples */
 } tm_server_config;
 
 int tm_serve_open(const tm_server_config *cfg, tm_machine *const *machines, uint32_t count,
                   tm_server **out);
-/* Queues a request; the input is copied before return.  Returns a request
- * id in *id.  Fails with TM_ERR_OOM if the request alone exceeds the
- * budget. */
+/* Queues a request; the input is copied before return (and dropped once it
+ * is staged for the device).  Returns a request id in *id.  Fails with
+ * TM_ERR_OOM if the request alone exceeds a launch slot, TM_ERR_BUSY if the
+ * queue is full. */
 int tm_serve_submit(tm_server *s, uint32_t machine, const uint8_t *problems, uint64_t n,
                     uint64_t *id);
-/* Non-blocking: 1 when done (result copied to out_classes / out_codes),
- * 0 while pending.  timeout_us > 0 waits up to that long. */
+/* Non-blocking: 1 when done (result copied to out_classes / out_codes; the
+ * request is released and its id becomes unknown to later polls), 0 while
+ * pending.  timeout_us > 0 waits up to that long. */
 int tm_serve_poll(tm_server *s, uint64_t id, int64_t *out_classes, uint8_t *out_codes,
                   uint64_t timeout_us);
-/* submit -> done latency of a completed request, microseconds */
+/* submit -> done latency of a completed request, microseconds (also after
+ * it was polled, for the last 65,536 polled requests) */
 int tm_serve_latency_us(tm_server *s, uint64_t id, double *us);
+/* out[5]: queued requests, queued samples, requests not yet polled, busy
+ * launch slots, launch slots */
+int tm_serve_stats(tm_server *s, uint64_t *out);
 int tm_serve_close(tm_server *s);
 
 #ifdef __cplusplus

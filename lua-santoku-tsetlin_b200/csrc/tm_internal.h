@@ -154,6 +154,34 @@ uint32_t predict_job_tiles(uint32_t n, uint32_t classes, uint32_t clauses, uint3
                            uint32_t *tpc);
 cudaError_t launch_predict_multi(const PredictJob *jobs_dev, uint32_t njobs, uint32_t total_tiles,
                                  cudaStream_t st);
+// A small predict job (k_predict_small_multi): samples s0 .. s0 + ns - 1
+// (ns <= 16) of x against a machine; blocks block0 .. block0 + classes *
+// cblocks - 1 of the launch.
+struct SmallJob {
+  const uint32_t *act;
+  const int32_t *lits;
+  const ClassDev *cls;
+  const uint32_t *x;
+  int32_t *sums;
+  uint32_t clauses, tol, classes, s0, ns, cblocks, block0, pad;
+};
+uint32_t small_job_blocks(uint32_t classes, uint32_t clauses, uint32_t *cblocks);
+cudaError_t launch_predict_small_multi(const SmallJob *jobs_dev, uint32_t njobs,
+                                       uint32_t total_blocks, cudaStream_t st);
+
+// One request of a serving launch: its staged byte rows, padded rows, vote
+// sums and output within the launch slot's buffers.
+struct ServeJob {
+  const uint8_t *raw;   // n rows of row_bytes
+  uint32_t *x;          // n rows of Wp words
+  int32_t *sums;        // n x classes
+  uint8_t *out;         // n int64 classes or n x ceil(classes / 8) code bytes
+  uint64_t row_bytes;
+  uint32_t n, Wp, classes, type;
+};
+cudaError_t launch_serve_repack(const ServeJob *jobs_dev, uint32_t njobs, cudaStream_t st);
+cudaError_t launch_serve_finalize(const ServeJob *jobs_dev, uint32_t njobs, cudaStream_t st);
+
 // Predicts of at most this many samples read each clause row once with one
 // warp per row (k_predict_small) instead of the 64 x 64 tiles.
 constexpr uint32_t TM_SMALL_N_MAX = 32;

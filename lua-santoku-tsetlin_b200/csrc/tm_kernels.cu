@@ -1573,15 +1573,15 @@ __device__ __forceinline__ uint4 ld_stream16(const void *p) {
 }
 
 template <int NS>
-__global__ void __launch_bounds__(256)
-    k_predict_small(const uint32_t *__restrict__ act, const int32_t *__restrict__ lits,
-                    const ClassDev *__restrict__ cls, uint32_t clauses, uint32_t tol,
-                    const uint32_t *__restrict__ x, uint32_t s0, uint32_t ns, uint32_t classes,
-                    int32_t *__restrict__ sums) {
-  const uint32_t h = blockIdx.y;
-  const ClassDev C = cls[h];
+__device__ __forceinline__ void predict_small_body(const uint32_t *__restrict__ act,
+                                                   const int32_t *__restrict__ lits,
+                                                   const ClassDev &C, uint32_t h, uint32_t cblock,
+                                                   uint32_t clauses, uint32_t tol,
+                                                   const uint32_t *__restrict__ x, uint32_t s0,
+                                                   uint32_t ns, uint32_t classes,
+                                                   int32_t *__restrict__ sums) {
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint32_t cb = blockIdx.x * TM_SMALL_CPB;
+  const uint32_t cb = cblock * TM_SMALL_CPB;
   const uint32_t ce = cb + TM_SMALL_CPB < clauses ? cb + TM_SMALL_CPB : clauses;
   const uint32_t Q = C.Wp >> 2, qlast = (C.W - 1) >> 2, klast = (C.W - 1) & 3;
   const uint4 *xr = (const uint4 *)(x + C.x_off + (uint64_t)s0 * C.Wp);
@@ -1631,6 +1631,36 @@ __global__ void __launch_bounds__(256)
 }
 
 template <int NS>
+__global__ void __launch_bounds__(256)
+    k_predict_small(const uint32_t *__restrict__ act, const int32_t *__restrict__ lits,
+                    const ClassDev *__restrict__ cls, uint32_t clauses, uint32_t tol,
+                    const uint32_t *__restrict__ x, uint32_t s0, uint32_t ns, uint32_t classes,
+                    int32_t *__restrict__ sums) {
+  const ClassDev C = cls[blockIdx.y];
+  predict_small_body<NS>(act, lits, C, blockIdx.y, blockIdx.x, clauses, tol, x, s0, ns, classes,
+                         sums);
+}
+
+// Many small predict jobs (at most 16 samples each, any machines) in one
+// launch: block b serves (class, clause block) b - jobs[j].block0 of the job
+// j whose blocks contain b (jobs in ascending block0).
+__global__ void __launch_bounds__(256, 2)
+    k_predict_small_multi(const SmallJob *__restrict__ jobs, uint32_t njobs) {
+  uint32_t lo = 0, hi = njobs;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (jobs[mid].block0 <= blockIdx.x) lo = mid;
+    else hi = mid;
+  }
+  const SmallJob J = jobs[lo];
+  const uint32_t t = blockIdx.x - J.block0;
+  const uint32_t h = t / J.cblocks;
+  const ClassDev C = J.cls[h];
+  predict_small_body<16>(J.act, J.lits, C, h, t % J.cblocks, J.clauses, J.tol, J.x, J.s0, J.ns,
+                         J.classes, J.sums);
+}
+
+template <int NS>
 static void small_launch(dim3 grid, cudaStream_t st, const uint32_t *act, const int32_t *lits,
                          const ClassDev *cls, uint32_t clauses, uint32_t tol, const uint32_t *x,
                          uint32_t s0, uint32_t ns, uint32_t classes, int32_t *sums) {
@@ -1660,6 +1690,74 @@ cudaError_t launch_predict(const uint32_t *act, const int32_t *lits, const Class
   const uint32_t tpc = (clauses + PT_C - 1) / PT_C;
   dim3 grid((n + PT_S - 1) / PT_S, classes * tpc);
   k_predict<<<grid, 256, 0, st>>>(act, lits, cls, clauses, tpc, tol, x, n, classes, sums);
+  return cudaGetLastError();
+}
+
+uint32_t small_job_blocks(uint32_t classes, uint32_t clauses, uint32_t *cblocks) {
+  *cblocks = (clauses + TM_SMALL_CPB - 1) / TM_SMALL_CPB;
+  return *cblocks * classes;
+}
+
+cudaError_t launch_predict_small_multi(const SmallJob *jobs_dev, uint32_t njobs,
+                                       uint32_t total_blocks, cudaStream_t st) {
+  if (!njobs || !total_blocks) return cudaSuccess;
+  k_predict_small_multi<<<total_blocks, 256, 0, st>>>(jobs_dev, njobs);
+  return cudaGetLastError();
+}
+
+// Per request of a serving launch (grid.y = request): its reference byte
+// rows -> padded words (k_repack's rule), and its vote sums -> classes or
+// code bits (k_finalize's rule, capi.c:934-942, 982-990).
+__global__ void k_repack_multi(const ServeJob *__restrict__ jobs) {
+  const ServeJob J = jobs[blockIdx.y];
+  const uint64_t total = (uint64_t)J.n * J.Wp;
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t r = t / J.Wp;
+    const uint64_t b0 = (t - r * J.Wp) * 4;
+    const uint8_t *row = J.raw + r * J.row_bytes;
+    uint32_t v = 0;
+#pragma unroll
+    for (int b = 0; b < 4; b++)
+      if (b0 + b < J.row_bytes) v |= (uint32_t)row[b0 + b] << (8 * b);
+    J.x[t] = v;
+  }
+}
+
+__global__ void k_finalize_multi(const ServeJob *__restrict__ jobs) {
+  const ServeJob J = jobs[blockIdx.y];
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < J.n; s += gridDim.x * blockDim.x) {
+    const int32_t *r = J.sums + (uint64_t)s * J.classes;
+    if (J.type == 0) {
+      int32_t best = r[0];
+      uint32_t bc = 0;
+      for (uint32_t h = 1; h < J.classes; h++)
+        if (r[h] > best) {
+          best = r[h];
+          bc = h;
+        }
+      ((int64_t *)J.out)[s] = bc;
+    } else {
+      const uint32_t nb = (J.classes + 7) >> 3;
+      for (uint32_t b = 0; b < nb; b++) {
+        uint32_t byte = 0;
+        for (uint32_t q = 0; q < 8 && b * 8 + q < J.classes; q++)
+          byte |= (r[b * 8 + q] > 0 ? 1u : 0u) << q;
+        J.out[(uint64_t)s * nb + b] = (uint8_t)byte;
+      }
+    }
+  }
+}
+
+cudaError_t launch_serve_repack(const ServeJob *jobs_dev, uint32_t njobs, cudaStream_t st) {
+  if (!njobs) return cudaSuccess;
+  k_repack_multi<<<dim3(64, njobs), 256, 0, st>>>(jobs_dev);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_serve_finalize(const ServeJob *jobs_dev, uint32_t njobs, cudaStream_t st) {
+  if (!njobs) return cudaSuccess;
+  k_finalize_multi<<<dim3(16, njobs), 256, 0, st>>>(jobs_dev);
   return cudaGetLastError();
 }
 

@@ -4,17 +4,23 @@
 //
 // A worker thread owns S launch slots (one CUDA stream, pinned host staging
 // and device buffers each; S is bounded by max_inflight and by how many
-// slots the HBM budget pays for).  It repeatedly
-//   1. retires slots whose completion event has fired: results are copied
-//      to their requests, which become visible to tm_serve_poll;
-//   2. fills every free slot with the oldest queued request and every later
-//      queued request for the same machine that still fits the slot
-//      (max_batch_samples), then launches repack -> predict -> finalize and
-//      the result copy on the slot's stream.
-// Requests that arrive while slots are busy are admitted as soon as a slot
-// frees up, and the slots' streams overlap on the device.  Predict is
-// independent per sample, so each request's result is the same alone or
-// packed with others.
+// slots the HBM budget pays for).  Whenever a slot is free and requests are
+// queued, it takes the queued requests in arrival order -- for any of the
+// resident machines -- while they fit the slot (max_batch_samples, at most
+// TM_SERVE_MAX_PACK requests), and outside the server lock stages their rows
+// into the slot's pinned buffer (dropping each request's copy of its
+// input), then launches on the slot's stream: one copy of the rows, one
+// repack of every request's rows, the predict kernels of every request
+// (requests of at most 32 samples as warp-per-clause jobs reading each
+// clause row once, larger ones as 64 x 64 tiles; each kind for all requests
+// and machines in one launch), the finalize of every request and one copy
+// of the results.  A host function queued behind the copy completes the
+// slot's requests and frees the slot the moment the GPU is done.  Requests
+// that arrive while slots are busy are admitted as slots free up, and the
+// slots' streams overlap on the device.  Predict is independent per
+// sample, so each request's result is the same alone or packed with
+// others.  The queue is bounded (max_queued_samples): a request beyond it
+// is refused with TM_ERR_BUSY rather than left to wait without limit.
 #include <stdio.h>
 #include <string.h>
 
@@ -25,6 +31,7 @@
 #include <map>
 #include <mutex>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/tsetlin_b200.h"
@@ -35,26 +42,32 @@ using clk = std::chrono::steady_clock;
 
 namespace {
 
+constexpr uint32_t TM_SERVE_MAX_PACK = 64;     // requests per launch slot
+constexpr size_t TM_SERVE_LATENCY_KEEP = 1 << 16;  // polled requests whose latency is kept
+
 struct Request {
   uint64_t id;
   uint32_t machine;
   uint64_t n;
-  std::vector<uint8_t> input;
+  std::vector<uint8_t> input;   // dropped once staged
   std::vector<uint8_t> result;  // int64 classes or code bytes
   clk::time_point t_submit, t_done;
   bool done = false;
 };
 
 struct Slot {
+  tm_server *srv = nullptr;
   cudaStream_t st = nullptr;
-  cudaEvent_t ev = nullptr;
-  uint8_t *h_in = nullptr, *h_out = nullptr;  // pinned
-  uint8_t *d_raw = nullptr, *d_out = nullptr;
+  uint8_t *h_in = nullptr, *h_out = nullptr, *h_jobs = nullptr;  // pinned
+  uint8_t *d_raw = nullptr, *d_out = nullptr, *d_jobs = nullptr;
   uint32_t *d_x = nullptr;
   int32_t *d_sums = nullptr;
   std::vector<Request *> reqs;
+  std::vector<uint64_t> out_off;  // each request's result offset in h_out
   bool busy = false;
 };
+
+uint64_t round_up(uint64_t v, uint64_t a) { return (v + a - 1) / a * a; }
 
 }  // namespace
 
@@ -62,11 +75,14 @@ struct tm_server {
   tm_server_config cfg{};
   std::vector<MachineView> mv;
   std::vector<Slot> slots;
-  uint64_t cap_in = 0, cap_out = 0, cap_x = 0, cap_sums = 0;
+  uint64_t cap_in = 0, cap_out = 0, cap_x = 0, cap_sums = 0, cap_jobs = 0;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::deque<Request *> queue;
-  std::map<uint64_t, Request *> all;
+  uint64_t queued_samples = 0;
+  std::unordered_map<uint64_t, Request *> live;  // submitted, not yet polled done
+  std::unordered_map<uint64_t, double> latency;   // polled: submit -> done, microseconds
+  std::deque<uint64_t> latency_order;
   uint64_t next_id = 1;
   bool stop = false;
   std::thread worker;
@@ -77,113 +93,158 @@ static uint64_t out_bytes(const MachineView &v, uint64_t n) {
   return v.type == TM_CLASSIFIER ? n * 8 : n * v.class_chunks;
 }
 
-static bool launch_slot(tm_server *s, Slot &sl) {
-  const MachineView &v = s->mv[sl.reqs[0]->machine];
-  uint64_t n = 0;
-  for (Request *r : sl.reqs) {
-    memcpy(sl.h_in + n * v.input_chunks, r->input.data(), r->n * v.input_chunks);
-    n += r->n;
+// CUDA runs this on its own thread once the slot's result copy is done: it
+// completes the slot's requests and frees the slot (no CUDA calls here).
+static void CUDART_CB slot_done(void *p) {
+  Slot *sl = (Slot *)p;
+  tm_server *s = sl->srv;
+  const clk::time_point now = clk::now();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    for (size_t i = 0; i < sl->reqs.size(); i++) {
+      Request *r = sl->reqs[i];
+      const uint64_t b = out_bytes(s->mv[r->machine], r->n);
+      r->result.assign(sl->h_out + sl->out_off[i], sl->h_out + sl->out_off[i] + b);
+      r->t_done = now;
+      r->done = true;
+    }
+    sl->reqs.clear();
+    sl->busy = false;
   }
-  cudaError_t e = cudaMemcpyAsync(sl.d_raw, sl.h_in, n * v.input_chunks, cudaMemcpyHostToDevice, sl.st);
-  if (e == cudaSuccess)
-    e = launch_repack(sl.d_raw, n, v.input_chunks, v.input_chunks, sl.d_x, v.Wp, sl.st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(sl.d_sums, 0, n * v.classes * 4, sl.st);
-  if (e == cudaSuccess)
-    e = launch_predict(v.act, v.lits, v.cls, nullptr, v.classes, v.clauses, v.tol, sl.d_x,
-                       (uint32_t)n, sl.d_sums, sl.st);
-  if (e == cudaSuccess)
-    e = launch_finalize(sl.d_sums, (uint32_t)n, v.classes, (int32_t)v.type,
-                        v.type == TM_CLASSIFIER ? (int64_t *)sl.d_out : nullptr,
-                        v.type == TM_ENCODER ? sl.d_out : nullptr, nullptr, sl.st);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(sl.h_out, sl.d_out, out_bytes(v, n), cudaMemcpyDeviceToHost, sl.st);
-  if (e == cudaSuccess) e = cudaEventRecord(sl.ev, sl.st);
-  return e == cudaSuccess;
+  s->cv_done.notify_all();
+  s->cv_work.notify_one();
 }
 
-static void retire_slot(tm_server *s, Slot &sl) {
-  const MachineView &v = s->mv[sl.reqs[0]->machine];
-  uint64_t off = 0;
-  const clk::time_point now = clk::now();
-  for (Request *r : sl.reqs) {
-    const uint64_t b = out_bytes(v, r->n);
-    r->result.assign(sl.h_out + off, sl.h_out + off + b);
-    off += b;
-    r->t_done = now;
-    r->done = true;
+// Stages the slot's requests and queues its launches (called without the
+// server lock: the slot and its requests belong to the worker until
+// slot_done).
+static cudaError_t launch_slot(tm_server *s, Slot &sl) {
+  const uint32_t R = (uint32_t)sl.reqs.size();
+  ServeJob *sj = (ServeJob *)sl.h_jobs;
+  SmallJob *mj = (SmallJob *)(sl.h_jobs + round_up(TM_SERVE_MAX_PACK * sizeof(ServeJob), 256));
+  PredictJob *pj = (PredictJob *)((uint8_t *)mj +
+                                  round_up(2 * TM_SERVE_MAX_PACK * sizeof(SmallJob), 256));
+  const size_t o_mj = (uint8_t *)mj - sl.h_jobs, o_pj = (uint8_t *)pj - sl.h_jobs;
+  uint64_t in_off = 0, x_off = 0, s_off = 0, o_off = 0;
+  uint32_t nsmall = 0, npred = 0, small_blocks = 0, tiles = 0;
+  sl.out_off.assign(R, 0);
+  for (uint32_t i = 0; i < R; i++) {
+    Request *r = sl.reqs[i];
+    const MachineView &v = s->mv[r->machine];
+    memcpy(sl.h_in + in_off, r->input.data(), r->input.size());
+    std::vector<uint8_t>().swap(r->input);
+    ServeJob &J = sj[i];
+    J.raw = sl.d_raw + in_off;
+    J.x = sl.d_x + x_off;
+    J.sums = sl.d_sums + s_off;
+    J.out = sl.d_out + o_off;
+    J.row_bytes = v.input_chunks;
+    J.n = (uint32_t)r->n;
+    J.Wp = v.Wp;
+    J.classes = v.classes;
+    J.type = v.type;
+    if (r->n <= TM_SMALL_N_MAX) {
+      for (uint32_t s0 = 0; s0 < r->n; s0 += 16) {
+        SmallJob &M = mj[nsmall++];
+        M = SmallJob{v.act, v.lits, v.cls, J.x, J.sums, v.clauses, v.tol, v.classes, s0,
+                     (uint32_t)std::min<uint64_t>(16, r->n - s0), 0, small_blocks, 0};
+        small_blocks += small_job_blocks(v.classes, v.clauses, &M.cblocks);
+      }
+    } else {
+      PredictJob &P = pj[npred++];
+      P = PredictJob{};
+      P.act = v.act;
+      P.lits = v.lits;
+      P.cls = v.cls;
+      P.x = J.x;
+      P.sums = J.sums;
+      P.clauses = v.clauses;
+      P.tol = v.tol;
+      P.n = (uint32_t)r->n;
+      P.classes = v.classes;
+      P.tile0 = tiles;
+      tiles += predict_job_tiles(P.n, v.classes, v.clauses, &P.stiles, &P.tpc);
+    }
+    sl.out_off[i] = o_off;
+    in_off = round_up(in_off + r->n * v.input_chunks, 16);
+    x_off = round_up(x_off + r->n * v.Wp, 4);
+    s_off = round_up(s_off + r->n * v.classes, 4);
+    o_off = round_up(o_off + out_bytes(v, r->n), 16);
   }
-  sl.reqs.clear();
-  sl.busy = false;
+  cudaError_t e = cudaMemcpyAsync(sl.d_raw, sl.h_in, in_off, cudaMemcpyHostToDevice, sl.st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(sl.d_jobs, sl.h_jobs, o_pj + npred * sizeof(PredictJob),
+                        cudaMemcpyHostToDevice, sl.st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(sl.d_sums, 0, s_off * 4, sl.st);
+  if (e == cudaSuccess) e = launch_serve_repack((const ServeJob *)sl.d_jobs, R, sl.st);
+  if (e == cudaSuccess)
+    e = launch_predict_small_multi((const SmallJob *)(sl.d_jobs + o_mj), nsmall, small_blocks,
+                                   sl.st);
+  if (e == cudaSuccess)
+    e = launch_predict_multi((const PredictJob *)(sl.d_jobs + o_pj), npred, tiles, sl.st);
+  if (e == cudaSuccess) e = launch_serve_finalize((const ServeJob *)sl.d_jobs, R, sl.st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(sl.h_out, sl.d_out, o_off, cudaMemcpyDeviceToHost, sl.st);
+  if (e == cudaSuccess) e = cudaLaunchHostFunc(sl.st, slot_done, &sl);
+  return e;
 }
 
 static void worker_main(tm_server *s) {
   cudaSetDevice(s->cfg.device);
   std::unique_lock<std::mutex> lk(s->mu);
   while (true) {
-    bool progressed = false;
-    for (Slot &sl : s->slots) {
-      if (sl.busy && cudaEventQuery(sl.ev) == cudaSuccess) {
-        retire_slot(s, sl);
-        progressed = true;
-      }
-    }
-    if (progressed) s->cv_done.notify_all();
-    for (Slot &sl : s->slots) {
-      if (sl.busy || s->queue.empty()) continue;
-      Request *head = s->queue.front();
-      s->queue.pop_front();
-      sl.reqs.push_back(head);
-      uint64_t n = head->n;
-      for (auto it = s->queue.begin(); it != s->queue.end();) {
-        Request *r = *it;
-        if (r->machine == head->machine && n + r->n <= s->cfg.max_batch_samples) {
-          sl.reqs.push_back(r);
-          n += r->n;
-          it = s->queue.erase(it);
-        } else {
-          ++it;
+    Slot *free_slot = nullptr;
+    s->cv_work.wait(lk, [&] {
+      if (s->stop) return true;
+      if (s->queue.empty()) return false;
+      for (Slot &sl : s->slots)
+        if (!sl.busy) {
+          free_slot = &sl;
+          return true;
         }
-      }
-      sl.busy = true;
-      if (!launch_slot(s, sl)) {
-        s->error = TM_ERR_CUDA;
-        s->stop = true;
-      }
-      progressed = true;
-    }
+      return false;
+    });
     if (s->stop) break;
-    bool any_busy = false;
-    for (Slot &sl : s->slots) any_busy |= sl.busy;
-    if (!progressed) {
-      if (any_busy) {
-        lk.unlock();
-        std::this_thread::sleep_for(std::chrono::microseconds(20));
-        lk.lock();
-      } else {
-        s->cv_work.wait(lk, [&] { return s->stop || !s->queue.empty(); });
-      }
+    Slot &sl = *free_slot;
+    // the oldest queued requests, any machine, while they fit the slot
+    uint64_t n = 0;
+    while (!s->queue.empty() && sl.reqs.size() < TM_SERVE_MAX_PACK) {
+      Request *r = s->queue.front();
+      if (!sl.reqs.empty() && n + r->n > s->cfg.max_batch_samples) break;
+      s->queue.pop_front();
+      sl.reqs.push_back(r);
+      n += r->n;
+    }
+    s->queued_samples -= n;
+    sl.busy = true;
+    lk.unlock();
+    const cudaError_t e = launch_slot(s, sl);
+    lk.lock();
+    if (e != cudaSuccess) {
+      s->error = TM_ERR_CUDA;
+      s->stop = true;
+      break;
     }
   }
-  for (Slot &sl : s->slots)
-    if (sl.busy) {
-      cudaEventSynchronize(sl.ev);
-      retire_slot(s, sl);
-    }
+  lk.unlock();
+  // drain: every queued launch completes its requests through slot_done
+  for (Slot &sl : s->slots) cudaStreamSynchronize(sl.st);
   s->cv_done.notify_all();
 }
 
 static void free_server(tm_server *s) {
   for (Slot &sl : s->slots) {
     if (sl.st) cudaStreamDestroy(sl.st);
-    if (sl.ev) cudaEventDestroy(sl.ev);
     if (sl.h_in) cudaFreeHost(sl.h_in);
     if (sl.h_out) cudaFreeHost(sl.h_out);
+    if (sl.h_jobs) cudaFreeHost(sl.h_jobs);
     if (sl.d_raw) cudaFree(sl.d_raw);
     if (sl.d_out) cudaFree(sl.d_out);
+    if (sl.d_jobs) cudaFree(sl.d_jobs);
     if (sl.d_x) cudaFree(sl.d_x);
     if (sl.d_sums) cudaFree(sl.d_sums);
   }
-  for (auto &kv : s->all) delete kv.second;
+  for (Request *r : s->queue) s->live.erase(r->id), delete r;
+  for (auto &kv : s->live) delete kv.second;
   delete s;
 }
 
@@ -195,6 +256,7 @@ extern "C" int tm_serve_open(const tm_server_config *cfg, tm_machine *const *mac
   s->cfg = *cfg;
   if (!s->cfg.max_batch_samples) s->cfg.max_batch_samples = 8192;
   if (!s->cfg.max_inflight) s->cfg.max_inflight = 4;
+  if (!s->cfg.max_queued_samples) s->cfg.max_queued_samples = 64ull * s->cfg.max_batch_samples;
   cudaSetDevice(s->cfg.device);
   for (uint32_t i = 0; i < count; i++) {
     MachineView v{};
@@ -209,14 +271,18 @@ extern "C" int tm_serve_open(const tm_server_config *cfg, tm_machine *const *mac
     }
     s->mv.push_back(v);
   }
-  const uint64_t B = s->cfg.max_batch_samples;
+  // a slot holds up to max_batch_samples of the widest machine, plus the
+  // alignment of up to TM_SERVE_MAX_PACK requests
+  const uint64_t B = s->cfg.max_batch_samples, P = TM_SERVE_MAX_PACK;
   for (const MachineView &v : s->mv) {
-    s->cap_in = std::max<uint64_t>(s->cap_in, B * v.input_chunks);
-    s->cap_x = std::max<uint64_t>(s->cap_x, B * v.Wp * 4);
-    s->cap_sums = std::max<uint64_t>(s->cap_sums, B * v.classes * 4);
-    s->cap_out = std::max<uint64_t>(s->cap_out, out_bytes(v, B));
+    s->cap_in = std::max<uint64_t>(s->cap_in, B * v.input_chunks + 16 * P);
+    s->cap_x = std::max<uint64_t>(s->cap_x, (B * v.Wp + 4 * P) * 4);
+    s->cap_sums = std::max<uint64_t>(s->cap_sums, (B * v.classes + 4 * P) * 4);
+    s->cap_out = std::max<uint64_t>(s->cap_out, out_bytes(v, B) + 16 * P);
   }
-  const uint64_t per_slot = s->cap_in + s->cap_x + s->cap_sums + s->cap_out;
+  s->cap_jobs = round_up(P * sizeof(ServeJob), 256) + round_up(2 * P * sizeof(SmallJob), 256) +
+                P * sizeof(PredictJob);
+  const uint64_t per_slot = s->cap_in + s->cap_x + s->cap_sums + s->cap_out + s->cap_jobs;
   uint64_t nslots = s->cfg.hbm_budget_bytes ? s->cfg.hbm_budget_bytes / per_slot : s->cfg.max_inflight;
   nslots = std::min<uint64_t>(nslots, s->cfg.max_inflight);
   if (nslots == 0) {
@@ -225,12 +291,14 @@ extern "C" int tm_serve_open(const tm_server_config *cfg, tm_machine *const *mac
   }
   s->slots.resize(nslots);
   for (Slot &sl : s->slots) {
+    sl.srv = s;
     bool ok = cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking) == cudaSuccess &&
-              cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming) == cudaSuccess &&
               cudaHostAlloc(&sl.h_in, s->cap_in, cudaHostAllocDefault) == cudaSuccess &&
               cudaHostAlloc(&sl.h_out, s->cap_out, cudaHostAllocDefault) == cudaSuccess &&
+              cudaHostAlloc(&sl.h_jobs, s->cap_jobs, cudaHostAllocDefault) == cudaSuccess &&
               tmb_dev_malloc((void **)&sl.d_raw, s->cap_in) == cudaSuccess &&
               tmb_dev_malloc((void **)&sl.d_out, s->cap_out) == cudaSuccess &&
+              tmb_dev_malloc((void **)&sl.d_jobs, s->cap_jobs) == cudaSuccess &&
               tmb_dev_malloc((void **)&sl.d_x, s->cap_x) == cudaSuccess &&
               tmb_dev_malloc((void **)&sl.d_sums, s->cap_sums) == cudaSuccess;
     if (!ok) {
@@ -260,9 +328,17 @@ extern "C" int tm_serve_submit(tm_server *s, uint32_t machine, const uint8_t *pr
       delete r;
       return tmb_fail(s->error ? s->error : TM_ERR_STATE, "serve_submit: server stopped");
     }
+    if (s->queued_samples + n > s->cfg.max_queued_samples) {
+      char msg[96];
+      snprintf(msg, sizeof msg, "serve_submit: queue full (%llu samples waiting)",
+               (unsigned long long)s->queued_samples);
+      delete r;
+      return tmb_fail(TM_ERR_BUSY, msg);
+    }
     r->id = s->next_id++;
-    s->all[r->id] = r;
+    s->live[r->id] = r;
     s->queue.push_back(r);
+    s->queued_samples += n;
     *id = r->id;
   }
   s->cv_work.notify_one();
@@ -273,8 +349,8 @@ extern "C" int tm_serve_poll(tm_server *s, uint64_t id, int64_t *out_classes, ui
                              uint64_t timeout_us) {
   if (!s) return tmb_fail(TM_ERR_ARG, "serve_poll: null server");
   std::unique_lock<std::mutex> lk(s->mu);
-  auto it = s->all.find(id);
-  if (it == s->all.end()) return tmb_fail(TM_ERR_ARG, "serve_poll: unknown request");
+  auto it = s->live.find(id);
+  if (it == s->live.end()) return tmb_fail(TM_ERR_ARG, "serve_poll: unknown or already polled request");
   Request *r = it->second;
   if (!r->done && timeout_us)
     s->cv_done.wait_for(lk, std::chrono::microseconds(timeout_us),
@@ -283,15 +359,43 @@ extern "C" int tm_serve_poll(tm_server *s, uint64_t id, int64_t *out_classes, ui
   const MachineView &v = s->mv[r->machine];
   if (v.type == TM_CLASSIFIER && out_classes) memcpy(out_classes, r->result.data(), r->result.size());
   if (v.type == TM_ENCODER && out_codes) memcpy(out_codes, r->result.data(), r->result.size());
+  // the request is released; its latency stays queryable for a while
+  s->latency[id] = std::chrono::duration<double, std::micro>(r->t_done - r->t_submit).count();
+  s->latency_order.push_back(id);
+  while (s->latency_order.size() > TM_SERVE_LATENCY_KEEP) {
+    s->latency.erase(s->latency_order.front());
+    s->latency_order.pop_front();
+  }
+  s->live.erase(it);
+  delete r;
   return 1;
 }
 
 extern "C" int tm_serve_latency_us(tm_server *s, uint64_t id, double *us) {
   if (!s || !us) return tmb_fail(TM_ERR_ARG, "serve_latency_us: bad arguments");
   std::lock_guard<std::mutex> lk(s->mu);
-  auto it = s->all.find(id);
-  if (it == s->all.end() || !it->second->done) return tmb_fail(TM_ERR_ARG, "serve_latency_us: request not done");
+  auto lt = s->latency.find(id);
+  if (lt != s->latency.end()) {
+    *us = lt->second;
+    return TM_OK;
+  }
+  auto it = s->live.find(id);
+  if (it == s->live.end() || !it->second->done)
+    return tmb_fail(TM_ERR_ARG, "serve_latency_us: request not done");
   *us = std::chrono::duration<double, std::micro>(it->second->t_done - it->second->t_submit).count();
+  return TM_OK;
+}
+
+extern "C" int tm_serve_stats(tm_server *s, uint64_t *out) {
+  if (!s || !out) return tmb_fail(TM_ERR_ARG, "serve_stats: bad arguments");
+  std::lock_guard<std::mutex> lk(s->mu);
+  uint32_t busy = 0;
+  for (const Slot &sl : s->slots) busy += sl.busy ? 1 : 0;
+  out[0] = s->queue.size();
+  out[1] = s->queued_samples;
+  out[2] = s->live.size();
+  out[3] = busy;
+  out[4] = s->slots.size();
   return TM_OK;
 }
 

@@ -38,9 +38,9 @@ def _machine(tm, kind, features, classes, clauses, seed):
     return t
 
 
-def _open(tm, machines, budget, inflight=4, batch=4096):
+def _open(tm, machines, budget, inflight=4, batch=4096, queued=0):
     L = tm.lib()
-    cfg = tm._ServerConfig(budget, inflight, batch, 0)
+    cfg = tm._ServerConfig(budget, inflight, batch, 0, 0, queued)
     hs = (ctypes.c_void_p * len(machines))(*[m.handle.value for m in machines])
     srv = ctypes.c_void_p()
     rc = L.tm_serve_open(ctypes.byref(cfg), hs, len(machines), ctypes.byref(srv))
@@ -93,6 +93,14 @@ def test_alone_equals_mixed(tm):
         assert L.tm_serve_latency_us(srv, ids[i], ctypes.byref(us)) == 0
         lat.append(us.value)
     assert all(v > 0 for v in lat)
+    # a polled request is released: its id is unknown to a second poll, its
+    # latency stays readable, and nothing is left waiting
+    out = np.zeros(4096, dtype=np.int64)
+    assert L.tm_serve_poll(srv, ids[0], out.ctypes.data, out.ctypes.data, 0) < 0
+    assert b"unknown" in L.tm_last_error()
+    st = np.zeros(5, dtype=np.uint64)
+    assert L.tm_serve_stats(srv, st.ctypes.data) == 0
+    assert st[0] == 0 and st[1] == 0 and st[2] == 0 and st[3] == 0 and st[4] >= 1
     assert L.tm_serve_close(srv) == 0
 
 
@@ -110,4 +118,70 @@ def test_budget_and_oversized_requests(tm):
     out = np.zeros(64, dtype=np.int64)
     assert L.tm_serve_poll(srv, rid.value, out.ctypes.data, None, 10_000_000) == 1
     assert np.array_equal(out, m.predict(x, 64))
+    assert L.tm_serve_close(srv) == 0
+
+
+def test_queue_bound_refuses_with_busy(tm):
+    """A full queue refuses new requests with TM_ERR_BUSY (-7) instead of
+    letting the backlog grow without bound; refused requests can be
+    submitted again once the queue drains, and accepted ones complete
+    exactly."""
+    L = tm.lib()
+    m = _machine(tm, "classifier", 4096, 6, 64, 7)
+    # one slot of 256 samples, at most 512 samples waiting
+    rc, srv = _open(tm, [m], budget=1 << 30, inflight=1, batch=256, queued=512)
+    assert rc == 0, L.tm_last_error()
+    rng = np.random.default_rng(3)
+    x = np.packbits(np.concatenate([(b := rng.random((256, 4096)) < 0.2), ~b], axis=1), axis=1,
+                    bitorder="little").ravel()
+    want = m.predict(x, 256)
+    ok, busy = [], 0
+    for _ in range(40):
+        rid = ctypes.c_uint64()
+        rc = L.tm_serve_submit(srv, 0, x.ctypes.data, 256, ctypes.byref(rid))
+        if rc == 0:
+            ok.append(rid.value)
+        else:
+            assert rc == -7 and b"queue full" in L.tm_last_error()
+            busy += 1
+    assert busy > 0 and len(ok) >= 2
+    for rid in ok:
+        out = np.zeros(256, dtype=np.int64)
+        assert L.tm_serve_poll(srv, rid, out.ctypes.data, None, 30_000_000) == 1
+        assert np.array_equal(out, want)
+    rid = ctypes.c_uint64()
+    assert L.tm_serve_submit(srv, 0, x.ctypes.data, 256, ctypes.byref(rid)) == 0
+    out = np.zeros(256, dtype=np.int64)
+    assert L.tm_serve_poll(srv, rid.value, out.ctypes.data, None, 30_000_000) == 1
+    assert np.array_equal(out, want)
+    assert L.tm_serve_close(srv) == 0
+
+
+def test_small_requests_of_many_machines_share_launches(tm):
+    """Requests of 1-40 samples for different machines -- packed into the
+    same launch slots, the small ones as warp-per-clause jobs -- each equal
+    tm_predict alone."""
+    L = tm.lib()
+    ms = [_machine(tm, "classifier", 16384, 5, 24, 11), _machine(tm, "encoder", 700, 13, 16, 12),
+          _machine(tm, "classifier", 784, 10, 40, 13)]
+    infos = [m.info() for m in ms]
+    rc, srv = _open(tm, ms, budget=1 << 30, inflight=2, batch=512)
+    assert rc == 0, L.tm_last_error()
+    rng = np.random.default_rng(9)
+    reqs = []
+    for i in range(90):
+        k = i % 3
+        n = int(rng.integers(1, 41))
+        feats = infos[k]["features"]
+        x = np.packbits(np.concatenate([(b := rng.random((n, feats)) < 0.1), ~b], axis=1),
+                        axis=1, bitorder="little").ravel()
+        rid = ctypes.c_uint64()
+        assert L.tm_serve_submit(srv, k, x.ctypes.data, n, ctypes.byref(rid)) == 0
+        reqs.append((k, n, x, rid.value))
+    for k, n, x, rid in reqs:
+        info = infos[k]
+        out = np.zeros(n * (8 if info["type"] == 0 else info["class_chunks"]), dtype=np.uint8)
+        assert L.tm_serve_poll(srv, rid, out.ctypes.data, out.ctypes.data, 30_000_000) == 1
+        got = out.view(np.int64) if info["type"] == 0 else out
+        assert np.array_equal(got, ms[k].predict(x, n))
     assert L.tm_serve_close(srv) == 0
