@@ -886,6 +886,8 @@ def main():
                     help="search --impl reference: stop after this many measured CPU seconds")
     ap.add_argument("--profile-launch", default="", choices=["", "search"] + sorted(WORKLOADS),
                     help="run only the train launch a profiler capture looks at")
+    ap.add_argument("--epoch-times", type=int, default=0,
+                    help="c1/c0/c2: train this many epochs and print each epoch's kernel time")
     ap.add_argument("--requests", type=int, default=2000, help="serve: requests")
     ap.add_argument("--rate", type=float, default=5000.0, help="serve: arrivals per second")
     ap.add_argument("--hbm-budget", type=int, default=2048, help="serve: staging MB")
@@ -894,6 +896,9 @@ def main():
     args = ap.parse_args()
     if args.profile_launch and args.profile_launch != "search":
         run_profile_launch(args, WORKLOADS[args.profile_launch])
+        return
+    if args.epoch_times:
+        run_epoch_times(args, WORKLOADS[args.workload])
         return
     if args.workload == "search" or args.profile_launch == "search":
         if args.impl == "reference":
@@ -909,6 +914,40 @@ def main():
         run_reference(args, w)
     else:
         run_ours(args, w)
+
+
+def run_epoch_times(args, w):
+    """Device time of the train kernel in each of `--epoch-times` epochs of
+    one training (one launch per epoch: an `each` callback between epochs
+    that predicts 2,000 held-out samples)."""
+    import torch
+    import santoku_tsetlin as tm
+    d = make_data(w, 0)
+    n = w["n_train"]
+    nt = min(2000, w["n_test"])
+    lab_key = "y" if w["kind"] == "classifier" else "codes"
+    x = torch.from_numpy(np.ascontiguousarray(d["x"][:n])).cuda()
+    lab = torch.from_numpy(np.ascontiguousarray(d[lab_key][:n])).cuda()
+    xt = torch.from_numpy(np.ascontiguousarray(d["x"][n:n + nt])).cuda()
+    t = tm.create(w["kind"], create_table(w, seed=0))
+    t.stats_enable(True)
+    per, acc, last = [], [], [0.0]
+
+    def each(epoch):
+        st = t.stats()
+        per.append(st["train_kernel_ms"] - last[0])
+        last[0] = st["train_kernel_ms"]
+        if w["kind"] == "classifier":
+            acc.append(float((t.predict(xt, nt).cpu().numpy() == d["y"][n:n + nt]).mean()))
+        return True
+    tbl = train_table(w, x, lab)
+    tbl.update(iterations=args.epoch_times, each=each)
+    t.train(tbl)
+    st = t.stats()
+    print(json.dumps({"epoch_times": w["name"], "train_kernel_ms": per, "holdout_accuracy": acc,
+                      "mode": st["train_mode"], "cpw": st["train_cpw"],
+                      "mean_ms": float(np.mean(per))}), flush=True)
+    t.destroy()
 
 
 def run_profile_launch(args, w):

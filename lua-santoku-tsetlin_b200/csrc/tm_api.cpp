@@ -252,6 +252,13 @@ static int check_limits(tm_machine *m) {
   return TM_OK;
 }
 
+// A train-kernel variant a caller may pin: modes 0-3 with 1, 2 or 4
+// clauses per warp, or mode 4 with one of its configurations.
+static bool variant_ok(int mode, int cpw) {
+  if (mode == TM_MODE_WPT) return cpw >= 1 && cpw <= wpt_configs();
+  return mode >= -1 && mode <= TM_MODE_WARP && (cpw == 1 || cpw == 2 || cpw == 4);
+}
+
 extern "C" int tm_create(const tm_params *p, tm_machine **out) {
   if (!p || !out) return fail(TM_ERR_ARG, "null argument");
   *out = nullptr;
@@ -300,8 +307,7 @@ extern "C" int tm_create(const tm_params *p, tm_machine **out) {
     if (rw && rw[0] >= '0' && rw[0] <= '9') m->row_wait = (uint32_t)strtoul(rw, nullptr, 10);
     const char *v = getenv("TSETLIN_B200_VARIANT");
     int vm = -1, vc = 1;
-    if (v && sscanf(v, "%d:%d", &vm, &vc) >= 1 && vm >= 0 && vm <= TM_MODE_WARP &&
-        (vc == 1 || vc == 2 || vc == 4)) {
+    if (v && sscanf(v, "%d:%d", &vm, &vc) >= 1 && vm >= 0 && variant_ok(vm, vc)) {
       m->force_mode = vm;
       m->force_cpw = vc;
     }
@@ -369,8 +375,9 @@ extern "C" void tm_destroy(tm_machine *m) {
 
 extern "C" int tm_force_variant(tm_machine *m, int32_t mode, int32_t cpw) {
   if (!m) return fail(TM_ERR_ARG, "null machine");
-  if (mode < -1 || mode > TM_MODE_WARP || (cpw != 1 && cpw != 2 && cpw != 4))
-    return fail(TM_ERR_ARG, "force_variant: mode -1..3, clauses per warp 1, 2 or 4");
+  if (!variant_ok(mode, cpw))
+    return fail(TM_ERR_ARG, "force_variant: mode -1..3 with clauses per warp 1, 2 or 4, or mode 4 "
+                            "with a configuration 1..%d", wpt_configs());
   m->force_mode = mode;
   m->force_cpw = cpw;
   return TM_OK;
@@ -565,6 +572,15 @@ static bool plan_mode(int mode, const TrainShape &sh, TrainPlan &p, int cpw = 1)
   p = TrainPlan{};
   p.mode = mode;
   p.cpw = cpw;
+  if (mode == TM_MODE_WPT) {
+    // cpw is the configuration id; the automata of 8-bit units only
+    if (sh.Bmin != 8 || sh.Bmax != 8) return false;
+    size_t bytes = 0;
+    const int occ = train_wpt_occupancy(cpw, sh.Wpmax, sh.smax, &bytes);
+    if (occ <= 0 || (int)bytes > sh.optin) return false;
+    p.grid = (int)std::min<uint64_t>(sh.units, (uint64_t)sh.sms * occ);
+    return true;
+  }
   if (cpw != 1 && (mode == TM_MODE_WARP || mode == TM_MODE_PAIR || sh.Bmin != 8 || sh.Bmax != 8))
     return false;
   if (mode == TM_MODE_WARP) {
@@ -616,6 +632,7 @@ static int heuristic_plan(const TrainShape &sh, const tm_machine *m0, TrainPlan 
 // per unit, or a 2-CTA cluster per unit.
 static uint64_t resident_units(const TrainPlan &p) {
   if (p.mode == TM_MODE_WARP) return (uint64_t)p.grid * 4;
+  if (p.mode == TM_MODE_WPT) return (uint64_t)p.grid;
   if (p.mode == TM_MODE_PAIR) return (uint64_t)p.grid / 2;
   return (uint64_t)p.grid;
 }
@@ -645,6 +662,10 @@ static int launch_plan(const TrainPlan &p, const TrainShape &sh, const std::vect
     CK(launch_train_warp((const TrainDev *)base, (const WorkItem *)(base + off_w),
                          (uint32_t)work.size(), counter, e0, e1, sh.Wpmax, sh.Bmin, sh.Bmax,
                          sh.smax, p.grid, st, (unsigned long long *)(err + 2)));
+  else if (p.mode == TM_MODE_WPT)
+    CK(launch_train_wpt(p.cpw, (const TrainDev *)base, (const WorkItem *)(base + off_w),
+                        (uint32_t)work.size(), counter, e0, e1, sh.Wpmax, sh.smax, m0->row_wait,
+                        p.grid, err, st));
   else
     CK(launch_train((const TrainDev *)base, (const WorkItem *)(base + off_w),
                     (uint32_t)work.size(), counter, e0, e1, lay, p.mode, sh.Bmin, sh.Bmax,
@@ -701,8 +722,15 @@ static int autotune_plan(std::vector<TrainJob> &jobs, const std::vector<TrainDev
     CK(cudaEventCreate(&m0->ev1));
   }
   std::vector<TrainPlan> cand;
-  for (int mode : {TM_MODE_WARP, TM_MODE_SMEM, TM_MODE_GLOBAL, TM_MODE_PAIR}) {
+  for (int mode : {TM_MODE_WARP, TM_MODE_SMEM, TM_MODE_GLOBAL, TM_MODE_PAIR, TM_MODE_WPT}) {
     if (mode == TM_MODE_WARP && m0->no_warp) continue;
+    if (mode == TM_MODE_WPT) {
+      for (int id = 1; id <= wpt_configs(); id++) {
+        TrainPlan p;
+        if (plan_mode(mode, sh, p, id)) cand.push_back(p);
+      }
+      continue;
+    }
     for (int cpw : {1, 2, 4}) {
       TrainPlan p;
       if (plan_mode(mode, sh, p, cpw)) cand.push_back(p);
@@ -1286,10 +1314,7 @@ static int search_round(tm_machine *const *ms, const tm_train_args *args, uint32
   std::vector<WorkItem> work;
   TrainShape sh{};
   build_tables(jobs, 0, 1, m0, joff, td, work, sh);
-  for (uint32_t i = 0; i < count; i++) {
-    td[i].gate = &d_state[i].live;
-    td[i].epoch_dev = d_epoch;
-  }
+  for (uint32_t i = 0; i < count; i++) td[i].gate = &d_state[i].live;
   // epoch 0's orders: the tuner's trial launches read them (the graph
   // rebuilds them for every epoch from the device epoch counter)
   for (auto &kv : pidx)
@@ -1356,19 +1381,25 @@ static int search_round(tm_machine *const *ms, const tm_train_args *args, uint32
       launches += 1 + kSortKernels;
     }
     if (ce == cudaSuccess) ce = cudaMemsetAsync(counter, 0, 4, st);
-    if (ce == cudaSuccess && timing) ce = cudaEventRecord(tk0, st);
+    // external event records: real events inside the graph, so that the
+    // train kernel's time can be read after each replay
+    if (ce == cudaSuccess && timing) ce = cudaEventRecordWithFlags(tk0, st, cudaEventRecordExternal);
     if (ce == cudaSuccess && !work.empty()) {
       if (plan.mode == TM_MODE_WARP)
         ce = launch_train_warp((const TrainDev *)tbase, (const WorkItem *)(tbase + off_w),
                                (uint32_t)work.size(), counter, 0, 1, sh.Wpmax, sh.Bmin, sh.Bmax,
                                sh.smax, plan.grid, st, (unsigned long long *)(d_err + 2));
+      else if (plan.mode == TM_MODE_WPT)
+        ce = launch_train_wpt(plan.cpw, (const TrainDev *)tbase, (const WorkItem *)(tbase + off_w),
+                              (uint32_t)work.size(), counter, 0, 1, sh.Wpmax, sh.smax,
+                              m0->row_wait, plan.grid, d_err, st);
       else
         ce = launch_train((const TrainDev *)tbase, (const WorkItem *)(tbase + off_w),
                           (uint32_t)work.size(), counter, 0, 1, lay, plan.mode, sh.Bmin, sh.Bmax,
                           plan.cpw, plan.grid, d_err, st);
       launches++;
     }
-    if (ce == cudaSuccess && timing) ce = cudaEventRecord(tk1, st);
+    if (ce == cudaSuccess && timing) ce = cudaEventRecordWithFlags(tk1, st, cudaEventRecordExternal);
     if (ce == cudaSuccess)
       ce = launch_lits_multi((const LitsJob *)(base + o_lj), count, maxC, st);
     if (ce == cudaSuccess)
@@ -1379,11 +1410,12 @@ static int search_round(tm_machine *const *ms, const tm_train_args *args, uint32
     if (ce == cudaSuccess && sa->patience)
       ce = launch_copy_multi((const CopyJob *)(base + o_cj), count, st);
     if (ce == cudaSuccess) ce = launch_tick(d_epoch, st);
+    if (ce == cudaSuccess) ce = launch_tick_machines((TrainDev *)tbase, count, st);
     if (ce == cudaSuccess)
       ce = cudaMemcpyAsync(h_state, d_state, count * sizeof(SearchState), cudaMemcpyDeviceToHost,
                            st);
     if (ce == cudaSuccess) ce = cudaMemcpyAsync(h_err, d_err, 4, cudaMemcpyDeviceToHost, st);
-    launches += 4 + (sa->patience ? 1 : 0);
+    launches += 5 + (sa->patience ? 1 : 0);
     cudaError_t ee = cudaStreamEndCapture(st, &graph);
     if (ce == cudaSuccess) ce = ee;
   }
@@ -1411,6 +1443,7 @@ static int search_round(tm_machine *const *ms, const tm_train_args *args, uint32
         m0->stats.search_train_ms += tms;
         m0->stats.train_kernel_ms += tms;
       }
+      cudaGetLastError();  // a failed timing query leaves no error behind
       m0->stats.search_epochs++;
     }
     m0->stats.kernel_launches += launches;

@@ -50,7 +50,6 @@ struct TrainDev {
   uint32_t epochs;          // epochs this machine trains in this launch group
   uint32_t epoch_base;      // draw-contract epoch index of local epoch 0
   const uint32_t *gate;     // optional: the machine's units are skipped while *gate == 0
-  const uint32_t *epoch_dev;  // optional: added to epoch_base (a graph replayed per epoch)
 };
 
 struct WorkItem {
@@ -124,6 +123,16 @@ cudaError_t launch_train_warp(const TrainDev *machines, const WorkItem *work, ui
 // The fused train kernels report through err[0] (status bits) and
 // err[2..3], a 64-bit count of active (unit, sample) steps -- the samples
 // each unit actually trained on after negative sampling.
+// k_train_wpt (tm_train_wpt.cu): one CTA per unit, every thread owning a
+// few words of all eight clauses, the automata held in registers and shared
+// memory; `cpw` of a plan with this mode is the configuration id (1-based).
+constexpr int TM_MODE_WPT = 4;
+int wpt_configs();
+int train_wpt_occupancy(int id, uint32_t Wpmax, uint32_t smax, size_t *smem_bytes);
+cudaError_t launch_train_wpt(int id, const TrainDev *machines, const WorkItem *work,
+                             uint32_t nwork, uint32_t *counter, uint32_t e_begin, uint32_t e_end,
+                             uint32_t Wpmax, uint32_t smax, uint32_t wait_limit, int grid,
+                             uint32_t *err, cudaStream_t st);
 cudaError_t launch_lits(const uint32_t *act, const ClassDev *cls, uint32_t classes,
                         uint32_t clauses, int32_t *lits, cudaStream_t st);
 cudaError_t launch_predict(const uint32_t *act, const int32_t *lits, const ClassDev *cls,
@@ -241,6 +250,9 @@ cudaError_t launch_search_score(const ScoreJob *jobs, SearchState *state, double
                                 int final_pass, cudaStream_t st);
 cudaError_t launch_copy_multi(const CopyJob *jobs, uint32_t njobs, cudaStream_t st);
 cudaError_t launch_tick(uint32_t *counter, cudaStream_t st);
+// epoch_base += 1 of every machine of a launch's device table (a graph
+// replayed once per epoch trains the next epoch on each replay)
+cudaError_t launch_tick_machines(TrainDev *machines, uint32_t count, cudaStream_t st);
 
 // Read-only view of a resident dense machine for the server (tm_serve.cpp).
 struct MachineView {

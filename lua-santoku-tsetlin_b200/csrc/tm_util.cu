@@ -432,6 +432,16 @@ cudaError_t launch_copy_multi(const CopyJob *jobs, uint32_t njobs, cudaStream_t 
 
 __global__ void k_tick(uint32_t *counter) { *counter += 1; }
 
+__global__ void k_tick_machines(TrainDev *machines, uint32_t count) {
+  for (uint32_t i = threadIdx.x; i < count; i += blockDim.x) machines[i].epoch_base += 1;
+}
+
+cudaError_t launch_tick_machines(TrainDev *machines, uint32_t count, cudaStream_t st) {
+  if (!count) return cudaSuccess;
+  k_tick_machines<<<1, 256, 0, st>>>(machines, count);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_tick(uint32_t *counter, cudaStream_t st) {
   k_tick<<<1, 1, 0, st>>>(counter);
   return cudaGetLastError();

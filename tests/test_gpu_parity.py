@@ -448,6 +448,12 @@ def test_every_train_variant_matches_oracle(tm, features):
     variants = [(0, 1), (0, 2), (0, 4), (1, 1), (1, 2), (1, 4), (2, 1)]
     if features <= 1024:
         variants.append((3, 1))
+    # the word-per-thread kernel's configurations that hold these rows
+    # (4500 features: 282 words -> 512 threads x 2 words; 784: 52 words)
+    wp = ((2 * features + 31) // 32 + 3) // 4 * 4
+    for cid, words in ((1, 1024), (2, 256), (3, 512), (4, 256), (5, 64)):
+        if wp <= words:
+            variants.append((4, cid))
     kind, tbl = ref_table(cfg, seed=31)
     for mode, cpw in variants:
         t = tm.create(kind, tbl)
@@ -464,6 +470,8 @@ def test_every_train_variant_matches_oracle(tm, features):
     t.force_variant(3, 2)
     with pytest.raises(tm.TsetlinError):
         t.force_variant(1, 3)
+    with pytest.raises(tm.TsetlinError):
+        t.force_variant(4, 9)
     with pytest.raises(tm.TsetlinError):  # the warp kernel has one clause layout
         t.train(train_table(kind, inp, 1))
     t.destroy()
@@ -486,8 +494,8 @@ def c1_multiwave():
     return cfg, inp, (m.actions(), m.state(), m.predict(inp["xt"], 300, scores=True)[1])
 
 
-@pytest.mark.parametrize("mode,cpw", [(-1, 1), (1, 1), (1, 2), (1, 4), (2, 1)],
-                         ids=["auto", "global1", "global2", "global4", "pair"])
+@pytest.mark.parametrize("mode,cpw", [(-1, 1), (1, 1), (1, 2), (1, 4), (2, 1), (4, 1)],
+                         ids=["auto", "global1", "global2", "global4", "pair", "wpt512"])
 def test_multiwave_wide_rows_match_oracle(tm, c1_multiwave, mode, cpw):
     cfg, inp, (wa, ws, wsc) = c1_multiwave
     kind, tbl = ref_table(cfg, seed=41)
