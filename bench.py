@@ -238,7 +238,19 @@ def balanced_chunks(classes, threads, at_most):
 #       --metrics smsp__inst_executed.sum python bench.py --profile-launch search
 #   ncu --clock-control none -k regex:k_train -c 1 --metrics smsp__inst_executed.sum \
 #       python bench.py --profile-launch c1_small
-INSTR_PER_PAIR = {}
+INSTR_PER_PAIR = {
+    # batched search rows (784 / 392 features), 64 machines, 6,000 samples:
+    # 64.31e9 / 105.91e6, 172.75e9 / 105.91e6, 274.95e9 / 105.91e6
+    ("search", 3, 1): 607.2,     # one warp per unit
+    ("search", 0, 2): 1631.1,    # CTA per unit, planes in shared memory, 2 clauses per warp
+    ("search", 1, 1): 2596.0,    # CTA per unit, count planes in global memory
+    # large sparse classifier rows (16,384 features), c1_small (1.091e6 active
+    # steps): 13.54e9 global planes; 11.66e9 word-per-thread (512 x 2 words)
+    ("c1", 1, 1): 12410.0,
+    ("c1_small", 1, 1): 12410.0,
+    ("c1", 4, 1): 10681.0,
+    ("c1_small", 4, 1): 10681.0,
+}
 
 
 def issue_roofline(key, pairs, kernel_ms, sm_mhz, extra=None):
