@@ -869,11 +869,18 @@ def serve_at(args, L, tm, machines, pools, rng, rate, requests=None):
                    "hbm_budget_mb": args.hbm_budget,
                    "queue_bound_samples": 64 * 4096},
         "p50_ms": float(np.percentile(lat, 50)),
+        "small_requests": {"max_samples": 256,
+                           "p50_ms": float(np.percentile([v for v, z in zip(lat, acc_sizes)
+                                                          if z <= 256] or [0], 50)),
+                           "p99_ms": float(np.percentile([v for v, z in zip(lat, acc_sizes)
+                                                          if z <= 256] or [0], 99))},
         "accepted": len(lat), "refused_queue_full": nreq - len(lat),
         "offered_samples_per_s": float(sizes.sum() / arrive[-1]),
         "samples_per_s": float(sum(acc_sizes)) / makespan,
         "serial": {"p50_ms": float(np.percentile(lat_s, 50)),
                    "p99_ms": float(np.percentile(lat_s, 99)),
+                   "small_p99_ms": float(np.percentile([v for v, z in zip(lat_s, sizes)
+                                                        if z <= 256] or [0], 99)),
                    "samples_per_s": total / (t_end_s - t0),
                    "form": "one tm_predict call per request, in arrival order"},
     }

@@ -349,9 +349,10 @@ typedef struct tm_stats {
 /* Train-kernel variant choice.  All variants end in the same automaton
  * state; they differ in speed.  mode 0: heuristic (resident CTAs per SM);
  * 1 (default, or TSETLIN_B200_AUTOTUNE at create): the first train call of
- * a launch shape times every feasible variant on a short trial (up to 1,024
- * samples of epoch 0 on up to eight units per SM, on the freshly reset
- * automata, which are reset again afterwards) and caches the fastest for
+ * a launch shape times every feasible variant on a short trial (up to 2,048
+ * samples of epoch 0 on up to 32 units per SM taken evenly from the launch's
+ * work list, on the freshly reset automata, which are reset again
+ * afterwards) and caches the fastest for
  * the process; 2: tune on every train call.  No counterpart in the
  * reference (it has one CPU code path). */
 int tm_set_autotune(tm_machine *m, int32_t mode);

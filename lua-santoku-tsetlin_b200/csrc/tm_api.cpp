@@ -737,11 +737,16 @@ static int autotune_plan(std::vector<TrainJob> &jobs, const std::vector<TrainDev
     }
   }
   if (cand.size() < 2) return TM_OK;  // nothing to choose: the heuristic plan
-  // trial: up to 2 x 4 waves of the heaviest units, up to 1024 samples each
+  // trial: up to 2,048 samples of epoch 0 on up to 32 units per SM, taken
+  // evenly from the cost-ordered work list -- enough units that every
+  // candidate's grid is full (the most resident units per SM of any
+  // variant is below 32), so that occupancy counts as in the real launch
   std::vector<TrainDev> ttd = td;
-  for (auto &t : ttd) t.n = std::min<uint32_t>(t.n, 1024);
-  const size_t nu = std::min<size_t>(work.size(), (size_t)sh.sms * 8);
-  std::vector<WorkItem> tw(work.begin(), work.begin() + nu);
+  for (auto &t : ttd) t.n = std::min<uint32_t>(t.n, 2048);
+  const size_t nu = std::min<size_t>(work.size(), (size_t)sh.sms * 32);
+  std::vector<WorkItem> tw;
+  tw.reserve(nu);
+  for (size_t i = 0; i < nu; i++) tw.push_back(work[i * work.size() / nu]);
   TrainShape tsh = sh;
   tsh.units = (uint32_t)nu;
   int best = -1;

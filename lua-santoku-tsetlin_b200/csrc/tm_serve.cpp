@@ -19,8 +19,11 @@
 // that arrive while slots are busy are admitted as slots free up, and the
 // slots' streams overlap on the device.  Predict is independent per
 // sample, so each request's result is the same alone or packed with
-// others.  The queue is bounded (max_queued_samples): a request beyond it
-// is refused with TM_ERR_BUSY rather than left to wait without limit.
+// others.  Small requests (at most TM_SERVE_SMALL samples) queue apart and
+// launch on high-priority streams, so a small request does not wait behind
+// the blocks of large requests already on the device.  The queues are
+// bounded together (max_queued_samples): a request beyond the bound is
+// refused with TM_ERR_BUSY rather than left to wait without limit.
 #include <stdio.h>
 #include <string.h>
 
@@ -43,6 +46,10 @@ using clk = std::chrono::steady_clock;
 namespace {
 
 constexpr uint32_t TM_SERVE_MAX_PACK = 64;     // requests per launch slot
+// Requests of at most this many samples are "small": they queue apart and
+// launch on high-priority streams, so that the device's block scheduler
+// starts their blocks ahead of those of large requests already queued
+constexpr uint64_t TM_SERVE_SMALL = 256;
 constexpr size_t TM_SERVE_LATENCY_KEEP = 1 << 16;  // polled requests whose latency is kept
 
 struct Request {
@@ -65,6 +72,7 @@ struct Slot {
   std::vector<Request *> reqs;
   std::vector<uint64_t> out_off;  // each request's result offset in h_out
   bool busy = false;
+  bool high = false;  // a high-priority stream, kept for small requests
 };
 
 uint64_t round_up(uint64_t v, uint64_t a) { return (v + a - 1) / a * a; }
@@ -78,7 +86,8 @@ struct tm_server {
   uint64_t cap_in = 0, cap_out = 0, cap_x = 0, cap_sums = 0, cap_jobs = 0;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
-  std::deque<Request *> queue;
+  std::deque<Request *> queue;    // large requests, arrival order
+  std::deque<Request *> squeue;   // small requests, arrival order
   uint64_t queued_samples = 0;
   std::unordered_map<uint64_t, Request *> live;  // submitted, not yet polled done
   std::unordered_map<uint64_t, double> latency;   // polled: submit -> done, microseconds
@@ -188,29 +197,44 @@ static cudaError_t launch_slot(tm_server *s, Slot &sl) {
   return e;
 }
 
+// The next launch: a free slot and the queue it serves.  High-priority
+// slots take small requests only; normal slots take large ones, and small
+// ones when no large request waits (or when every slot is normal).
+static bool pick(tm_server *s, Slot *&slot, std::deque<Request *> *&q) {
+  for (Slot &sl : s->slots) {
+    if (sl.busy) continue;
+    if (sl.high && !s->squeue.empty()) {
+      slot = &sl, q = &s->squeue;
+      return true;
+    }
+    if (!sl.high && !s->queue.empty()) {
+      slot = &sl, q = &s->queue;
+      return true;
+    }
+  }
+  for (Slot &sl : s->slots)
+    if (!sl.busy && !sl.high && !s->squeue.empty()) {
+      slot = &sl, q = &s->squeue;
+      return true;
+    }
+  return false;
+}
+
 static void worker_main(tm_server *s) {
   cudaSetDevice(s->cfg.device);
   std::unique_lock<std::mutex> lk(s->mu);
   while (true) {
     Slot *free_slot = nullptr;
-    s->cv_work.wait(lk, [&] {
-      if (s->stop) return true;
-      if (s->queue.empty()) return false;
-      for (Slot &sl : s->slots)
-        if (!sl.busy) {
-          free_slot = &sl;
-          return true;
-        }
-      return false;
-    });
+    std::deque<Request *> *q = nullptr;
+    s->cv_work.wait(lk, [&] { return s->stop || pick(s, free_slot, q); });
     if (s->stop) break;
     Slot &sl = *free_slot;
-    // the oldest queued requests, any machine, while they fit the slot
+    // the oldest requests of that queue, any machine, while they fit the slot
     uint64_t n = 0;
-    while (!s->queue.empty() && sl.reqs.size() < TM_SERVE_MAX_PACK) {
-      Request *r = s->queue.front();
+    while (!q->empty() && sl.reqs.size() < TM_SERVE_MAX_PACK) {
+      Request *r = q->front();
       if (!sl.reqs.empty() && n + r->n > s->cfg.max_batch_samples) break;
-      s->queue.pop_front();
+      q->pop_front();
       sl.reqs.push_back(r);
       n += r->n;
     }
@@ -243,7 +267,8 @@ static void free_server(tm_server *s) {
     if (sl.d_x) cudaFree(sl.d_x);
     if (sl.d_sums) cudaFree(sl.d_sums);
   }
-  for (Request *r : s->queue) s->live.erase(r->id), delete r;
+  for (auto *qq : {&s->queue, &s->squeue})
+    for (Request *r : *qq) s->live.erase(r->id), delete r;
   for (auto &kv : s->live) delete kv.second;
   delete s;
 }
@@ -290,9 +315,17 @@ extern "C" int tm_serve_open(const tm_server_config *cfg, tm_machine *const *mac
     return tmb_fail(TM_ERR_OOM, "serve_open: the HBM budget does not cover one launch slot");
   }
   s->slots.resize(nslots);
-  for (Slot &sl : s->slots) {
+  int prio_lo = 0, prio_hi = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+  // a third of the slots (at least one when there are two or more) on
+  // high-priority streams for small requests
+  const uint64_t nhigh = nslots >= 2 ? std::max<uint64_t>(1, nslots / 3) : 0;
+  for (size_t i = 0; i < s->slots.size(); i++) {
+    Slot &sl = s->slots[i];
     sl.srv = s;
-    bool ok = cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking) == cudaSuccess &&
+    sl.high = i < nhigh;
+    bool ok = cudaStreamCreateWithPriority(&sl.st, cudaStreamNonBlocking,
+                                           sl.high ? prio_hi : prio_lo) == cudaSuccess &&
               cudaHostAlloc(&sl.h_in, s->cap_in, cudaHostAllocDefault) == cudaSuccess &&
               cudaHostAlloc(&sl.h_out, s->cap_out, cudaHostAllocDefault) == cudaSuccess &&
               cudaHostAlloc(&sl.h_jobs, s->cap_jobs, cudaHostAllocDefault) == cudaSuccess &&
@@ -337,7 +370,7 @@ extern "C" int tm_serve_submit(tm_server *s, uint32_t machine, const uint8_t *pr
     }
     r->id = s->next_id++;
     s->live[r->id] = r;
-    s->queue.push_back(r);
+    (n <= TM_SERVE_SMALL ? s->squeue : s->queue).push_back(r);
     s->queued_samples += n;
     *id = r->id;
   }
@@ -391,7 +424,7 @@ extern "C" int tm_serve_stats(tm_server *s, uint64_t *out) {
   std::lock_guard<std::mutex> lk(s->mu);
   uint32_t busy = 0;
   for (const Slot &sl : s->slots) busy += sl.busy ? 1 : 0;
-  out[0] = s->queue.size();
+  out[0] = s->queue.size() + s->squeue.size();
   out[1] = s->queued_samples;
   out[2] = s->live.size();
   out[3] = busy;

@@ -473,7 +473,9 @@ __global__ void __launch_bounds__(NT, MINB)
   X(2, 256, 1, 0, 3, 2)     \
   X(3, 256, 2, 2, 2, 2)     \
   X(4, 128, 2, 1, 4, 2)     \
-  X(5, 64, 1, 0, 8, 2)
+  X(5, 64, 1, 0, 8, 2)      \
+  X(6, 32, 2, 0, 14, 2)     \
+  X(7, 32, 2, 1, 14, 2)
 
 struct WptConfig {
   int nt, wpt, rp, minb, ibs;

@@ -451,7 +451,7 @@ def test_every_train_variant_matches_oracle(tm, features):
     # the word-per-thread kernel's configurations that hold these rows
     # (4500 features: 282 words -> 512 threads x 2 words; 784: 52 words)
     wp = ((2 * features + 31) // 32 + 3) // 4 * 4
-    for cid, words in ((1, 1024), (2, 256), (3, 512), (4, 256), (5, 64)):
+    for cid, words in ((1, 1024), (2, 256), (3, 512), (4, 256), (5, 64), (6, 64), (7, 64)):
         if wp <= words:
             variants.append((4, cid))
     kind, tbl = ref_table(cfg, seed=31)
