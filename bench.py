@@ -244,6 +244,10 @@ INSTR_PER_PAIR = {
     ("search", 3, 1): 607.2,     # one warp per unit
     ("search", 0, 2): 1631.1,    # CTA per unit, planes in shared memory, 2 clauses per warp
     ("search", 1, 1): 2596.0,    # CTA per unit, count planes in global memory
+    # word-per-thread configurations 5-7: 89.35e9, 67.98e9, 69.18e9 / 105.91e6
+    ("search", 4, 5): 843.6,
+    ("search", 4, 6): 641.9,
+    ("search", 4, 7): 653.2,
     # large sparse classifier rows (16,384 features), c1_small (1.091e6 active
     # steps): 13.54e9 global planes; 11.66e9 word-per-thread (512 x 2 words)
     ("c1", 1, 1): 12410.0,
@@ -587,7 +591,9 @@ def run_search_bench(args):
         round_(1, stats=st)
         print(json.dumps({"profile_launch": "search", "mode": st[0]["train_mode"],
                           "cpw": st[0]["train_cpw"],
-                          "active_pairs": st[0]["train_active_pairs"]}), flush=True)
+                          "active_pairs": st[0]["train_active_pairs"],
+                          "train_kernel_ms": st[0]["search_train_ms"],
+                          "resident_units": st[0]["train_resident"]}), flush=True)
         return
     # ---- warm-up: W epochs (tuning, first-touch allocations) ---------------
     round_(max(1, args.warmup))
@@ -664,10 +670,30 @@ def run_search_bench(args):
         d["yt"].nbytes
     sm_mhz = (ck or {}).get("sm_mhz") or 1965.0
     key = ("search",) + (modes[-1] if len(modes) == 1 else (-1, -1))
+    # HBM view of one epoch's train launch: the automata read and written
+    # once, the rows once per wave of resident units
+    wp = {p["negated"]: ((2 * p["features"] + 31) // 32 + 3) // 4 * 4 for p in params}
+    state = sum(SEARCH["classes"] * p["clauses"] * 8 * wp[p["negated"]] * 4 for p in params)
+    resident = stats[0]["train_resident"] if stats else 1
+    units = sum(SEARCH["classes"] * p["clauses"] // 8 for p in params)
+    waves = -(-units // max(1, resident))
+    alg = 2 * state + waves * n_train * max(wp.values()) * 4
+    per_launch_ms = train_ms / max(1, K)
     roof = issue_roofline(key, pairs, train_ms, sm_mhz, extra={
-        "kernel": "k_train_warp" if key[1] == 3 else "k_train",
+        "kernel": "k_train_warp" if key[1] == 3 else ("k_train_wpt" if key[1] == 4 else "k_train"),
         "epoch_graph_ms": graph_ms, "train_share_of_graph": train_ms / graph_ms if graph_ms else None,
-        "resident_units": stats[0]["train_resident"] if stats else None, "traffic": None})
+        "resident_units": resident,
+        "hbm": {"algorithmic_bytes_per_launch": alg,
+                "achieved_gbs": alg / (per_launch_ms / 1e3) / 1e9 if per_launch_ms else None,
+                "peak_gbs": measured_peaks()[0]["hbm_gbs"]},
+        # DRAM bytes of the one-warp kernel's launch in an ncu capture of
+        # one epoch over 2,000 samples (0.95 GB read + 0.89 GB written):
+        # the automata once each way; the rows of both literal layouts stay
+        # in L2 between waves, so only their first read grows with samples
+        "traffic": (1.840e9 + (n_train - 2000) * sum(wp.values()) * 4)
+        if key[1] == 3 else None,
+        "traffic_source": "ncu capture at 2,000 samples, rows' first read scaled to the "
+                          "launch's samples"})
     peaks, peak_kind = measured_peaks()
     out = {
         "metric": METRIC + " (batched vs plain, equal accuracy)", "value": value, "unit": UNIT,
@@ -907,6 +933,8 @@ def main():
                     help="run only the train launch a profiler capture looks at")
     ap.add_argument("--epoch-times", type=int, default=0,
                     help="c1/c0/c2: train this many epochs and print each epoch's kernel time")
+    ap.add_argument("--predict-sizes", default="",
+                    help="c1/c0/c2: comma-separated batch sizes; print each predict's kernel time")
     ap.add_argument("--requests", type=int, default=2000, help="serve: requests")
     ap.add_argument("--rate", type=float, default=5000.0, help="serve: arrivals per second")
     ap.add_argument("--hbm-budget", type=int, default=2048, help="serve: staging MB")
@@ -918,6 +946,9 @@ def main():
         return
     if args.epoch_times:
         run_epoch_times(args, WORKLOADS[args.workload])
+        return
+    if args.predict_sizes:
+        run_predict_sizes(args, WORKLOADS[args.workload])
         return
     if args.workload == "search" or args.profile_launch == "search":
         if args.impl == "reference":
@@ -966,6 +997,38 @@ def run_epoch_times(args, w):
     print(json.dumps({"epoch_times": w["name"], "train_kernel_ms": per, "holdout_accuracy": acc,
                       "mode": st["train_mode"], "cpw": st["train_cpw"],
                       "mean_ms": float(np.mean(per))}), flush=True)
+    t.destroy()
+
+
+def run_predict_sizes(args, w):
+    """Device time of predict on a trained-state-sized machine with random
+    actions (1 % of the automata included) for each batch size of
+    `--predict-sizes`: the small-batch (warp per clause row) and tiled
+    kernels across their switch."""
+    import torch
+    import santoku_tsetlin as tm
+    d = make_data(w, 0)
+    t = tm.create(w["kind"], create_table(w, seed=0))
+    info = t.info()
+    rng = np.random.default_rng(5)
+    t.import_state(actions=np.packbits(rng.random(info["action_chunks"] * 8) < 0.01,
+                                       bitorder="little"))
+    t.stats_enable(True)
+    out = {}
+    for k in [int(v) for v in args.predict_sizes.split(",")]:
+        xs = torch.from_numpy(np.ascontiguousarray(d["x"][:k])).cuda()
+        for _ in range(3):
+            t.predict(xs, k)
+        torch.cuda.synchronize()
+        t.reset_stats()
+        for _ in range(20):
+            t.predict(xs, k)
+        st = t.stats()
+        out[k] = st["predict_kernel_ms"] / max(1, st["predict_launches"])
+    a_bytes = info["action_chunks"]
+    print(json.dumps({"predict_sizes": w["name"], "kernel_ms": out, "action_bytes": a_bytes,
+                      "hbm_floor_ms": a_bytes / (measured_peaks()[0]["hbm_gbs"] * 1e9) * 1e3}),
+          flush=True)
     t.destroy()
 
 
