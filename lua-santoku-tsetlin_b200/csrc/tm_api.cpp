@@ -147,7 +147,41 @@ struct tm_machine {
   // device-resident search round: checkpoint of the actions, and (owner of
   // the round) its tables and the staged holdout truth
   DevBuf ckpt, search, search_truth;
+  // pinned staging of small host requests (TM_PIN_STAGE bytes each way):
+  // inputs go host -> pin -> device, outputs device -> pin -> host, so that
+  // a one-sample predict makes no pageable (synchronously staged) copy.
+  // pin_ev marks the end of the last copy out of the input half.
+  uint8_t *pin = nullptr;
+  cudaEvent_t pin_ev = nullptr;
+  bool pin_pending = false;
 };
+
+constexpr uint64_t TM_PIN_STAGE = 256 << 10;
+
+// The input half of the machine's pinned staging buffer, ready to be
+// written, or null when the request is too large for it (or pinned memory
+// cannot be had: the caller then copies from the pageable source).
+static uint8_t *pin_stage(tm_machine *m, uint64_t bytes) {
+  if (bytes > TM_PIN_STAGE) return nullptr;
+  if (!m->pin) {
+    if (cudaHostAlloc((void **)&m->pin, 2 * TM_PIN_STAGE, cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      m->pin = nullptr;
+      return nullptr;
+    }
+    if (cudaEventCreateWithFlags(&m->pin_ev, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      cudaFreeHost(m->pin);
+      m->pin = nullptr;
+      return nullptr;
+    }
+  }
+  if (m->pin_pending) {
+    if (cudaEventSynchronize(m->pin_ev) != cudaSuccess) return nullptr;
+    m->pin_pending = false;
+  }
+  return m->pin;
+}
 
 // Kernels launched by a CUB 64-bit radix sort of pairs: upsweep histogram,
 // exclusive scan and one onesweep pass per 8-bit digit.
@@ -369,6 +403,8 @@ extern "C" void tm_destroy(tm_machine *m) {
     b->release();
   if (m->ev0) cudaEventDestroy(m->ev0);
   if (m->ev1) cudaEventDestroy(m->ev1);
+  if (m->pin_ev) cudaEventDestroy(m->pin_ev);
+  if (m->pin) cudaFreeHost(m->pin);
   if (m->st) cudaStreamDestroy(m->st);
   delete m;
 }
@@ -451,7 +487,14 @@ static int stage_rows(tm_machine *m, DevBuf &dst, const uint8_t *src, const int6
     const uint8_t *dsrc = s;
     if (!on_device) {
       CK(m->raw.ensure(std::max<uint64_t>(n * nch, 16)));
-      CK(cudaMemcpyAsync(m->raw.p, s, n * nch, cudaMemcpyHostToDevice, m->st));
+      if (uint8_t *pb = pin_stage(m, n * nch)) {
+        memcpy(pb, s, n * nch);
+        CK(cudaMemcpyAsync(m->raw.p, pb, n * nch, cudaMemcpyHostToDevice, m->st));
+        CK(cudaEventRecord(m->pin_ev, m->st));
+        m->pin_pending = true;
+      } else {
+        CK(cudaMemcpyAsync(m->raw.p, s, n * nch, cudaMemcpyHostToDevice, m->st));
+      }
       dsrc = m->raw.as<uint8_t>();
     }
     CK(launch_repack(dsrc, n, nch, nch, dst.as<uint32_t>() + cls[h].x_off, cls[h].Wp, m->st));
@@ -706,9 +749,10 @@ static bool lookup_tuned(const TrainShape &sh, const tm_machine *m0, TrainPlan &
   return plan_mode(v.first, sh, out, v.second);
 }
 
-// Times every feasible variant on the first `trial` samples of epoch 0 of
-// (at most) the first few waves of units, keeps the fastest, and resets the
-// automata of every job to their initial state.
+// Times every feasible variant on the first samples of epoch 0 of a
+// sample of the launch's units, keeps the one whose time extrapolated to
+// the launch's samples is lowest, and resets the automata of every job to
+// their initial state.
 static int autotune_plan(std::vector<TrainJob> &jobs, const std::vector<TrainDev> &td,
                          const std::vector<WorkItem> &work, const TrainShape &sh,
                          tm_machine *m0, TrainPlan &out, bool &tuned) {
@@ -740,9 +784,20 @@ static int autotune_plan(std::vector<TrainJob> &jobs, const std::vector<TrainDev
   // trial: up to 2,048 samples of epoch 0 on up to 32 units per SM, taken
   // evenly from the cost-ordered work list -- enough units that every
   // candidate's grid is full (the most resident units per SM of any
-  // variant is below 32), so that occupancy counts as in the real launch
-  std::vector<TrainDev> ttd = td;
-  for (auto &t : ttd) t.n = std::min<uint32_t>(t.n, 2048);
+  // variant is below 32), so that occupancy counts as in the real launch.
+  // Each candidate runs at two lengths (all samples of the trial, and a
+  // quarter of them): the difference is its cost per sample, the rest its
+  // fixed cost per unit (loading and storing the automata), and the choice
+  // goes by both extrapolated to the launch's samples -- a variant that
+  // stages more of the automata on chip pays more up front and less per
+  // sample.
+  uint32_t nmax = 0;
+  for (const auto &t : td) nmax = std::max(nmax, t.n);
+  const uint32_t n_long = std::min<uint32_t>(nmax, 2048), n_short = n_long / 4;
+  std::vector<TrainDev> tl = td, ts = td;
+  for (auto &t : tl) t.n = std::min<uint32_t>(t.n, n_long);
+  for (auto &t : ts) t.n = std::min<uint32_t>(t.n, n_short);
+  const bool extrapolate = nmax > n_long && n_short >= 64;
   const size_t nu = std::min<size_t>(work.size(), (size_t)sh.sms * 32);
   std::vector<WorkItem> tw;
   tw.reserve(nu);
@@ -750,21 +805,34 @@ static int autotune_plan(std::vector<TrainJob> &jobs, const std::vector<TrainDev
   TrainShape tsh = sh;
   tsh.units = (uint32_t)nu;
   int best = -1;
-  float best_ms = 0;
-  for (size_t i = 0; i < cand.size(); i++) {
-    TrainPlan p;
-    if (!plan_mode(cand[i].mode, tsh, p, cand[i].cpw)) continue;
-    float t = 0, tmin = 0;
+  double best_ms = 0;
+  auto timed = [&](const TrainPlan &p, const std::vector<TrainDev> &tt, float &tmin) -> int {
+    float t = 0;
     for (int rep = 0; rep < 2; rep++) {
       uint32_t herr = 0;
-      int rc = launch_plan(p, tsh, ttd, tw, 0, 1, m0, &t, &herr);
+      int rc = launch_plan(p, tsh, tt, tw, 0, 1, m0, &t, &herr);
       if (rc) return rc;
       if (herr) return fail(TM_ERR_DEVICE, "train: a sample copy did not complete (status %u)", herr);
       tmin = rep == 0 ? t : std::min(tmin, t);
     }
-    if (best < 0 || tmin < best_ms) {
+    return TM_OK;
+  };
+  for (size_t i = 0; i < cand.size(); i++) {
+    TrainPlan p;
+    if (!plan_mode(cand[i].mode, tsh, p, cand[i].cpw)) continue;
+    float tlong = 0, tshort = 0;
+    int rc = timed(p, tl, tlong);
+    if (rc) return rc;
+    double est = tlong;
+    if (extrapolate) {
+      rc = timed(p, ts, tshort);
+      if (rc) return rc;
+      const double per = std::max(0.0, (double)(tlong - tshort)) / (n_long - n_short);
+      est = tlong + per * (double)(nmax - n_long);
+    }
+    if (best < 0 || est < best_ms) {
       best = (int)i;
-      best_ms = tmin;
+      best_ms = est;
     }
   }
   // back to the initial state (capi.c:1136-1146)
@@ -1558,8 +1626,12 @@ static int predict_common(tm_machine *m, const uint8_t *problems, const int64_t 
   std::vector<ClassDev> cls;
   int rc = stage_rows(m, m->x, problems, dim_offsets, n, on_device, cls);
   if (rc) return rc;
-  rc = upload_cls(m, m->d_cls, cls);
-  if (rc) return rc;
+  // a dense machine's rows start at offset 0 for every class: its resident
+  // class table already describes them
+  if (m->individualized) {
+    rc = upload_cls(m, m->d_cls, cls);
+    if (rc) return rc;
+  }
   rc = ensure_lits(m);
   if (rc) return rc;
   const uint64_t sb = n * m->classes * 4;
@@ -1589,12 +1661,29 @@ static int predict_common(tm_machine *m, const uint8_t *problems, const int64_t 
   CK(launch_finalize(m->sums.as<int32_t>(), (uint32_t)n, m->classes, m->type, dcls, dcod, dsc,
                      m->st));
   note_launch(m, 1);
+  // small results come back through the output half of the pinned buffer
+  uint8_t *po = nullptr;
+  const uint64_t outb = (out_classes ? clsb : 0) + (out_codes ? codb : 0) + (out_scores ? scb : 0);
+  if (!on_device && outb <= TM_PIN_STAGE && pin_stage(m, 0)) po = m->pin + TM_PIN_STAGE;
   if (!on_device) {
-    if (out_classes) CK(cudaMemcpyAsync(out_classes, dcls, clsb, cudaMemcpyDeviceToHost, m->st));
-    if (out_codes) CK(cudaMemcpyAsync(out_codes, dcod, codb, cudaMemcpyDeviceToHost, m->st));
-    if (out_scores) CK(cudaMemcpyAsync(out_scores, dsc, scb, cudaMemcpyDeviceToHost, m->st));
+    uint8_t *q = po;
+    auto back = [&](void *dst, const void *src, uint64_t b) -> cudaError_t {
+      if (!po) return cudaMemcpyAsync(dst, src, b, cudaMemcpyDeviceToHost, m->st);
+      const cudaError_t e = cudaMemcpyAsync(q, src, b, cudaMemcpyDeviceToHost, m->st);
+      q += b;
+      return e;
+    };
+    if (out_classes) CK(back(out_classes, dcls, clsb));
+    if (out_codes) CK(back(out_codes, dcod, codb));
+    if (out_scores) CK(back(out_scores, dsc, scb));
   }
   CK(cudaStreamSynchronize(m->st));
+  if (po) {
+    const uint8_t *q = po;
+    if (out_classes) memcpy(out_classes, q, clsb), q += clsb;
+    if (out_codes) memcpy(out_codes, q, codb), q += codb;
+    if (out_scores) memcpy(out_scores, q, scb);
+  }
   if (m->timing) {
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, m->ev0, m->ev1));

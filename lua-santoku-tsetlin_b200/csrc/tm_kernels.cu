@@ -1242,20 +1242,27 @@ __global__ void __launch_bounds__(256, 2)
 // Small-batch predict (at most 16 samples per launch): one warp per clause
 // row.  The row streams once through the warp in 128-bit loads that do not
 // allocate in L1 (every action word is read once per launch: the HBM-bound
-// regime of a serving request), and each word is tested against all the
-// launch's samples, whose rows every CTA re-reads through L1.  Lane s keeps
-// sample s's vote sum over the warp's clauses (capi.c:110-118 votes, signed
-// by clause parity as in capi.c:148-161) and adds it to sums once.  The
-// same integer votes as k_predict, so the same sums bit for bit.
+// regime of a serving request), up to 8 loads per lane issued before any is
+// used so that a warp keeps up to 4 KB of the row in flight, and
+// each word is tested against all the launch's samples, whose rows every
+// CTA re-reads through L1.  Lane s keeps sample s's vote sum over the
+// warp's clauses (capi.c:110-118 votes, signed by clause parity as in
+// capi.c:148-161); the CTA's warps add theirs in shared memory and one
+// atomic per sample goes to sums.  The same integer votes as k_predict, so
+// the same sums bit for bit.
 // Grid: (clause blocks of TM_SMALL_CPB clauses, classes).
 // ---------------------------------------------------------------------------
-constexpr uint32_t TM_SMALL_CPB = 64;
+constexpr uint32_t TM_SMALL_CPB = 32;
+// 128-bit loads per lane in flight: fewer as more samples' rows are tested
+// against each word (their loads and counters take the registers)
+template <int NS>
+__host__ __device__ constexpr int small_lpl() { return NS <= 2 ? 8 : (NS <= 8 ? 4 : 2); }
 
 __device__ __forceinline__ uint4 ld_stream16(const void *p) {
   uint4 v;
-  asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0, %1, %2, %3}, [%4];"
-               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
-               : "l"(p));
+  asm("ld.global.nc.L1::no_allocate.v4.u32 {%0, %1, %2, %3}, [%4];"
+      : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+      : "l"(p));
   return v;
 }
 
@@ -1267,6 +1274,7 @@ __device__ __forceinline__ void predict_small_body(const uint32_t *__restrict__ 
                                                    const uint32_t *__restrict__ x, uint32_t s0,
                                                    uint32_t ns, uint32_t classes,
                                                    int32_t *__restrict__ sums) {
+  __shared__ int32_t red[8][NS];
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t cb = cblock * TM_SMALL_CPB;
   const uint32_t ce = cb + TM_SMALL_CPB < clauses ? cb + TM_SMALL_CPB : clauses;
@@ -1275,28 +1283,38 @@ __device__ __forceinline__ void predict_small_body(const uint32_t *__restrict__ 
   int32_t part = 0;  // lane s < ns: sample s0 + s
   for (uint32_t c = cb + warp; c < ce; c += 8) {
     const uint4 *ar = (const uint4 *)(act + C.act_off + (uint64_t)c * C.Wp);
+    const int32_t L = lits[(uint64_t)h * clauses + c];
     uint32_t f[NS];
 #pragma unroll
     for (int s = 0; s < NS; s++) f[s] = 0;
-#pragma unroll 2
-    for (uint32_t q = lane; q < Q; q += 32) {
-      uint4 a = ld_stream16(ar + q);
-      if (q == qlast) {  // evaluation mask on word W-1 (capi.c:104-106)
-        if (klast == 0) a.x &= C.emask;
-        if (klast == 1) a.y &= C.emask;
-        if (klast == 2) a.z &= C.emask;
-        if (klast == 3) a.w &= C.emask;
+    constexpr int LPL = small_lpl<NS>();
+    for (uint32_t q0 = 0; q0 < Q; q0 += 32 * LPL) {
+      uint4 a[LPL];
+#pragma unroll
+      for (int k = 0; k < LPL; k++) {
+        const uint32_t q = q0 + k * 32 + lane;
+        a[k] = q < Q ? ld_stream16(ar + q) : make_uint4(0u, 0u, 0u, 0u);
       }
 #pragma unroll
-      for (int s = 0; s < NS; s++) {
-        if ((uint32_t)s < ns) {
-          const uint4 v = __ldg(xr + (uint64_t)s * Q + q);
-          f[s] += __popc(a.x & ~v.x) + __popc(a.y & ~v.y) + __popc(a.z & ~v.z) +
-                  __popc(a.w & ~v.w);
+      for (int k = 0; k < LPL; k++) {
+        const uint32_t q = q0 + k * 32 + lane;
+        if (q == qlast) {  // evaluation mask on word W-1 (capi.c:104-106)
+          if (klast == 0) a[k].x &= C.emask;
+          if (klast == 1) a[k].y &= C.emask;
+          if (klast == 2) a[k].z &= C.emask;
+          if (klast == 3) a[k].w &= C.emask;
+        }
+        const uint32_t qs = q < Q ? q : 0;  // past the row: a[k] is zero, any x word will do
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+          if ((uint32_t)s < ns) {
+            const uint4 v = __ldg(xr + (uint64_t)s * Q + qs);
+            f[s] += __popc(a[k].x & ~v.x) + __popc(a[k].y & ~v.y) + __popc(a[k].z & ~v.z) +
+                    __popc(a[k].w & ~v.w);
+          }
         }
       }
     }
-    const int32_t L = lits[(uint64_t)h * clauses + c];
 #pragma unroll
     for (int s = 0; s < NS; s++) {
       if ((uint32_t)s < ns) {
@@ -1314,11 +1332,18 @@ __device__ __forceinline__ void predict_small_body(const uint32_t *__restrict__ 
       }
     }
   }
-  if (lane < ns && part != 0) atomicAdd(&sums[(uint64_t)(s0 + lane) * classes + h], part);
+  if (lane < (uint32_t)NS) red[warp][lane] = part;
+  __syncthreads();
+  if (warp == 0 && lane < ns) {
+    int32_t t = 0;
+#pragma unroll
+    for (int w = 0; w < 8; w++) t += red[w][lane];
+    if (t != 0) atomicAdd(&sums[(uint64_t)(s0 + lane) * classes + h], t);
+  }
 }
 
 template <int NS>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, NS <= 2 ? 4 : 2)
     k_predict_small(const uint32_t *__restrict__ act, const int32_t *__restrict__ lits,
                     const ClassDev *__restrict__ cls, uint32_t clauses, uint32_t tol,
                     const uint32_t *__restrict__ x, uint32_t s0, uint32_t ns, uint32_t classes,
