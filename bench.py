@@ -1040,6 +1040,7 @@ def run_predict_sizes(args, w):
         args_c = (t.handle, xh.ctypes.data_as(ctypes.c_void_p), None, k) + (
             (yh.ctypes.data_as(ctypes.c_void_p), None) if info["type"] == tm.CLASSIFIER
             else (None, yh.ctypes.data_as(ctypes.c_void_p))) + (0,)
+        t.stats_enable(False)  # no timing events on the measured calls
         for _ in range(20):
             lib.tm_predict(*args_c)
         reps = 200 if k <= 64 else 20
@@ -1048,6 +1049,7 @@ def run_predict_sizes(args, w):
             rc = lib.tm_predict(*args_c)
         call[k] = (time.perf_counter() - t0) / reps * 1e6
         assert rc == 0
+        t.stats_enable(True)
     a_bytes = info["action_chunks"]
     print(json.dumps({"predict_sizes": w["name"], "kernel_ms": out, "call_us": call,
                       "action_bytes": a_bytes,

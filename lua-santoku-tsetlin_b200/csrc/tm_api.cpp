@@ -477,7 +477,8 @@ static uint64_t x_layout(tm_machine *m, uint64_t n, std::vector<ClassDev> &cls) 
 }
 
 static int stage_rows(tm_machine *m, DevBuf &dst, const uint8_t *src, const int64_t *dim_offsets,
-                      uint64_t n, bool on_device, std::vector<ClassDev> &cls) {
+                      uint64_t n, bool on_device, std::vector<ClassDev> &cls,
+                      uint32_t *zero = nullptr, uint64_t zero_words = 0) {
   const uint64_t words = x_layout(m, n, cls);
   CK(dst.ensure(std::max<uint64_t>(words, 4) * 4));
   const uint32_t nblk = m->individualized ? m->classes : 1;
@@ -497,7 +498,8 @@ static int stage_rows(tm_machine *m, DevBuf &dst, const uint8_t *src, const int6
       }
       dsrc = m->raw.as<uint8_t>();
     }
-    CK(launch_repack(dsrc, n, nch, nch, dst.as<uint32_t>() + cls[h].x_off, cls[h].Wp, m->st));
+    CK(launch_repack(dsrc, n, nch, nch, dst.as<uint32_t>() + cls[h].x_off, cls[h].Wp, m->st,
+                     h == 0 ? zero : nullptr, h == 0 ? zero_words : 0));
     note_launch(m, 1);
     if (!on_device && m->individualized) CK(cudaStreamSynchronize(m->st));  // raw reuse
   }
@@ -1624,7 +1626,11 @@ static int predict_common(tm_machine *m, const uint8_t *problems, const int64_t 
   if (n == 0) return TM_OK;
   DevGuard g(m->device);
   std::vector<ClassDev> cls;
-  int rc = stage_rows(m, m->x, problems, dim_offsets, n, on_device, cls);
+  const uint64_t sb = n * m->classes * 4;
+  CK(m->sums.ensure(sb));
+  // the repack launch also clears the vote sums
+  int rc = stage_rows(m, m->x, problems, dim_offsets, n, on_device, cls, m->sums.as<uint32_t>(),
+                      sb / 4);
   if (rc) return rc;
   // a dense machine's rows start at offset 0 for every class: its resident
   // class table already describes them
@@ -1634,9 +1640,6 @@ static int predict_common(tm_machine *m, const uint8_t *problems, const int64_t 
   }
   rc = ensure_lits(m);
   if (rc) return rc;
-  const uint64_t sb = n * m->classes * 4;
-  CK(m->sums.ensure(sb));
-  CK(cudaMemsetAsync(m->sums.p, 0, sb, m->st));
   if (m->timing) CK(cudaEventRecord(m->ev0, m->st));
   CK(launch_predict(m->d_act, m->d_lits, m->d_cls, nullptr, m->classes, m->clauses, m->tol,
                     m->x.as<uint32_t>(), (uint32_t)n, m->sums.as<int32_t>(), m->st));

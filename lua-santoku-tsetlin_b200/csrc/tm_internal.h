@@ -91,8 +91,11 @@ constexpr uint32_t ST_IB = 0x01000000u;
 constexpr uint32_t ST_PERM = 0xFFFFFFFFu;
 
 // ---- launchers (tm_kernels.cu) -------------------------------------------
+// Reference byte rows -> padded words; `zero` (optional) is cleared in the
+// same launch (the vote sums of the predict that follows).
 cudaError_t launch_repack(const uint8_t *src, uint64_t n, uint64_t row_bytes, uint64_t src_stride,
-                          uint32_t *dst, uint32_t dst_words, cudaStream_t st);
+                          uint32_t *dst, uint32_t dst_words, cudaStream_t st,
+                          uint32_t *zero = nullptr, uint64_t zero_words = 0);
 cudaError_t launch_labels(const int64_t *src, int32_t *dst, uint64_t n, cudaStream_t st);
 cudaError_t launch_setup(uint32_t *act, uint32_t *cnt, const ClassDev *cls, uint32_t classes,
                          uint32_t clauses, uint32_t B, uint64_t act_words, cudaStream_t st);

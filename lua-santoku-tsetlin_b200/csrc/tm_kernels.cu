@@ -20,7 +20,12 @@ namespace tmb {
 // Layout kernels
 // ---------------------------------------------------------------------------
 __global__ void k_repack(const uint8_t *__restrict__ src, uint64_t n, uint64_t row_bytes,
-                         uint64_t src_stride, uint32_t *__restrict__ dst, uint32_t dst_words) {
+                         uint64_t src_stride, uint32_t *__restrict__ dst, uint32_t dst_words,
+                         uint32_t *__restrict__ zero, uint64_t zero_words) {
+  // the vote sums of the predict that reads these rows start at zero
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < zero_words;
+       t += (uint64_t)gridDim.x * blockDim.x)
+    zero[t] = 0;
   const uint64_t total = n * dst_words;
   for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
        t += (uint64_t)gridDim.x * blockDim.x) {
@@ -36,11 +41,13 @@ __global__ void k_repack(const uint8_t *__restrict__ src, uint64_t n, uint64_t r
 }
 
 cudaError_t launch_repack(const uint8_t *src, uint64_t n, uint64_t row_bytes, uint64_t src_stride,
-                          uint32_t *dst, uint32_t dst_words, cudaStream_t st) {
-  const uint64_t total = n * dst_words;
+                          uint32_t *dst, uint32_t dst_words, cudaStream_t st, uint32_t *zero,
+                          uint64_t zero_words) {
+  const uint64_t total = std::max<uint64_t>(n * dst_words, zero_words);
   if (!total) return cudaSuccess;
   const int blocks = (int)std::min<uint64_t>((total + 255) / 256, 148ull * 32);
-  k_repack<<<blocks, 256, 0, st>>>(src, n, row_bytes, src_stride, dst, dst_words);
+  k_repack<<<blocks, 256, 0, st>>>(src, n, row_bytes, src_stride, dst, dst_words, zero,
+                                   zero_words);
   return cudaGetLastError();
 }
 
@@ -1239,20 +1246,21 @@ __global__ void __launch_bounds__(256, 2)
 }
 
 // ---------------------------------------------------------------------------
-// Small-batch predict (at most 16 samples per launch): one warp per clause
-// row.  The row streams once through the warp in 128-bit loads that do not
-// allocate in L1 (every action word is read once per launch: the HBM-bound
-// regime of a serving request), up to 8 loads per lane issued before any is
-// used so that a warp keeps up to 4 KB of the row in flight, and
-// each word is tested against all the launch's samples, whose rows every
-// CTA re-reads through L1.  Lane s keeps sample s's vote sum over the
-// warp's clauses (capi.c:110-118 votes, signed by clause parity as in
-// capi.c:148-161); the CTA's warps add theirs in shared memory and one
-// atomic per sample goes to sums.  The same integer votes as k_predict, so
-// the same sums bit for bit.
-// Grid: (clause blocks of TM_SMALL_CPB clauses, classes).
+// Small-batch predict (at most 16 samples per launch).  A warp evaluates one
+// clause row at a time: the row streams once through the warp in 128-bit
+// loads that do not allocate in L1 (every action word is read once per
+// launch: the HBM-bound regime of a serving request), up to 8 loads per
+// lane issued before any is used so that a warp keeps up to 4 KB of the row
+// in flight, and each word is tested against all the launch's samples,
+// whose rows the CTAs re-read through L1.  From 4 samples on, the failed-
+// literal counts popc(a & ~x) go through carry-save adders on every other
+// 4-word step (one POPC per four words there, the logic ops on the other
+// pipe), since POPC throughput, not HBM, bounds those launches.  Lane s
+// keeps sample s's vote sum (capi.c:110-118 votes, signed by clause parity
+// as in capi.c:148-161) and adds it to sums at the end of each class.  The
+// same integer votes as k_predict, so the same sums bit for bit.
 // ---------------------------------------------------------------------------
-constexpr uint32_t TM_SMALL_CPB = 32;
+constexpr uint32_t TM_SMALL_CPB = 32;  // clauses per CTA of the multi-job kernel
 // 128-bit loads per lane in flight: fewer as more samples' rows are tested
 // against each word (their loads and counters take the registers)
 template <int NS>
@@ -1266,6 +1274,95 @@ __device__ __forceinline__ uint4 ld_stream16(const void *p) {
   return v;
 }
 
+// Lane-partial failed-literal counts of one clause row `ar` for the ns
+// samples whose padded rows start at xr (Q 4-word groups per row); the
+// caller reduces them over the warp.
+template <int NS>
+__device__ __forceinline__ void small_clause(const uint4 *__restrict__ ar,
+                                             const uint4 *__restrict__ xr, const ClassDev &C,
+                                             uint32_t ns, uint32_t lane, uint32_t (&f)[NS]) {
+  const uint32_t Q = C.Wp >> 2, qlast = (C.W - 1) >> 2, klast = (C.W - 1) & 3;
+  constexpr bool CSA = NS >= 4;
+  uint32_t ones[NS], twos[NS];
+#pragma unroll
+  for (int s = 0; s < NS; s++) f[s] = ones[s] = twos[s] = 0;
+  constexpr int LPL = small_lpl<NS>();
+  for (uint32_t q0 = 0; q0 < Q; q0 += 32 * LPL) {
+    uint4 a[LPL];
+#pragma unroll
+    for (int k = 0; k < LPL; k++) {
+      const uint32_t q = q0 + k * 32 + lane;
+      a[k] = q < Q ? ld_stream16(ar + q) : make_uint4(0u, 0u, 0u, 0u);
+    }
+#pragma unroll
+    for (int k = 0; k < LPL; k++) {
+      const uint32_t q = q0 + k * 32 + lane;
+      if (q == qlast) {  // evaluation mask on word W-1 (capi.c:104-106)
+        if (klast == 0) a[k].x &= C.emask;
+        if (klast == 1) a[k].y &= C.emask;
+        if (klast == 2) a[k].z &= C.emask;
+        if (klast == 3) a[k].w &= C.emask;
+      }
+      const uint32_t qs = q < Q ? q : 0;  // past the row: a[k] is zero, any x word will do
+#pragma unroll
+      for (int s = 0; s < NS; s++) {
+        if ((uint32_t)s < ns) {
+          const uint4 v = __ldg(xr + (uint64_t)s * Q + qs);
+          const uint32_t t0 = a[k].x & ~v.x, t1 = a[k].y & ~v.y;
+          const uint32_t t2 = a[k].z & ~v.z, t3 = a[k].w & ~v.w;
+          if (CSA && (k & 1) == 0) {
+            // (ones, twos) hold bit-sliced partial counts of weight 1 and 2;
+            // only the weight-4 carries are popcounted
+            uint32_t o = ones[s];
+            const uint32_t h1 = (o & t0) | (o & t1) | (t0 & t1);
+            o ^= t0 ^ t1;
+            const uint32_t h2 = (o & t2) | (o & t3) | (t2 & t3);
+            o ^= t2 ^ t3;
+            const uint32_t tw = twos[s];
+            const uint32_t f4 = (tw & h1) | (tw & h2) | (h1 & h2);
+            twos[s] = tw ^ h1 ^ h2;
+            ones[s] = o;
+            f[s] += 4 * __popc(f4);
+          } else {
+            f[s] += __popc(t0) + __popc(t1) + __popc(t2) + __popc(t3);
+          }
+        }
+      }
+    }
+  }
+  if (CSA) {
+#pragma unroll
+    for (int s = 0; s < NS; s++) f[s] += 2 * __popc(twos[s]) + __popc(ones[s]);
+  }
+}
+
+// Warp-reduces the counts of clause c (literal count L) and adds each
+// sample's signed vote to lane s's `part`.
+template <int NS>
+__device__ __forceinline__ void small_vote(const uint32_t (&f)[NS], int32_t L, uint32_t c,
+                                           uint32_t tol, uint32_t ns, uint32_t lane,
+                                           int32_t &part) {
+#pragma unroll
+  for (int s = 0; s < NS; s++) {
+    if ((uint32_t)s < ns) {
+      const int32_t F = (int32_t)__reduce_add_sync(0xFFFFFFFFu, f[s]);
+      if (lane == (uint32_t)s) {
+        int32_t vote;
+        if (L == 0)
+          vote = (int32_t)tol;
+        else {
+          vote = (L < (int32_t)tol ? L : (int32_t)tol) - F;
+          vote = vote < 0 ? 0 : vote;
+        }
+        part += (c & 1) ? -vote : vote;
+      }
+    }
+  }
+}
+
+// Multi-job form: the CTA's 8 warps take the clauses of one block of
+// TM_SMALL_CPB clauses of class h in turn, add their votes in shared memory
+// and send one atomic per sample to sums.
 template <int NS>
 __device__ __forceinline__ void predict_small_body(const uint32_t *__restrict__ act,
                                                    const int32_t *__restrict__ lits,
@@ -1278,59 +1375,14 @@ __device__ __forceinline__ void predict_small_body(const uint32_t *__restrict__ 
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t cb = cblock * TM_SMALL_CPB;
   const uint32_t ce = cb + TM_SMALL_CPB < clauses ? cb + TM_SMALL_CPB : clauses;
-  const uint32_t Q = C.Wp >> 2, qlast = (C.W - 1) >> 2, klast = (C.W - 1) & 3;
   const uint4 *xr = (const uint4 *)(x + C.x_off + (uint64_t)s0 * C.Wp);
   int32_t part = 0;  // lane s < ns: sample s0 + s
   for (uint32_t c = cb + warp; c < ce; c += 8) {
     const uint4 *ar = (const uint4 *)(act + C.act_off + (uint64_t)c * C.Wp);
     const int32_t L = lits[(uint64_t)h * clauses + c];
     uint32_t f[NS];
-#pragma unroll
-    for (int s = 0; s < NS; s++) f[s] = 0;
-    constexpr int LPL = small_lpl<NS>();
-    for (uint32_t q0 = 0; q0 < Q; q0 += 32 * LPL) {
-      uint4 a[LPL];
-#pragma unroll
-      for (int k = 0; k < LPL; k++) {
-        const uint32_t q = q0 + k * 32 + lane;
-        a[k] = q < Q ? ld_stream16(ar + q) : make_uint4(0u, 0u, 0u, 0u);
-      }
-#pragma unroll
-      for (int k = 0; k < LPL; k++) {
-        const uint32_t q = q0 + k * 32 + lane;
-        if (q == qlast) {  // evaluation mask on word W-1 (capi.c:104-106)
-          if (klast == 0) a[k].x &= C.emask;
-          if (klast == 1) a[k].y &= C.emask;
-          if (klast == 2) a[k].z &= C.emask;
-          if (klast == 3) a[k].w &= C.emask;
-        }
-        const uint32_t qs = q < Q ? q : 0;  // past the row: a[k] is zero, any x word will do
-#pragma unroll
-        for (int s = 0; s < NS; s++) {
-          if ((uint32_t)s < ns) {
-            const uint4 v = __ldg(xr + (uint64_t)s * Q + qs);
-            f[s] += __popc(a[k].x & ~v.x) + __popc(a[k].y & ~v.y) + __popc(a[k].z & ~v.z) +
-                    __popc(a[k].w & ~v.w);
-          }
-        }
-      }
-    }
-#pragma unroll
-    for (int s = 0; s < NS; s++) {
-      if ((uint32_t)s < ns) {
-        const int32_t F = (int32_t)__reduce_add_sync(0xFFFFFFFFu, f[s]);
-        if (lane == (uint32_t)s) {
-          int32_t vote;
-          if (L == 0)
-            vote = (int32_t)tol;
-          else {
-            vote = (L < (int32_t)tol ? L : (int32_t)tol) - F;
-            vote = vote < 0 ? 0 : vote;
-          }
-          part += (c & 1) ? -vote : vote;
-        }
-      }
-    }
+    small_clause<NS>(ar, xr, C, ns, lane, f);
+    small_vote<NS>(f, L, c, tol, ns, lane, part);
   }
   if (lane < (uint32_t)NS) red[warp][lane] = part;
   __syncthreads();
@@ -1342,15 +1394,40 @@ __device__ __forceinline__ void predict_small_body(const uint32_t *__restrict__ 
   }
 }
 
+// One machine: warp w evaluates the contiguous clause range
+// [w * per_warp, (w + 1) * per_warp) of the flattened (class, clause)
+// order, so that the grid is one balanced wave of resident warps; a warp
+// sends its votes to sums when its range leaves a class and at its end.
 template <int NS>
-__global__ void __launch_bounds__(256, NS <= 2 ? 4 : 2)
+__global__ void __launch_bounds__(256, NS <= 2 ? 3 : 2)
     k_predict_small(const uint32_t *__restrict__ act, const int32_t *__restrict__ lits,
-                    const ClassDev *__restrict__ cls, uint32_t clauses, uint32_t tol,
-                    const uint32_t *__restrict__ x, uint32_t s0, uint32_t ns, uint32_t classes,
-                    int32_t *__restrict__ sums) {
-  const ClassDev C = cls[blockIdx.y];
-  predict_small_body<NS>(act, lits, C, blockIdx.y, blockIdx.x, clauses, tol, x, s0, ns, classes,
-                         sums);
+                    const ClassDev *__restrict__ cls, uint32_t classes, uint32_t clauses,
+                    uint32_t tol, const uint32_t *__restrict__ x, uint32_t s0, uint32_t ns,
+                    uint32_t per_warp, int32_t *__restrict__ sums) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t total = (uint64_t)classes * clauses;
+  uint64_t q = (((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * per_warp;
+  if (q >= total) return;  // the whole warp
+  const uint64_t qe = q + per_warp < total ? q + per_warp : total;
+  uint32_t h = (uint32_t)(q / clauses), c = (uint32_t)(q - (uint64_t)h * clauses);
+  ClassDev C = cls[h];
+  const uint4 *xr = (const uint4 *)(x + C.x_off + (uint64_t)s0 * C.Wp);
+  int32_t part = 0;  // lane s < ns: sample s0 + s
+  for (; q < qe; q++, c++) {
+    if (c == clauses) {
+      if (lane < ns && part != 0) atomicAdd(&sums[(uint64_t)(s0 + lane) * classes + h], part);
+      part = 0;
+      h++;
+      c = 0;
+      C = cls[h];
+      xr = (const uint4 *)(x + C.x_off + (uint64_t)s0 * C.Wp);
+    }
+    const uint4 *ar = (const uint4 *)(act + C.act_off + (uint64_t)c * C.Wp);
+    uint32_t f[NS];
+    small_clause<NS>(ar, xr, C, ns, lane, f);
+    small_vote<NS>(f, lits[(uint64_t)h * clauses + c], c, tol, ns, lane, part);
+  }
+  if (lane < ns && part != 0) atomicAdd(&sums[(uint64_t)(s0 + lane) * classes + h], part);
 }
 
 // Many small predict jobs (at most 16 samples each, any machines) in one
@@ -1372,11 +1449,34 @@ __global__ void __launch_bounds__(256, 2)
                          J.classes, J.sums);
 }
 
+// Launch shape of k_predict_small<NS>: one wave of resident warps, each
+// with an equal share of the machine's clauses.
 template <int NS>
-static void small_launch(dim3 grid, cudaStream_t st, const uint32_t *act, const int32_t *lits,
-                         const ClassDev *cls, uint32_t clauses, uint32_t tol, const uint32_t *x,
-                         uint32_t s0, uint32_t ns, uint32_t classes, int32_t *sums) {
-  k_predict_small<NS><<<grid, 256, 0, st>>>(act, lits, cls, clauses, tol, x, s0, ns, classes, sums);
+static cudaError_t small_launch(cudaStream_t st, const uint32_t *act, const int32_t *lits,
+                                const ClassDev *cls, uint32_t classes, uint32_t clauses,
+                                uint32_t tol, const uint32_t *x, uint32_t s0, uint32_t ns,
+                                int32_t *sums) {
+  static int per_sm[64];  // resident CTAs per SM, per device (0: not yet asked)
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  int sms = 0;
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  int &occ = per_sm[dev & 63];
+  if (occ <= 0) {
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_predict_small<NS>, 256, 0);
+    if (e != cudaSuccess) return e;
+    if (occ <= 0) occ = 1;
+  }
+  const uint64_t total = (uint64_t)classes * clauses;
+  const uint64_t resident = (uint64_t)sms * occ * 8;
+  const uint64_t warps = total < resident ? total : resident;
+  const uint32_t per_warp = (uint32_t)((total + warps - 1) / warps);
+  const uint64_t used = (total + per_warp - 1) / per_warp;
+  k_predict_small<NS><<<(unsigned)((used + 7) / 8), 256, 0, st>>>(act, lits, cls, classes, clauses,
+                                                                  tol, x, s0, ns, per_warp, sums);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_predict(const uint32_t *act, const int32_t *lits, const ClassDev *cls,
@@ -1386,15 +1486,14 @@ cudaError_t launch_predict(const uint32_t *act, const int32_t *lits, const Class
   (void)cls_host;
   if (!n) return cudaSuccess;
   if (n <= TM_SMALL_N_MAX) {
-    const dim3 grid((clauses + TM_SMALL_CPB - 1) / TM_SMALL_CPB, classes);
     for (uint32_t s0 = 0; s0 < n; s0 += 16) {
       const uint32_t ns = n - s0 < 16 ? n - s0 : 16;
-      if (ns <= 1) small_launch<1>(grid, st, act, lits, cls, clauses, tol, x, s0, ns, classes, sums);
-      else if (ns <= 2) small_launch<2>(grid, st, act, lits, cls, clauses, tol, x, s0, ns, classes, sums);
-      else if (ns <= 4) small_launch<4>(grid, st, act, lits, cls, clauses, tol, x, s0, ns, classes, sums);
-      else if (ns <= 8) small_launch<8>(grid, st, act, lits, cls, clauses, tol, x, s0, ns, classes, sums);
-      else small_launch<16>(grid, st, act, lits, cls, clauses, tol, x, s0, ns, classes, sums);
-      cudaError_t e = cudaGetLastError();
+      cudaError_t e;
+      if (ns <= 1) e = small_launch<1>(st, act, lits, cls, classes, clauses, tol, x, s0, ns, sums);
+      else if (ns <= 2) e = small_launch<2>(st, act, lits, cls, classes, clauses, tol, x, s0, ns, sums);
+      else if (ns <= 4) e = small_launch<4>(st, act, lits, cls, classes, clauses, tol, x, s0, ns, sums);
+      else if (ns <= 8) e = small_launch<8>(st, act, lits, cls, classes, clauses, tol, x, s0, ns, sums);
+      else e = small_launch<16>(st, act, lits, cls, classes, clauses, tol, x, s0, ns, sums);
       if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
