@@ -234,20 +234,16 @@ def balanced_chunks(classes, threads, at_most):
 # warp).  The int_issue roofline below is that count x the live active steps
 # / the train kernel's live time, against 4 warp-instructions per clock per
 # SM.  Capture commands:
-#   TSETLIN_B200_VARIANT=<mode>:<cpw> ncu --clock-control none -k regex:k_train -c 1 \
-#       --metrics smsp__inst_executed.sum python bench.py --profile-launch search
+#   TSETLIN_B200_AUTOTUNE=0 TSETLIN_B200_VARIANT=<mode>:<cpw> ncu --clock-control none \
+#       -k regex:k_train -c 1 --metrics smsp__inst_executed.sum \
+#       python bench.py --profile-launch search --search-train 6000
 #   ncu --clock-control none -k regex:k_train -c 1 --metrics smsp__inst_executed.sum \
 #       python bench.py --profile-launch c1_small
 INSTR_PER_PAIR = {
-    # batched search rows (784 / 392 features), 64 machines, 6,000 samples:
-    # 64.31e9 / 105.91e6, 172.75e9 / 105.91e6, 274.95e9 / 105.91e6
-    ("search", 3, 1): 607.2,     # one warp per unit
-    ("search", 0, 2): 1631.1,    # CTA per unit, planes in shared memory, 2 clauses per warp
-    ("search", 1, 1): 2596.0,    # CTA per unit, count planes in global memory
-    # word-per-thread configurations 5-7: 89.35e9, 67.98e9, 69.18e9 / 105.91e6
-    ("search", 4, 5): 843.6,
-    ("search", 4, 6): 641.9,
-    ("search", 4, 7): 653.2,
+    # batched search rows (784 / 392 features, 40 % flipped bits), 64
+    # machines, one epoch over 6,000 samples: 87.03e9 and 90.86e9 / 105.91e6
+    ("search", 3, 1): 821.7,     # one warp per unit
+    ("search", 4, 7): 857.9,     # one warp per unit, 2 words per lane in registers
     # large sparse classifier rows (16,384 features), c1_small (1.091e6 active
     # steps): 13.54e9 global planes; 11.66e9 word-per-thread (512 x 2 words)
     ("c1", 1, 1): 12410.0,
@@ -692,12 +688,12 @@ def run_search_bench(args):
                 "achieved_gbs": alg / (per_launch_ms / 1e3) / 1e9 if per_launch_ms else None,
                 "peak_gbs": measured_peaks()[0]["hbm_gbs"]},
         # DRAM bytes of the one-warp kernel's launch in an ncu capture of
-        # one epoch over 2,000 samples (0.95 GB read + 0.89 GB written):
+        # one epoch over 6,000 samples (0.967 GB read + 0.890 GB written):
         # the automata once each way; the rows of both literal layouts stay
         # in L2 between waves, so only their first read grows with samples
-        "traffic": (1.840e9 + (n_train - 2000) * sum(wp.values()) * 4)
+        "traffic": (1.857e9 + (n_train - 6000) * sum(wp.values()) * 4)
         if key[1] == 3 else None,
-        "traffic_source": "ncu capture at 2,000 samples, rows' first read scaled to the "
+        "traffic_source": "ncu capture at 6,000 samples, rows' first read scaled to the "
                           "launch's samples"})
     peaks, peak_kind = measured_peaks()
     out = {

@@ -352,9 +352,7 @@ typedef struct tm_stats {
  * a launch shape times every feasible variant on a short trial (up to 2,048
  * samples of epoch 0 on up to 32 units per SM taken evenly from the launch's
  * work list, on the freshly reset automata, which are reset again
- * afterwards; when the launch has more samples, also on a quarter of them,
- * and each variant's time is extrapolated to the launch's samples from the
- * two) and caches the fastest for
+ * afterwards) and caches the fastest for
  * the process; 2: tune on every train call.  No counterpart in the
  * reference (it has one CPU code path). */
 int tm_set_autotune(tm_machine *m, int32_t mode);
