@@ -336,9 +336,12 @@ typedef struct tm_stats {
   uint64_t train_unit_steps;  /* (unit, sample) steps examined by train kernels */
   int32_t train_mode;         /* last train kernel variant: 0 automata in shared memory,
                                  1 count planes in global memory, 2 split over a 2-CTA
-                                 cluster, 3 one warp per unit (rows of at most 64 words) */
+                                 cluster, 3 one warp per unit (rows of at most 64 words),
+                                 4 words owned by threads (automata in registers and
+                                 shared memory) */
   int32_t train_autotuned;    /* 1 if the autotuner chose that variant */
-  int32_t train_cpw;          /* clauses per warp of that variant */
+  int32_t train_cpw;          /* modes 0-2: clauses per warp; mode 3: 1 = four units per
+                                 CTA, 2 = one; mode 4: the configuration (1-7) */
   int32_t pad_;
   uint64_t train_active_pairs; /* (unit, sample) steps trained after negative sampling */
   double search_epoch_ms;     /* device-resident search rounds: summed epoch graph time */
@@ -359,7 +362,8 @@ int tm_set_autotune(tm_machine *m, int32_t mode);
 
 /* Pins the train-kernel variant (train_mode values of tm_stats; cpw, the
  * clauses evaluated per warp in a single-CTA variant with 8 state bits: 1,
- * 2 or 4 -- 256 / cpw threads per unit); mode -1 returns to the automatic
+ * 2 or 4 -- 256 / cpw threads per unit; for mode 3, 1 or 2: four units or
+ * one per CTA; for mode 4, the configuration); mode -1 returns to the automatic
  * choice.  A train call that the pinned variant cannot run fails with
  * TM_ERR_ARG.  The environment variable TSETLIN_B200_VARIANT=mode:cpw, read
  * when a machine is created, pins the same way.  For tests and

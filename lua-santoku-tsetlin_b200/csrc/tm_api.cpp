@@ -613,6 +613,9 @@ struct TrainPlan {
 
 // Fills `p` for `mode` (and `cpw` clauses per warp) when that variant can
 // run this launch.
+// Units per CTA of the one-warp-per-unit kernel for its variant number.
+static int warp_units_per_cta(int cpw) { return cpw == 2 ? 1 : 4; }
+
 static bool plan_mode(int mode, const TrainShape &sh, TrainPlan &p, int cpw = 1) {
   p = TrainPlan{};
   p.mode = mode;
@@ -626,16 +629,17 @@ static bool plan_mode(int mode, const TrainShape &sh, TrainPlan &p, int cpw = 1)
     p.grid = (int)std::min<uint64_t>(sh.units, (uint64_t)sh.sms * occ);
     return true;
   }
-  if (cpw != 1 && (mode == TM_MODE_WARP || mode == TM_MODE_PAIR || sh.Bmin != 8 || sh.Bmax != 8))
-    return false;
   if (mode == TM_MODE_WARP) {
-    if (sh.Wpmax > 64 || sh.Bmax > 8) return false;
+    // cpw selects the units per CTA: 1 -> four, 2 -> one
+    if (sh.Wpmax > 64 || sh.Bmax > 8 || (cpw != 1 && cpw != 2)) return false;
+    const int wpc = warp_units_per_cta(cpw);
     size_t wsm = 0;
-    const int occ = train_warp_occupancy(sh.Wpmax, sh.Bmin, sh.Bmax, sh.smax, &wsm);
+    const int occ = train_warp_occupancy(sh.Wpmax, sh.Bmin, sh.Bmax, sh.smax, wpc, &wsm);
     if (occ <= 0 || (int)wsm > sh.optin) return false;
-    p.grid = (int)std::min<uint64_t>((sh.units + 3) / 4, (uint64_t)sh.sms * occ);
+    p.grid = (int)std::min<uint64_t>((sh.units + wpc - 1) / wpc, (uint64_t)sh.sms * occ);
     return true;
   }
+  if (cpw != 1 && (mode == TM_MODE_PAIR || sh.Bmin != 8 || sh.Bmax != 8)) return false;
   if (mode == TM_MODE_PAIR && sh.Bmax > 8) return false;
   p.lay = plan_smem(sh.Wpmax, sh.Bmax, sh.smax, mode, cpw);
   if ((int)p.lay.total > sh.optin) return false;
@@ -673,10 +677,10 @@ static int heuristic_plan(const TrainShape &sh, const tm_machine *m0, TrainPlan 
               sh.Bmax);
 }
 
-// Units a launch of `p` holds at once: a warp per unit (4 per CTA), a CTA
+// Units a launch of `p` holds at once: a warp per unit (4 or 1 per CTA), a CTA
 // per unit, or a 2-CTA cluster per unit.
 static uint64_t resident_units(const TrainPlan &p) {
-  if (p.mode == TM_MODE_WARP) return (uint64_t)p.grid * 4;
+  if (p.mode == TM_MODE_WARP) return (uint64_t)p.grid * warp_units_per_cta(p.cpw);
   if (p.mode == TM_MODE_WPT) return (uint64_t)p.grid;
   if (p.mode == TM_MODE_PAIR) return (uint64_t)p.grid / 2;
   return (uint64_t)p.grid;
@@ -706,7 +710,8 @@ static int launch_plan(const TrainPlan &p, const TrainShape &sh, const std::vect
   if (p.mode == TM_MODE_WARP)
     CK(launch_train_warp((const TrainDev *)base, (const WorkItem *)(base + off_w),
                          (uint32_t)work.size(), counter, e0, e1, sh.Wpmax, sh.Bmin, sh.Bmax,
-                         sh.smax, p.grid, st, (unsigned long long *)(err + 2)));
+                         sh.smax, warp_units_per_cta(p.cpw), p.grid, st,
+                         (unsigned long long *)(err + 2)));
   else if (p.mode == TM_MODE_WPT)
     CK(launch_train_wpt(p.cpw, (const TrainDev *)base, (const WorkItem *)(base + off_w),
                         (uint32_t)work.size(), counter, e0, e1, sh.Wpmax, sh.smax, m0->row_wait,
@@ -1441,7 +1446,8 @@ static int search_round(tm_machine *const *ms, const tm_train_args *args, uint32
       if (plan.mode == TM_MODE_WARP)
         ce = launch_train_warp((const TrainDev *)tbase, (const WorkItem *)(tbase + off_w),
                                (uint32_t)work.size(), counter, 0, 1, sh.Wpmax, sh.Bmin, sh.Bmax,
-                               sh.smax, plan.grid, st, (unsigned long long *)(d_err + 2));
+                               sh.smax, warp_units_per_cta(plan.cpw), plan.grid, st,
+                               (unsigned long long *)(d_err + 2));
       else if (plan.mode == TM_MODE_WPT)
         ce = launch_train_wpt(plan.cpw, (const TrainDev *)tbase, (const WorkItem *)(tbase + off_w),
                               (uint32_t)work.size(), counter, 0, 1, sh.Wpmax, sh.smax,

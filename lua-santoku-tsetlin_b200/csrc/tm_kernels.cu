@@ -658,12 +658,12 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
 // position's skip decision and chance draws into registers; surviving
 // positions are visited in order through the ballot mask, their draws
 // broadcast by shuffles.  The next surviving sample's row is loaded while
-// the current one is processed.  Same rules and draws as k_train.
+// the current one is processed.  Same rules and draws as k_train.  WPC
+// warps (units) share a CTA: 4, or 1 so that the SM's shared memory is
+// divided among units without rounding to CTAs of four.
 // ---------------------------------------------------------------------------
-constexpr int TM_WARP_THREADS = 128;
-
-template <int BM, bool EXACT = false>
-__global__ void __launch_bounds__(TM_WARP_THREADS)
+template <int BM, bool EXACT, int WPC>
+__global__ void __launch_bounds__(WPC * 32)
     k_train_warp(const TrainDev *__restrict__ machines, const WorkItem *__restrict__ work,
                  uint32_t nwork, uint32_t *__restrict__ counter, uint32_t e_begin, uint32_t e_end,
                  uint32_t slice_words, uint32_t ib_words, uint32_t ovf_cap, uint32_t stride,
@@ -902,36 +902,58 @@ static uint32_t warp_slice_words(uint32_t Wpmax, uint32_t Bmax, uint32_t ib_word
   return (8 * Bmax * Wpmax + 2 * ib_words + ovf_cap + 32 + 31) / 32 * 32;
 }
 
-int train_warp_occupancy(uint32_t Wpmax, uint32_t Bmin, uint32_t Bmax, uint32_t smax,
-                         size_t *smem_bytes) {
-  const uint32_t ovf_cap = smax / 4 > 0 ? smax / 4 : 1;
-  const size_t bytes = (size_t)(TM_WARP_THREADS / 32) * warp_slice_words(Wpmax, Bmax, Wpmax, ovf_cap) * 4;
-  *smem_bytes = bytes;
-  const bool exact = Bmin == 8 && Bmax == 8;
-  cudaFuncSetAttribute(k_train_warp<7, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  cudaFuncSetAttribute(k_train_warp<7, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+template <int WPC>
+static int warp_occ(bool exact, size_t bytes) {
+  cudaFuncSetAttribute(k_train_warp<7, false, WPC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)bytes);
+  cudaFuncSetAttribute(k_train_warp<7, true, WPC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)bytes);
   int nb = 0;
   if (exact)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_train_warp<7, true>, TM_WARP_THREADS, bytes);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_train_warp<7, true, WPC>, WPC * 32, bytes);
   else
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_train_warp<7, false>, TM_WARP_THREADS, bytes);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_train_warp<7, false, WPC>, WPC * 32, bytes);
   return nb;
+}
+
+int train_warp_occupancy(uint32_t Wpmax, uint32_t Bmin, uint32_t Bmax, uint32_t smax, int wpc,
+                         size_t *smem_bytes) {
+  const uint32_t ovf_cap = smax / 4 > 0 ? smax / 4 : 1;
+  const size_t bytes = (size_t)wpc * warp_slice_words(Wpmax, Bmax, Wpmax, ovf_cap) * 4;
+  *smem_bytes = bytes;
+  const bool exact = Bmin == 8 && Bmax == 8;
+  return wpc == 1 ? warp_occ<1>(exact, bytes) : warp_occ<4>(exact, bytes);
+}
+
+template <int WPC>
+static void warp_launch(bool exact, int grid, size_t bytes, cudaStream_t st,
+                        const TrainDev *machines, const WorkItem *work, uint32_t nwork,
+                        uint32_t *counter, uint32_t e_begin, uint32_t e_end, uint32_t slice,
+                        uint32_t Wpmax, uint32_t ovf_cap, uint32_t stride,
+                        unsigned long long *pairs) {
+  if (exact)
+    k_train_warp<7, true, WPC><<<grid, WPC * 32, bytes, st>>>(
+        machines, work, nwork, counter, e_begin, e_end, slice, Wpmax, ovf_cap, stride, pairs);
+  else
+    k_train_warp<7, false, WPC><<<grid, WPC * 32, bytes, st>>>(
+        machines, work, nwork, counter, e_begin, e_end, slice, Wpmax, ovf_cap, stride, pairs);
 }
 
 cudaError_t launch_train_warp(const TrainDev *machines, const WorkItem *work, uint32_t nwork,
                               uint32_t *counter, uint32_t e_begin, uint32_t e_end, uint32_t Wpmax,
-                              uint32_t Bmin, uint32_t Bmax, uint32_t smax, int grid,
+                              uint32_t Bmin, uint32_t Bmax, uint32_t smax, int wpc, int grid,
                               cudaStream_t st, unsigned long long *pairs) {
   const uint32_t ovf_cap = smax / 4 > 0 ? smax / 4 : 1;
   const uint32_t slice = 8 * Bmax * Wpmax;
   const uint32_t stride = warp_slice_words(Wpmax, Bmax, Wpmax, ovf_cap);
-  const size_t bytes = (size_t)(TM_WARP_THREADS / 32) * stride * 4;
-  if (Bmin == 8 && Bmax == 8)
-    k_train_warp<7, true><<<grid, TM_WARP_THREADS, bytes, st>>>(
-        machines, work, nwork, counter, e_begin, e_end, slice, Wpmax, ovf_cap, stride, pairs);
+  const size_t bytes = (size_t)wpc * stride * 4;
+  const bool exact = Bmin == 8 && Bmax == 8;
+  if (wpc == 1)
+    warp_launch<1>(exact, grid, bytes, st, machines, work, nwork, counter, e_begin, e_end, slice,
+                   Wpmax, ovf_cap, stride, pairs);
   else
-    k_train_warp<7, false><<<grid, TM_WARP_THREADS, bytes, st>>>(
-        machines, work, nwork, counter, e_begin, e_end, slice, Wpmax, ovf_cap, stride, pairs);
+    warp_launch<4>(exact, grid, bytes, st, machines, work, nwork, counter, e_begin, e_end, slice,
+                   Wpmax, ovf_cap, stride, pairs);
   return cudaGetLastError();
 }
 

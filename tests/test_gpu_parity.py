@@ -432,9 +432,10 @@ def test_global_planes_chosen_by_occupancy(tm, monkeypatch):
 
 @pytest.mark.parametrize("features", [784, 4500])
 def test_every_train_variant_matches_oracle(tm, features):
-    """Each train-kernel variant, pinned in turn -- one warp per unit, shared
-    or global count planes with 1, 2 or 4 clauses per warp, the 2-CTA
-    cluster -- ends in the oracle's state, bit for bit."""
+    """Each train-kernel variant, pinned in turn -- one warp per unit (four
+    units or one per CTA), shared or global count planes with 1, 2 or 4
+    clauses per warp, the 2-CTA cluster, the word-per-thread
+    configurations -- ends in the oracle's state, bit for bit."""
     from santoku_tsetlin import datagen
     rng = np.random.default_rng(features + 7)
     n, classes = 200, 4
@@ -447,7 +448,7 @@ def test_every_train_variant_matches_oracle(tm, features):
     want = (m.actions(), m.state())
     variants = [(0, 1), (0, 2), (0, 4), (1, 1), (1, 2), (1, 4), (2, 1)]
     if features <= 1024:
-        variants.append((3, 1))
+        variants += [(3, 1), (3, 2)]
     # the word-per-thread kernel's configurations that hold these rows
     # (4500 features: 282 words -> 512 threads x 2 words; 784: 52 words)
     wp = ((2 * features + 31) // 32 + 3) // 4 * 4
@@ -467,12 +468,12 @@ def test_every_train_variant_matches_oracle(tm, features):
         assert np.array_equal(s, want[1]), (mode, cpw)
         t.destroy()
     t = tm.create(kind, tbl)
-    t.force_variant(3, 2)
+    t.force_variant(3, 4)
     with pytest.raises(tm.TsetlinError):
         t.force_variant(1, 3)
     with pytest.raises(tm.TsetlinError):
         t.force_variant(4, 9)
-    with pytest.raises(tm.TsetlinError):  # the warp kernel has one clause layout
+    with pytest.raises(tm.TsetlinError):  # the warp kernel holds four units or one per CTA
         t.train(train_table(kind, inp, 1))
     t.destroy()
 
