@@ -630,8 +630,9 @@ static bool plan_mode(int mode, const TrainShape &sh, TrainPlan &p, int cpw = 1)
     return true;
   }
   if (mode == TM_MODE_WARP) {
-    // cpw selects the units per CTA: 1 -> four, 2 -> one
+    // cpw selects the units per CTA: 1 -> four, 2 -> one (8-bit automata)
     if (sh.Wpmax > 64 || sh.Bmax > 8 || (cpw != 1 && cpw != 2)) return false;
+    if (cpw == 2 && (sh.Bmin != 8 || sh.Bmax != 8)) return false;
     const int wpc = warp_units_per_cta(cpw);
     size_t wsm = 0;
     const int occ = train_warp_occupancy(sh.Wpmax, sh.Bmin, sh.Bmax, sh.smax, wpc, &wsm);
