@@ -241,8 +241,10 @@ def balanced_chunks(classes, threads, at_most):
 #       python bench.py --profile-launch c1_small
 INSTR_PER_PAIR = {
     # batched search rows (784 / 392 features, 40 % flipped bits), 64
-    # machines, one epoch over 6,000 samples: 87.03e9 and 90.86e9 / 105.91e6
-    ("search", 3, 1): 821.7,     # one warp per unit
+    # machines, one epoch over 6,000 samples: 87.03e9, 87.91e9 and 90.86e9
+    # / 105.91e6
+    ("search", 3, 1): 821.7,     # one warp per unit, four units per CTA
+    ("search", 3, 2): 830.0,     # one warp per unit, one unit per CTA
     ("search", 4, 7): 857.9,     # one warp per unit, 2 words per lane in registers
     # large sparse classifier rows (16,384 features), c1_small (1.091e6 active
     # steps): 13.54e9 global planes; 11.66e9 word-per-thread (512 x 2 words)
