@@ -430,7 +430,7 @@ def test_global_planes_chosen_by_occupancy(tm, monkeypatch):
     assert np.array_equal(st, m.state())
 
 
-@pytest.mark.parametrize("features", [784, 4500])
+@pytest.mark.parametrize("features", [784, 4000, 4500])
 def test_every_train_variant_matches_oracle(tm, features):
     """Each train-kernel variant, pinned in turn -- one warp per unit (four
     units or one per CTA), shared or global count planes with 1, 2 or 4
@@ -455,6 +455,8 @@ def test_every_train_variant_matches_oracle(tm, features):
     for cid, words in ((1, 1024), (2, 256), (3, 512), (4, 256), (5, 64), (6, 64), (7, 64)):
         if wp <= words:
             variants.append((4, cid))
+    if wp <= 256:  # one warp per unit, count planes in global memory
+        variants.append((5, 1))
     kind, tbl = ref_table(cfg, seed=31)
     for mode, cpw in variants:
         t = tm.create(kind, tbl)
@@ -473,8 +475,38 @@ def test_every_train_variant_matches_oracle(tm, features):
         t.force_variant(1, 3)
     with pytest.raises(tm.TsetlinError):
         t.force_variant(4, 9)
+    with pytest.raises(tm.TsetlinError):
+        t.force_variant(5, 2)
     with pytest.raises(tm.TsetlinError):  # the warp kernel holds four units or one per CTA
         t.train(train_table(kind, inp, 1))
+    t.destroy()
+
+
+@pytest.mark.parametrize("visible,variant", [(2000, (5, 1)), (4096, (5, 1)), (4096, (1, 4))],
+                         ids=["warpg128", "warpg256", "global4"])
+def test_encoder_variants_match_oracle(tm, visible, variant):
+    """Encoders (every sample trains every unit, the target is the code
+    bit) on 125- and 256-word rows: the one-warp kernel with global count
+    planes (4 and 8 words per lane) and the CTA kernel with global planes
+    end in the oracle's state, bit for bit, over two epochs."""
+    from santoku_tsetlin import datagen
+    rng = np.random.default_rng(visible)
+    n, hidden = 160, 12
+    x = datagen.flip_pack(rng.random((n, visible)) < 0.05).ravel()
+    codes = rng.integers(0, 256, size=n * 2).astype(np.uint8)
+    cfg = dict(type="encoder", classes=hidden, features=visible, clauses=24,
+               clause_tolerance=16, clause_maximum=48, specificity=15.0, target=20)
+    inp = dict(n=n, x=x, codes=codes)
+    m = _oracle_pair("encoder", cfg, inp, 2, seed=5)
+    kind, tbl = ref_table(cfg, seed=5)
+    t = tm.create(kind, tbl)
+    t.force_variant(*variant)
+    t.stats_enable(True)
+    t.train(train_table(kind, inp, 2))
+    assert (t.stats()["train_mode"], t.stats()["train_cpw"]) == variant
+    a, st = t.export_state()
+    assert np.array_equal(a, m.actions())
+    assert np.array_equal(st, m.state())
     t.destroy()
 
 
