@@ -819,6 +819,21 @@ static int autotune_plan(std::vector<TrainJob> &jobs, const std::vector<TrainDev
   for (size_t i = 0; i < nu; i++) tw.push_back(work[i * work.size() / nu]);
   TrainShape tsh = sh;
   tsh.units = (uint32_t)nu;
+  // every trial starts from the initial state (capi.c:1136-1146): a trial
+  // on automata that earlier trials trained would see another feedback mix
+  auto reset = [&]() -> int {
+    for (auto &J : jobs) {
+      tm_machine *m = J.m;
+      cudaError_t e = launch_setup(m->d_act, m->d_cnt, m->d_cls, m->classes, m->clauses, m->B,
+                                   m->act_words, m0->st);
+      if (e != cudaSuccess) return fail(TM_ERR_CUDA, "setup: %s", cudaGetErrorString(e));
+      note_launch(m0, 1);
+    }
+    return TM_OK;
+  };
+  // TSETLIN_B200_TUNE_LOG=1: each candidate's trial time on stderr
+  const char *tl = getenv("TSETLIN_B200_TUNE_LOG");
+  const bool tune_log = tl && tl[0] == '1';
   int best = -1;
   float best_ms = 0;
   for (size_t i = 0; i < cand.size(); i++) {
@@ -826,24 +841,26 @@ static int autotune_plan(std::vector<TrainJob> &jobs, const std::vector<TrainDev
     if (!plan_mode(cand[i].mode, tsh, p, cand[i].cpw)) continue;
     float t = 0, tmin = 0;
     for (int rep = 0; rep < 2; rep++) {
+      int rc = reset();
+      if (rc) return rc;
       uint32_t herr = 0;
-      int rc = launch_plan(p, tsh, ttd, tw, 0, 1, m0, &t, &herr);
+      rc = launch_plan(p, tsh, ttd, tw, 0, 1, m0, &t, &herr);
       if (rc) return rc;
       if (herr) return fail(TM_ERR_DEVICE, "train: a sample copy did not complete (status %u)", herr);
       tmin = rep == 0 ? t : std::min(tmin, t);
     }
+    if (tune_log)
+      fprintf(stderr, "tsetlin_b200 tune: variant %d:%d  %.3f ms  (%zu units, grid %d)\n",
+              cand[i].mode, cand[i].cpw, tmin, nu, p.grid);
     if (best < 0 || tmin < best_ms) {
       best = (int)i;
       best_ms = tmin;
     }
   }
-  // back to the initial state (capi.c:1136-1146)
-  for (auto &J : jobs) {
-    tm_machine *m = J.m;
-    cudaError_t e = launch_setup(m->d_act, m->d_cnt, m->d_cls, m->classes, m->clauses, m->B,
-                                 m->act_words, m0->st);
-    if (e != cudaSuccess) return fail(TM_ERR_CUDA, "setup: %s", cudaGetErrorString(e));
-    note_launch(m0, 1);
+  // back to the initial state
+  {
+    int rc = reset();
+    if (rc) return rc;
   }
   if (best < 0) return TM_OK;
   {
