@@ -804,23 +804,26 @@ static int autotune_plan(std::vector<TrainJob> &jobs, const std::vector<TrainDev
     }
   }
   if (cand.size() < 2) return TM_OK;  // nothing to choose: the heuristic plan
-  // trial: up to 2,048 samples of epoch 0 on up to 32 units per SM, taken
-  // evenly from the cost-ordered work list -- enough units that every
-  // candidate's grid is full (the most resident units per SM of any
-  // variant is below 32), so that occupancy counts as in the real launch.
-  // (Extrapolating each variant's time to the launch's samples from a
-  // second, shorter trial was tried: on the encoder it chose a variant 7 %
-  // slower over the full epoch, and it changed no other choice.)
-  std::vector<TrainDev> ttd = td;
-  for (auto &t : ttd) t.n = std::min<uint32_t>(t.n, 2048);
-  const size_t nu = std::min<size_t>(work.size(), (size_t)sh.sms * 32);
-  std::vector<WorkItem> tw;
-  tw.reserve(nu);
-  for (size_t i = 0; i < nu; i++) tw.push_back(work[i * work.size() / nu]);
-  TrainShape tsh = sh;
-  tsh.units = (uint32_t)nu;
-  // every trial starts from the initial state (capi.c:1136-1146): a trial
-  // on automata that earlier trials trained would see another feedback mix
+  // Two trials, each on automata reset to the initial state (capi.c:1136-
+  // 1146; a trial on automata that earlier trials trained would see another
+  // feedback mix).  The first times every candidate on up to 2,048 samples
+  // of epoch 0 and up to 32 units per SM, taken evenly from the cost-ordered
+  // work list -- enough units that every candidate's grid is full, so that
+  // occupancy counts as in the real launch.  The second times the three
+  // fastest again on up to 8,192 samples and 64 units per SM, where wave
+  // tails and start-up costs weigh less, and decides.
+  auto trial_units = [&](size_t per_sm) {
+    const size_t nu = std::min<size_t>(work.size(), (size_t)sh.sms * per_sm);
+    std::vector<WorkItem> tw;
+    tw.reserve(nu);
+    for (size_t i = 0; i < nu; i++) tw.push_back(work[i * work.size() / nu]);
+    return tw;
+  };
+  auto trial_rows = [&](uint32_t cap) {
+    std::vector<TrainDev> tt = td;
+    for (auto &t : tt) t.n = std::min<uint32_t>(t.n, cap);
+    return tt;
+  };
   auto reset = [&]() -> int {
     for (auto &J : jobs) {
       tm_machine *m = J.m;
@@ -834,29 +837,58 @@ static int autotune_plan(std::vector<TrainJob> &jobs, const std::vector<TrainDev
   // TSETLIN_B200_TUNE_LOG=1: each candidate's trial time on stderr
   const char *tl = getenv("TSETLIN_B200_TUNE_LOG");
   const bool tune_log = tl && tl[0] == '1';
-  int best = -1;
-  float best_ms = 0;
-  for (size_t i = 0; i < cand.size(); i++) {
+  // the trials' (unit, sample) steps are not the caller's training
+  const uint64_t pairs0 = m0->stats.train_active_pairs;
+  auto timed = [&](size_t i, const std::vector<TrainDev> &tt, const std::vector<WorkItem> &tw,
+                   int stage, float &tmin) -> int {
+    TrainShape tsh = sh;
+    tsh.units = (uint32_t)tw.size();
     TrainPlan p;
-    if (!plan_mode(cand[i].mode, tsh, p, cand[i].cpw)) continue;
-    float t = 0, tmin = 0;
+    tmin = -1;
+    if (!plan_mode(cand[i].mode, tsh, p, cand[i].cpw)) return TM_OK;
+    float t = 0;
     for (int rep = 0; rep < 2; rep++) {
       int rc = reset();
       if (rc) return rc;
       uint32_t herr = 0;
-      rc = launch_plan(p, tsh, ttd, tw, 0, 1, m0, &t, &herr);
+      rc = launch_plan(p, tsh, tt, tw, 0, 1, m0, &t, &herr);
       if (rc) return rc;
       if (herr) return fail(TM_ERR_DEVICE, "train: a sample copy did not complete (status %u)", herr);
       tmin = rep == 0 ? t : std::min(tmin, t);
     }
     if (tune_log)
-      fprintf(stderr, "tsetlin_b200 tune: variant %d:%d  %.3f ms  (%zu units, grid %d)\n",
-              cand[i].mode, cand[i].cpw, tmin, nu, p.grid);
-    if (best < 0 || tmin < best_ms) {
-      best = (int)i;
-      best_ms = tmin;
+      fprintf(stderr, "tsetlin_b200 tune %d: variant %d:%d  %.3f ms  (%zu units, grid %d)\n",
+              stage, cand[i].mode, cand[i].cpw, tmin, tw.size(), p.grid);
+    return TM_OK;
+  };
+  std::vector<std::pair<float, size_t>> first;
+  {
+    const std::vector<TrainDev> tt = trial_rows(2048);
+    const std::vector<WorkItem> tw = trial_units(32);
+    for (size_t i = 0; i < cand.size(); i++) {
+      float tmin = -1;
+      int rc = timed(i, tt, tw, 1, tmin);
+      if (rc) return rc;
+      if (tmin >= 0) first.emplace_back(tmin, i);
     }
   }
+  std::sort(first.begin(), first.end());
+  int best = first.empty() ? -1 : (int)first[0].second;
+  if (first.size() > 1) {
+    const std::vector<TrainDev> tt = trial_rows(8192);
+    const std::vector<WorkItem> tw = trial_units(64);
+    float best_ms = -1;
+    for (size_t r = 0; r < first.size() && r < 3; r++) {
+      float tmin = -1;
+      int rc = timed(first[r].second, tt, tw, 2, tmin);
+      if (rc) return rc;
+      if (tmin >= 0 && (best_ms < 0 || tmin < best_ms)) {
+        best_ms = tmin;
+        best = (int)first[r].second;
+      }
+    }
+  }
+  m0->stats.train_active_pairs = pairs0;
   // back to the initial state
   {
     int rc = reset();
