@@ -630,6 +630,15 @@ def run_search_bench(args):
     # ---- plain: one machine at a time, one launch per epoch, host metric ---
     pe = min(args.plain_epochs, E)
     plain_final = {}
+    # untimed: one short train call per machine, so that the variant choice
+    # of every machine's launch shape is tuned and cached before the timing
+    # (the batched form's was, in its warm-up round)
+    for p in params:
+        m = make_search_machines(tm, [p])[0]
+        k = min(2048, n_train)
+        m.train({"samples": k, "problems": xd[p["negated"]][0][:k], "solutions": yd[:k],
+                 "iterations": 1})
+        m.destroy()
     barrier(ws)
     torch.cuda.synchronize()
     p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

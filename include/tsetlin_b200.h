@@ -338,8 +338,7 @@ typedef struct tm_stats {
                                  1 count planes in global memory, 2 split over a 2-CTA
                                  cluster, 3 one warp per unit (rows of at most 64 words),
                                  4 words owned by threads (automata in registers and
-                                 shared memory), 5 one warp per unit with the count
-                                 planes in global memory (rows of at most 256 words) */
+                                 shared memory) */
   int32_t train_autotuned;    /* 1 if the autotuner chose that variant */
   int32_t train_cpw;          /* modes 0-2: clauses per warp; mode 3: 1 = four units per
                                  CTA, 2 = one; mode 4: the configuration (1-7) */
@@ -365,7 +364,7 @@ int tm_set_autotune(tm_machine *m, int32_t mode);
 /* Pins the train-kernel variant (train_mode values of tm_stats; cpw, the
  * clauses evaluated per warp in a single-CTA variant with 8 state bits: 1,
  * 2 or 4 -- 256 / cpw threads per unit; for mode 3, 1 or 2: four units or
- * one per CTA; for mode 4, the configuration; for mode 5, 1); mode -1 returns to the automatic
+ * one per CTA; for mode 4, the configuration); mode -1 returns to the automatic
  * choice.  A train call that the pinned variant cannot run fails with
  * TM_ERR_ARG.  The environment variable TSETLIN_B200_VARIANT=mode:cpw, read
  * when a machine is created, pins the same way.  For tests and

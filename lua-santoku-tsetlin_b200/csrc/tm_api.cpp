@@ -290,7 +290,6 @@ static int check_limits(tm_machine *m) {
 // clauses per warp, or mode 4 with one of its configurations.
 static bool variant_ok(int mode, int cpw) {
   if (mode == TM_MODE_WPT) return cpw >= 1 && cpw <= wpt_configs();
-  if (mode == TM_MODE_WARPG) return cpw == 1;
   return mode >= -1 && mode <= TM_MODE_WARP && (cpw == 1 || cpw == 2 || cpw == 4);
 }
 
@@ -413,8 +412,8 @@ extern "C" void tm_destroy(tm_machine *m) {
 extern "C" int tm_force_variant(tm_machine *m, int32_t mode, int32_t cpw) {
   if (!m) return fail(TM_ERR_ARG, "null machine");
   if (!variant_ok(mode, cpw))
-    return fail(TM_ERR_ARG, "force_variant: mode -1..3 with clauses per warp 1, 2 or 4, mode 4 "
-                            "with a configuration 1..%d, or mode 5 with 1", wpt_configs());
+    return fail(TM_ERR_ARG, "force_variant: mode -1..3 with clauses per warp 1, 2 or 4, or mode 4 "
+                            "with a configuration 1..%d", wpt_configs());
   m->force_mode = mode;
   m->force_cpw = cpw;
   return TM_OK;
@@ -630,16 +629,6 @@ static bool plan_mode(int mode, const TrainShape &sh, TrainPlan &p, int cpw = 1)
     p.grid = (int)std::min<uint64_t>(sh.units, (uint64_t)sh.sms * occ);
     return true;
   }
-  if (mode == TM_MODE_WARPG) {
-    // one warp per unit, count planes in global memory: rows of at most 256
-    // words, 8-bit automata
-    if (cpw != 1 || sh.Bmin != 8 || sh.Bmax != 8 || !train_warpg_wpl(sh.Wpmax)) return false;
-    size_t bytes = 0;
-    const int occ = train_warpg_occupancy(sh.Wpmax, sh.smax, &bytes);
-    if (occ <= 0 || (int)bytes > sh.optin) return false;
-    p.grid = (int)std::min<uint64_t>(sh.units, (uint64_t)sh.sms * occ);
-    return true;
-  }
   if (mode == TM_MODE_WARP) {
     // cpw selects the units per CTA: 1 -> four, 2 -> one (8-bit automata)
     if (sh.Wpmax > 64 || sh.Bmax > 8 || (cpw != 1 && cpw != 2)) return false;
@@ -693,7 +682,7 @@ static int heuristic_plan(const TrainShape &sh, const tm_machine *m0, TrainPlan 
 // per unit, or a 2-CTA cluster per unit.
 static uint64_t resident_units(const TrainPlan &p) {
   if (p.mode == TM_MODE_WARP) return (uint64_t)p.grid * warp_units_per_cta(p.cpw);
-  if (p.mode == TM_MODE_WPT || p.mode == TM_MODE_WARPG) return (uint64_t)p.grid;
+  if (p.mode == TM_MODE_WPT) return (uint64_t)p.grid;
   if (p.mode == TM_MODE_PAIR) return (uint64_t)p.grid / 2;
   return (uint64_t)p.grid;
 }
@@ -724,10 +713,6 @@ static int launch_plan(const TrainPlan &p, const TrainShape &sh, const std::vect
                          (uint32_t)work.size(), counter, e0, e1, sh.Wpmax, sh.Bmin, sh.Bmax,
                          sh.smax, warp_units_per_cta(p.cpw), p.grid, st,
                          (unsigned long long *)(err + 2)));
-  else if (p.mode == TM_MODE_WARPG)
-    CK(launch_train_warpg((const TrainDev *)base, (const WorkItem *)(base + off_w),
-                          (uint32_t)work.size(), counter, e0, e1, sh.Wpmax, sh.smax, p.grid, st,
-                          (unsigned long long *)(err + 2)));
   else if (p.mode == TM_MODE_WPT)
     CK(launch_train_wpt(p.cpw, (const TrainDev *)base, (const WorkItem *)(base + off_w),
                         (uint32_t)work.size(), counter, e0, e1, sh.Wpmax, sh.smax, m0->row_wait,
@@ -788,9 +773,8 @@ static int autotune_plan(std::vector<TrainJob> &jobs, const std::vector<TrainDev
     CK(cudaEventCreate(&m0->ev1));
   }
   std::vector<TrainPlan> cand;
-  for (int mode : {TM_MODE_WARP, TM_MODE_SMEM, TM_MODE_GLOBAL, TM_MODE_PAIR, TM_MODE_WPT,
-                   TM_MODE_WARPG}) {
-    if ((mode == TM_MODE_WARP || mode == TM_MODE_WARPG) && m0->no_warp) continue;
+  for (int mode : {TM_MODE_WARP, TM_MODE_SMEM, TM_MODE_GLOBAL, TM_MODE_PAIR, TM_MODE_WPT}) {
+    if (mode == TM_MODE_WARP && m0->no_warp) continue;
     if (mode == TM_MODE_WPT) {
       for (int id = 1; id <= wpt_configs(); id++) {
         TrainPlan p;
@@ -1514,10 +1498,6 @@ static int search_round(tm_machine *const *ms, const tm_train_args *args, uint32
                                (uint32_t)work.size(), counter, 0, 1, sh.Wpmax, sh.Bmin, sh.Bmax,
                                sh.smax, warp_units_per_cta(plan.cpw), plan.grid, st,
                                (unsigned long long *)(d_err + 2));
-      else if (plan.mode == TM_MODE_WARPG)
-        ce = launch_train_warpg((const TrainDev *)tbase, (const WorkItem *)(tbase + off_w),
-                                (uint32_t)work.size(), counter, 0, 1, sh.Wpmax, sh.smax,
-                                plan.grid, st, (unsigned long long *)(d_err + 2));
       else if (plan.mode == TM_MODE_WPT)
         ce = launch_train_wpt(plan.cpw, (const TrainDev *)tbase, (const WorkItem *)(tbase + off_w),
                               (uint32_t)work.size(), counter, 0, 1, sh.Wpmax, sh.smax,

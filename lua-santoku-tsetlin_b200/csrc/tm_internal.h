@@ -124,15 +124,6 @@ cudaError_t launch_train_warp(const TrainDev *machines, const WorkItem *work, ui
                               uint32_t *counter, uint32_t e_begin, uint32_t e_end, uint32_t Wpmax,
                               uint32_t Bmin, uint32_t Bmax, uint32_t smax, int wpc, int grid,
                               cudaStream_t st, unsigned long long *pairs);
-// k_train_warpg (tm_train_warpg.cu): one warp per unit for rows of at most
-// 256 words with 8-bit automata, count planes in global memory
-constexpr int TM_MODE_WARPG = 5;
-int train_warpg_wpl(uint32_t Wpmax);  // words per lane (4 or 8), 0 if the rows are too wide
-int train_warpg_occupancy(uint32_t Wpmax, uint32_t smax, size_t *smem_bytes);
-cudaError_t launch_train_warpg(const TrainDev *machines, const WorkItem *work, uint32_t nwork,
-                               uint32_t *counter, uint32_t e_begin, uint32_t e_end,
-                               uint32_t Wpmax, uint32_t smax, int grid, cudaStream_t st,
-                               unsigned long long *pairs);
 // The fused train kernels report through err[0] (status bits) and
 // err[2..3], a 64-bit count of active (unit, sample) steps -- the samples
 // each unit actually trained on after negative sampling.

@@ -455,8 +455,6 @@ def test_every_train_variant_matches_oracle(tm, features):
     for cid, words in ((1, 1024), (2, 256), (3, 512), (4, 256), (5, 64), (6, 64), (7, 64)):
         if wp <= words:
             variants.append((4, cid))
-    if wp <= 256:  # one warp per unit, count planes in global memory
-        variants.append((5, 1))
     kind, tbl = ref_table(cfg, seed=31)
     for mode, cpw in variants:
         t = tm.create(kind, tbl)
@@ -476,19 +474,20 @@ def test_every_train_variant_matches_oracle(tm, features):
     with pytest.raises(tm.TsetlinError):
         t.force_variant(4, 9)
     with pytest.raises(tm.TsetlinError):
-        t.force_variant(5, 2)
+        t.force_variant(5, 1)
     with pytest.raises(tm.TsetlinError):  # the warp kernel holds four units or one per CTA
         t.train(train_table(kind, inp, 1))
     t.destroy()
 
 
-@pytest.mark.parametrize("visible,variant", [(2000, (5, 1)), (4096, (5, 1)), (4096, (1, 4))],
-                         ids=["warpg128", "warpg256", "global4"])
+@pytest.mark.parametrize("visible,variant", [(2000, (1, 4)), (4096, (1, 4)), (4096, (4, 2)),
+                                             (4096, (4, 4))],
+                         ids=["global4_128", "global4_256", "wpt2_256", "wpt4_256"])
 def test_encoder_variants_match_oracle(tm, visible, variant):
     """Encoders (every sample trains every unit, the target is the code
-    bit) on 125- and 256-word rows: the one-warp kernel with global count
-    planes (4 and 8 words per lane) and the CTA kernel with global planes
-    end in the oracle's state, bit for bit, over two epochs."""
+    bit) on 128- and 256-word rows: the CTA kernel with global count planes
+    and the word-per-thread configurations that hold these rows end in the
+    oracle's state, bit for bit, over two epochs."""
     from santoku_tsetlin import datagen
     rng = np.random.default_rng(visible)
     n, hidden = 160, 12
