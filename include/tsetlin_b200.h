@@ -342,7 +342,7 @@ typedef struct tm_stats {
   int32_t train_autotuned;    /* 1 if the autotuner chose that variant */
   int32_t train_cpw;          /* modes 0-2: clauses per warp; mode 3: 1 = four units per
                                  CTA, 2 = one; mode 4: the configuration (1-7) */
-  int32_t pad_;
+  int32_t predict_gemm;       /* last predict: 0 bitwise kernels, 1 int8 GEMM, 2 e4m3 GEMM */
   uint64_t train_active_pairs; /* (unit, sample) steps trained after negative sampling */
   double search_epoch_ms;     /* device-resident search rounds: summed epoch graph time */
   uint64_t search_epochs;     /* epoch graph replays */

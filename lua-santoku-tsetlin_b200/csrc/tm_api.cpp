@@ -147,6 +147,12 @@ struct tm_machine {
   // device-resident search round: checkpoint of the actions, and (owner of
   // the round) its tables and the staged holdout truth
   DevBuf ckpt, search, search_truth;
+  // large-batch predict as a GEMM: the action bytes (valid while act8_valid,
+  // in the encoding of act8_kind), a chunk of sample bytes, the chunk's
+  // clause x sample products and the library's workspace
+  DevBuf act8, x8, gemm_c, gemm_ws;
+  bool act8_valid = false;
+  int act8_kind = 0;
   // pinned staging of small host requests (TM_PIN_STAGE bytes each way):
   // inputs go host -> pin -> device, outputs device -> pin -> host, so that
   // a one-sample predict makes no pageable (synchronously staged) copy.
@@ -155,6 +161,13 @@ struct tm_machine {
   cudaEvent_t pin_ev = nullptr;
   bool pin_pending = false;
 };
+
+// The automata changed: the literal counts and the action bytes of the GEMM
+// predict are stale.
+static void invalidate_derived(tm_machine *m) {
+  m->lits_valid = false;
+  m->act8_valid = false;
+}
 
 constexpr uint64_t TM_PIN_STAGE = 256 << 10;
 
@@ -261,7 +274,7 @@ static int alloc_device(tm_machine *m, bool with_state) {
   CK(cudaMemcpyAsync(m->d_cls, m->cls.data(), m->classes * sizeof(ClassDev),
                      cudaMemcpyHostToDevice, m->st));
   CK(tmb_dev_malloc((void **)&m->d_lits, std::max<uint64_t>((uint64_t)m->classes * m->clauses, 1) * 4));
-  m->lits_valid = false;
+  invalidate_derived(m);
   m->has_state = with_state;
   return TM_OK;
 }
@@ -399,7 +412,7 @@ extern "C" void tm_destroy(tm_machine *m) {
   free_device(m);
   for (DevBuf *b : {&m->x, &m->tx, &m->raw, &m->labels, &m->codes, &m->perm, &m->perm_scratch, &m->sums,
                     &m->outc, &m->work, &m->tdev, &m->cls_job, &m->errf, &m->ckpt, &m->search,
-                    &m->search_truth})
+                    &m->search_truth, &m->act8, &m->x8, &m->gemm_c, &m->gemm_ws})
     b->release();
   if (m->ev0) cudaEventDestroy(m->ev0);
   if (m->ev1) cudaEventDestroy(m->ev1);
@@ -1076,7 +1089,7 @@ static int prepare_job(TrainJob &J, DevBuf &xbuf, DevBuf &lbuf, DevBuf &cbuf, De
 }
 
 static int finish_train(tm_machine *m) {
-  m->lits_valid = false;
+  invalidate_derived(m);
   m->trained = true;
   if (!m->reusable) {
     // capi.c:1187-1188 / :718-723: a non-reusable machine drops its state
@@ -1116,7 +1129,7 @@ extern "C" int tm_train(tm_machine *m, const tm_train_args *a) {
     for (uint32_t e0 = 0; e0 < E; e0++) {
       rc = run_epochs(jobs, e0, e0 + 1, m);
       if (rc) return rc;
-      m->lits_valid = false;
+      invalidate_derived(m);
       // capi.c:1168-1182: `each(epoch)`; false (non-zero here) stops
       if (a->each(a->each_user, e0 + 1) != 0) break;
     }
@@ -1234,7 +1247,7 @@ static int train_batch_impl(tm_machine *const *ms, const tm_train_args *args, ui
       if (live.empty()) break;
       int rc = run_epochs(live, e0, e0 + 1, m0);
       if (rc) return rc;
-      for (uint32_t i = 0; i < count; i++) ms[i]->lits_valid = false;
+      for (uint32_t i = 0; i < count; i++) invalidate_derived(ms[i]);
       std::vector<int32_t> req(count, 0);
       const int all = each(user, e0 + 1, req.data(), count);
       for (uint32_t i = 0; i < count; i++)
@@ -1650,6 +1663,92 @@ static int ensure_lits(tm_machine *m) {
   return TM_OK;
 }
 
+// ---- large-batch predict as a GEMM ------------------------------------------
+// The 8-bit encoding the GEMM uses on each device: 0 not yet tried, a
+// TM_GEMM_* kind, or -1 when the library offers neither (the bitwise
+// kernels then serve every size).  TSETLIN_B200_GEMM=off|int8|fp8 overrides
+// the choice at the first large predict of the process.
+static std::mutex g_gemm_mu;
+static int g_gemm_kind[64];
+
+static int gemm_kind_of(int dev) {
+  std::lock_guard<std::mutex> lk(g_gemm_mu);
+  if (dev < 0 || dev >= 64) return -1;
+  if (g_gemm_kind[dev] == 0) {
+    const char *e = getenv("TSETLIN_B200_GEMM");
+    if (e && !strcmp(e, "off")) g_gemm_kind[dev] = -1;
+    else if (e && !strcmp(e, "fp8")) g_gemm_kind[dev] = TM_GEMM_FP8;
+    else g_gemm_kind[dev] = TM_GEMM_INT8;
+  }
+  return g_gemm_kind[dev];
+}
+
+static void gemm_kind_failed(int dev, int kind) {
+  std::lock_guard<std::mutex> lk(g_gemm_mu);
+  if (dev >= 0 && dev < 64 && g_gemm_kind[dev] == kind)
+    g_gemm_kind[dev] = kind == TM_GEMM_INT8 ? TM_GEMM_FP8 : -1;
+}
+
+// Whether a predict of n samples goes through the GEMM: dense machines,
+// past the small-batch kernel's sizes, and enough bitwise work (clauses x
+// samples x row words >= 2^28, about 50 µs of the bitwise kernel) to pay
+// for the byte expansions and the library call.
+static bool gemm_wanted(tm_machine *m, uint64_t n) {
+  if (m->individualized || n <= TM_SMALL_N_MAX) return false;
+  const uint64_t M = (uint64_t)m->classes * m->clauses;
+  if (M * n * m->cls[0].W < (1ull << 28)) return false;
+  return gemm_kind_of(m->device) > 0;
+}
+
+// The vote sums of the n staged rows (m->x) through the GEMM.  Returns
+// TM_OK, a TM_ERR_* code, or 1 when the library has no algorithm for the
+// device's encoding (nothing was written; the caller uses the bitwise
+// kernels).
+static int predict_gemm(tm_machine *m, uint64_t n) {
+  const ClassDev &c0 = m->cls[0];
+  const uint64_t M = (uint64_t)m->classes * m->clauses, K = (uint64_t)c0.W * 32;
+  while (true) {
+    const int kind = gemm_kind_of(m->device);
+    if (kind <= 0) return 1;
+    if (!m->act8_valid || m->act8_kind != kind) {
+      CK(m->act8.ensure(M * K));
+      // dense machines: the classes' clause rows follow each other
+      CK(launch_expand_bits(m->d_act + c0.act_off, M, c0.Wp, c0.W, c0.emask, kind,
+                            m->act8.as<uint8_t>(), m->st));
+      note_launch(m, 1);
+      m->act8_valid = true;
+      m->act8_kind = kind;
+    }
+    // samples per chunk: products of at most 512 MB, in multiples of 64
+    uint64_t nc = ((512ull << 20) / (4 * M)) / 64 * 64;
+    nc = std::max<uint64_t>(nc, 64);
+    nc = std::min<uint64_t>(nc, n);
+    const size_t ws_bytes = 32u << 20;
+    CK(m->x8.ensure(nc * K));
+    CK(m->gemm_c.ensure(nc * M * 4));
+    CK(m->gemm_ws.ensure(ws_bytes));
+    bool retry = false;
+    for (uint64_t s0 = 0; s0 < n; s0 += nc) {
+      const uint64_t k = std::min<uint64_t>(nc, n - s0);
+      CK(launch_expand_bits(m->x.as<uint32_t>() + s0 * c0.Wp, k, c0.Wp, c0.W, 0xFFFFFFFFu, kind,
+                            m->x8.as<uint8_t>(), m->st));
+      const int g = gemm_clause_products(m->device, kind, m->act8.as<uint8_t>(),
+                                         m->x8.as<uint8_t>(), m->gemm_c.p, M, k, K,
+                                         m->gemm_ws.p, ws_bytes, m->st);
+      if (g < 0 && s0 == 0) {
+        gemm_kind_failed(m->device, kind);
+        retry = true;
+        break;
+      }
+      if (g != 0) return fail(TM_ERR_CUDA, "predict: cuBLASLt matmul failed (status %d)", g);
+      CK(launch_gemm_votes(m->gemm_c.p, kind, m->d_lits, m->classes, m->clauses, m->tol,
+                           (uint32_t)k, m->sums.as<int32_t>() + s0 * m->classes, m->st));
+      note_launch(m, 3);
+    }
+    if (!retry) return TM_OK;
+  }
+}
+
 static int predict_common(tm_machine *m, const uint8_t *problems, const int64_t *dim_offsets,
                           uint64_t n, int64_t *out_classes, uint8_t *out_codes,
                           int64_t *out_scores, bool on_device) {
@@ -1675,10 +1774,15 @@ static int predict_common(tm_machine *m, const uint8_t *problems, const int64_t 
   rc = ensure_lits(m);
   if (rc) return rc;
   if (m->timing) CK(cudaEventRecord(m->ev0, m->st));
-  CK(launch_predict(m->d_act, m->d_lits, m->d_cls, nullptr, m->classes, m->clauses, m->tol,
-                    m->x.as<uint32_t>(), (uint32_t)n, m->sums.as<int32_t>(), m->st));
+  int gr = gemm_wanted(m, n) ? predict_gemm(m, n) : 1;
+  if (gr < 0) return gr;
+  m->stats.predict_gemm = gr == 0 ? m->act8_kind : 0;
+  if (gr == 1) {
+    CK(launch_predict(m->d_act, m->d_lits, m->d_cls, nullptr, m->classes, m->clauses, m->tol,
+                      m->x.as<uint32_t>(), (uint32_t)n, m->sums.as<int32_t>(), m->st));
+    note_launch(m, n <= TM_SMALL_N_MAX ? (n + 15) / 16 : 1);
+  }
   if (m->timing) CK(cudaEventRecord(m->ev1, m->st));
-  note_launch(m, n <= TM_SMALL_N_MAX ? (n + 15) / 16 : 1);
   m->stats.predict_launches++;
   // outputs
   int64_t *dcls = nullptr, *dsc = nullptr;
@@ -1843,7 +1947,7 @@ extern "C" int tm_import_state(tm_machine *m, const uint8_t *actions, const uint
   if (actions) {
     int rc = copy_all(m, false, (uint8_t *)actions, false);
     if (rc) return rc;
-    m->lits_valid = false;
+    invalidate_derived(m);
   }
   if (state) {
     if (!m->d_cnt) return fail(TM_ERR_STATE, "machine has no state");
@@ -1892,7 +1996,7 @@ static int classes_io(tm_machine *m, uint32_t lo, uint32_t hi, bool to_buf, uint
   if (actions) {
     int rc = copy_classes(m, lo, hi, to_buf, actions, false, on_device != 0);
     if (rc) return rc;
-    if (!to_buf) m->lits_valid = false;
+    if (!to_buf) invalidate_derived(m);
   }
   if (state) {
     int rc = copy_classes(m, lo, hi, to_buf, state, true, on_device != 0);

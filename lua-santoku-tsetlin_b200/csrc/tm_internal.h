@@ -124,6 +124,17 @@ cudaError_t launch_train_warp(const TrainDev *machines, const WorkItem *work, ui
                               uint32_t *counter, uint32_t e_begin, uint32_t e_end, uint32_t Wpmax,
                               uint32_t Bmin, uint32_t Bmax, uint32_t smax, int wpc, int grid,
                               cudaStream_t st, unsigned long long *pairs);
+// Large-batch predict as an 8-bit GEMM (tm_gemm.cu)
+constexpr int TM_GEMM_INT8 = 1;  // int8 operands, int32 accumulation
+constexpr int TM_GEMM_FP8 = 2;   // e4m3 operands, fp32 accumulation
+cudaError_t launch_expand_bits(const uint32_t *src, uint64_t rows, uint32_t stride, uint32_t W,
+                               uint32_t last_mask, int kind, uint8_t *dst, cudaStream_t st);
+cudaError_t launch_gemm_votes(const void *C, int kind, const int32_t *lits, uint32_t classes,
+                              uint32_t clauses, uint32_t tol, uint32_t N, int32_t *sums,
+                              cudaStream_t st);
+int gemm_clause_products(int dev, int kind, const uint8_t *A, const uint8_t *B, void *C,
+                         uint64_t M, uint64_t N, uint64_t K, void *ws, size_t ws_bytes,
+                         cudaStream_t st);
 // The fused train kernels report through err[0] (status bits) and
 // err[2..3], a 64-bit count of active (unit, sample) steps -- the samples
 // each unit actually trained on after negative sampling.

@@ -136,7 +136,7 @@ class Stats(ctypes.Structure):
         ("train_mode", ctypes.c_int32),
         ("train_autotuned", ctypes.c_int32),
         ("train_cpw", ctypes.c_int32),
-        ("pad_", ctypes.c_int32),
+        ("predict_gemm", ctypes.c_int32),
         ("train_active_pairs", ctypes.c_uint64),
         ("search_epoch_ms", ctypes.c_double),
         ("search_epochs", ctypes.c_uint64),
