@@ -1683,11 +1683,6 @@ static int gemm_kind_of(int dev) {
   return g_gemm_kind[dev];
 }
 
-static void gemm_kind_failed(int dev, int kind) {
-  std::lock_guard<std::mutex> lk(g_gemm_mu);
-  if (dev >= 0 && dev < 64 && g_gemm_kind[dev] == kind)
-    g_gemm_kind[dev] = kind == TM_GEMM_INT8 ? TM_GEMM_FP8 : -1;
-}
 
 // Whether a predict of n samples goes through the GEMM: dense machines,
 // past the small-batch kernel's sizes, and enough bitwise work (clauses x
@@ -1701,14 +1696,14 @@ static bool gemm_wanted(tm_machine *m, uint64_t n) {
 }
 
 // The vote sums of the n staged rows (m->x) through the GEMM.  Returns
-// TM_OK, a TM_ERR_* code, or 1 when the library has no algorithm for the
-// device's encoding (nothing was written; the caller uses the bitwise
-// kernels).
+// TM_OK, a TM_ERR_* code, or 1 when the library has no algorithm for this
+// shape in either encoding (nothing was written; the caller uses the
+// bitwise kernels).
 static int predict_gemm(tm_machine *m, uint64_t n) {
   const ClassDev &c0 = m->cls[0];
   const uint64_t M = (uint64_t)m->classes * m->clauses, K = (uint64_t)c0.W * 32;
+  int kind = gemm_kind_of(m->device);
   while (true) {
-    const int kind = gemm_kind_of(m->device);
     if (kind <= 0) return 1;
     if (!m->act8_valid || m->act8_kind != kind) {
       CK(m->act8.ensure(M * K));
@@ -1735,8 +1730,8 @@ static int predict_gemm(tm_machine *m, uint64_t n) {
       const int g = gemm_clause_products(m->device, kind, m->act8.as<uint8_t>(),
                                          m->x8.as<uint8_t>(), m->gemm_c.p, M, k, K,
                                          m->gemm_ws.p, ws_bytes, m->st);
-      if (g < 0 && s0 == 0) {
-        gemm_kind_failed(m->device, kind);
+      if (g < 0 && s0 == 0) {  // no algorithm: the other encoding, then the bitwise kernels
+        kind = kind == TM_GEMM_INT8 ? TM_GEMM_FP8 : -1;
         retry = true;
         break;
       }

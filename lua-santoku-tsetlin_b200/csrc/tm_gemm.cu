@@ -14,6 +14,9 @@
 #include <cublasLt.h>
 #include <cuda_runtime.h>
 
+#include <stdio.h>
+#include <stdlib.h>
+
 #include <mutex>
 
 #include "tm_internal.h"
@@ -94,7 +97,7 @@ int grid_for(uint64_t items, int threads) {
 
 std::mutex g_lt_mu;
 cublasLtHandle_t g_lt[64];
-int g_lt_state[64];  // 0 unknown, 1 ready, -1 unavailable
+int g_lt_state[64];  // 0 not created, 1 ready
 
 }  // namespace
 
@@ -133,10 +136,10 @@ int gemm_clause_products(int dev, int kind, const uint8_t *A, const uint8_t *B, 
   cublasLtHandle_t lt = nullptr;
   {
     std::lock_guard<std::mutex> lk(g_lt_mu);
-    if (g_lt_state[dev] == 0) {
-      g_lt_state[dev] = cublasLtCreate(&g_lt[dev]) == CUBLAS_STATUS_SUCCESS ? 1 : -1;
-    }
-    if (g_lt_state[dev] < 0) return -1;
+    // a failed creation is tried again at the next call
+    if (g_lt_state[dev] == 0 && cublasLtCreate(&g_lt[dev]) == CUBLAS_STATUS_SUCCESS)
+      g_lt_state[dev] = 1;
+    if (g_lt_state[dev] != 1) return -1;
     lt = g_lt[dev];
   }
   const bool fp8 = kind == TM_GEMM_FP8;
@@ -168,6 +171,14 @@ int gemm_clause_products(int dev, int kind, const uint8_t *A, const uint8_t *B, 
   int found = 0;
   if (s == CUBLAS_STATUS_SUCCESS)
     s = cublasLtMatmulAlgoGetHeuristic(lt, op, la, lb, lc, lc, pref, 1, &h, &found);
+  {
+    // TSETLIN_B200_GEMM_LOG=1: the library's answer for each shape on stderr
+    const char *lg = getenv("TSETLIN_B200_GEMM_LOG");
+    if (lg && lg[0] == '1')
+      fprintf(stderr, "tsetlin_b200 gemm: %s M=%llu N=%llu K=%llu status=%d algorithms=%d\n",
+              fp8 ? "e4m3" : "int8", (unsigned long long)M, (unsigned long long)N,
+              (unsigned long long)K, (int)s, found);
+  }
   if (s != CUBLAS_STATUS_SUCCESS || found == 0) {
     rc = -1;
   } else {
