@@ -462,11 +462,26 @@ def run_ours(args, w):
                                             / 1e3 + 1e-12),
         },
     }
-    if rank == 0:
+    if rank == 0 and st["predict_gemm"]:
+        # the predict ran as an 8-bit GEMM: clauses x samples x literal
+        # bytes (32 per row word), two operations per product
+        words = (((2 * w["features"] + 7) // 8 + 3) // 4)
+        ops = 2.0 * w["classes"] * w["clauses"] * (hi_s - lo_s) * 32 * words
+        t_s = st["predict_kernel_ms"] / max(1, st["predict_launches"]) / 1e3 + 1e-12
+        out["kernels"].update({
+            "predict_path": "int8 GEMM" if st["predict_gemm"] == 1 else "e4m3 GEMM",
+            "predict_tensor_ops_per_s": ops / t_s,
+            "predict_tensor_peak_ops_per_s": 4.5e15,
+            "predict_tensor_peak_source": "nominal dense 8-bit rate of a B200 (no measured "
+                                          "8-bit peak here); the predict time includes the "
+                                          "byte expansions and the vote epilogue",
+            "predict_frac_of_tensor_peak": ops / t_s / 4.5e15})
+    elif rank == 0:
         pk = tm.int_peaks(dev.index if dev.index is not None else 0)
         wops = out["kernels"]["predict_literal_evals_per_s"] / 32
         bound = min(32 * pk["lop3"] / 62, 32 * pk["popc"] / 17)
-        out["kernels"].update({"int_peaks_ops_per_s": pk, "predict_word_ops_per_s": wops,
+        out["kernels"].update({"predict_path": "bitwise", "int_peaks_ops_per_s": pk,
+                               "predict_word_ops_per_s": wops,
                                "predict_int_bound_word_ops_per_s": bound,
                                "predict_frac_of_int_bound": wops / bound})
     if ck:
