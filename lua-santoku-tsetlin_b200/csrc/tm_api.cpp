@@ -1699,21 +1699,30 @@ static bool gemm_wanted(tm_machine *m, uint64_t n) {
 // TM_OK, a TM_ERR_* code, or 1 when the library has no algorithm for this
 // shape in either encoding (nothing was written; the caller uses the
 // bitwise kernels).
+// The action bytes of a dense machine in `kind`'s encoding (queued on the
+// machine's stream).
+static int ensure_act8(tm_machine *m, int kind) {
+  if (m->act8_valid && m->act8_kind == kind) return TM_OK;
+  const ClassDev &c0 = m->cls[0];
+  const uint64_t M = (uint64_t)m->classes * m->clauses, K = (uint64_t)c0.W * 32;
+  CK(m->act8.ensure(M * K));
+  // dense machines: the classes' clause rows follow each other
+  CK(launch_expand_bits(m->d_act + c0.act_off, M, c0.Wp, c0.W, c0.emask, kind,
+                        m->act8.as<uint8_t>(), m->st));
+  note_launch(m, 1);
+  m->act8_valid = true;
+  m->act8_kind = kind;
+  return TM_OK;
+}
+
 static int predict_gemm(tm_machine *m, uint64_t n) {
   const ClassDev &c0 = m->cls[0];
   const uint64_t M = (uint64_t)m->classes * m->clauses, K = (uint64_t)c0.W * 32;
   int kind = gemm_kind_of(m->device);
   while (true) {
     if (kind <= 0) return 1;
-    if (!m->act8_valid || m->act8_kind != kind) {
-      CK(m->act8.ensure(M * K));
-      // dense machines: the classes' clause rows follow each other
-      CK(launch_expand_bits(m->d_act + c0.act_off, M, c0.Wp, c0.W, c0.emask, kind,
-                            m->act8.as<uint8_t>(), m->st));
-      note_launch(m, 1);
-      m->act8_valid = true;
-      m->act8_kind = kind;
-    }
+    int rc = ensure_act8(m, kind);
+    if (rc) return rc;
     // samples per chunk: products of at most 512 MB, in multiples of 64
     uint64_t nc = ((512ull << 20) / (4 * M)) / 64 * 64;
     nc = std::max<uint64_t>(nc, 64);
@@ -1835,6 +1844,21 @@ static int predict_common(tm_machine *m, const uint8_t *problems, const int64_t 
 
 int tmb_fail(int code, const char *msg) { return fail(code, "%s", msg); }
 
+int tmb_machine_act8(tm_machine *m, MachineView *v) {
+  v->act8 = nullptr;
+  v->act8_kind = 0;
+  if (!m || m->individualized) return TM_OK;
+  const int kind = gemm_kind_of(m->device);
+  if (kind <= 0) return TM_OK;
+  DevGuard g(m->device);
+  int rc = ensure_act8(m, kind);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(m->st));
+  v->act8 = m->act8.as<uint8_t>();
+  v->act8_kind = kind;
+  return TM_OK;
+}
+
 int tmb_machine_view(tm_machine *m, MachineView *v, const char *who) {
   if (!m || !v) return fail(TM_ERR_ARG, "null argument");
   if (m->individualized)
@@ -1859,6 +1883,9 @@ int tmb_machine_view(tm_machine *m, MachineView *v, const char *who) {
   v->type = (uint32_t)m->type;
   v->input_chunks = m->input_chunks;
   v->Wp = m->cls[0].Wp;
+  v->W = m->cls[0].W;
+  v->act8 = nullptr;
+  v->act8_kind = 0;
   v->class_chunks = m->class_chunks;
   v->device = m->device;
   v->st = m->st;

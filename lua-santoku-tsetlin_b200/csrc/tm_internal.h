@@ -274,9 +274,11 @@ struct MachineView {
   const uint32_t *act;
   const int32_t *lits;
   const ClassDev *cls;
-  uint32_t classes, clauses, tol, type, input_chunks, Wp, class_chunks;
+  uint32_t classes, clauses, tol, type, input_chunks, Wp, class_chunks, W;
   int device;
   cudaStream_t st;  // the machine's own stream
+  const uint8_t *act8;  // action bytes for the GEMM predict (tmb_machine_act8), or null
+  int act8_kind;        // their TM_GEMM_* encoding
 };
 
 }  // namespace tmb
@@ -286,5 +288,10 @@ struct tm_machine;
 // `who` names the caller in the error message.
 int tmb_machine_view(tm_machine *m, tmb::MachineView *v, const char *who);
 int tmb_fail(int code, const char *msg);
+// Fills v->act8 / v->act8_kind with the machine's action bytes for the GEMM
+// predict (built if stale, the machine's stream drained), or leaves them
+// null when the device has no GEMM encoding or the machine is
+// individualized.  The bytes stay valid until the automata change.
+int tmb_machine_act8(tm_machine *m, tmb::MachineView *v);
 // cudaMalloc behind the failure injection of tm_debug_fail_alloc
 cudaError_t tmb_dev_malloc(void **p, size_t n);

@@ -69,6 +69,10 @@ struct Slot {
   uint8_t *d_raw = nullptr, *d_out = nullptr, *d_jobs = nullptr;
   uint32_t *d_x = nullptr;
   int32_t *d_sums = nullptr;
+  // large requests through the GEMM: a chunk of sample bytes, the chunk's
+  // clause x sample products, the library's workspace
+  uint8_t *d_x8 = nullptr, *d_ws = nullptr;
+  void *d_gc = nullptr;
   std::vector<Request *> reqs;
   std::vector<uint64_t> out_off;  // each request's result offset in h_out
   bool busy = false;
@@ -76,6 +80,24 @@ struct Slot {
 };
 
 uint64_t round_up(uint64_t v, uint64_t a) { return (v + a - 1) / a * a; }
+
+// The GEMM path of a slot: products of at most TM_SERVE_GEMM_C bytes per
+// library call, its workspace.
+constexpr uint64_t TM_SERVE_GEMM_C = 64ull << 20;
+constexpr size_t TM_SERVE_GEMM_WS = 32u << 20;
+
+// Samples per GEMM call for a machine of M clauses (a multiple of 64).
+uint64_t gemm_chunk(uint64_t M) {
+  return std::max<uint64_t>(64, TM_SERVE_GEMM_C / (4 * M) / 64 * 64);
+}
+
+// Whether a request goes through the GEMM (as the single-machine predict
+// decides: past the small-batch sizes, at least 2^28 clause x sample x row
+// word products).
+bool gemm_request(const MachineView &v, uint64_t n) {
+  return v.act8 && n > TM_SMALL_N_MAX &&
+         (uint64_t)v.classes * v.clauses * n * v.W >= (1ull << 28);
+}
 
 }  // namespace
 
@@ -152,7 +174,9 @@ static cudaError_t launch_slot(tm_server *s, Slot &sl) {
     J.Wp = v.Wp;
     J.classes = v.classes;
     J.type = v.type;
-    if (r->n <= TM_SMALL_N_MAX) {
+    if (gemm_request(v, r->n)) {
+      // after the repack, below
+    } else if (r->n <= TM_SMALL_N_MAX) {
       for (uint32_t s0 = 0; s0 < r->n; s0 += 16) {
         SmallJob &M = mj[nsmall++];
         M = SmallJob{v.act, v.lits, v.cls, J.x, J.sums, v.clauses, v.tol, v.classes, s0,
@@ -186,6 +210,28 @@ static cudaError_t launch_slot(tm_server *s, Slot &sl) {
                         cudaMemcpyHostToDevice, sl.st);
   if (e == cudaSuccess) e = cudaMemsetAsync(sl.d_sums, 0, s_off * 4, sl.st);
   if (e == cudaSuccess) e = launch_serve_repack((const ServeJob *)sl.d_jobs, R, sl.st);
+  for (uint32_t i = 0; i < R && e == cudaSuccess; i++) {
+    const Request *r = sl.reqs[i];
+    const MachineView &v = s->mv[r->machine];
+    if (!gemm_request(v, r->n)) continue;
+    // the request's rows were repacked to sj[i].x; its sums go to sj[i].sums
+    const uint64_t M = (uint64_t)v.classes * v.clauses, K = (uint64_t)v.W * 32;
+    const uint64_t nc = gemm_chunk(M);
+    for (uint64_t s0 = 0; s0 < r->n && e == cudaSuccess; s0 += nc) {
+      const uint64_t k = std::min<uint64_t>(nc, r->n - s0);
+      e = launch_expand_bits(sj[i].x + s0 * v.Wp, k, v.Wp, v.W, 0xFFFFFFFFu, v.act8_kind,
+                             sl.d_x8, sl.st);
+      if (e != cudaSuccess) break;
+      const int g = gemm_clause_products(v.device, v.act8_kind, v.act8, sl.d_x8, sl.d_gc, M, k, K,
+                                         sl.d_ws, TM_SERVE_GEMM_WS, sl.st);
+      if (g != 0) {
+        e = cudaErrorUnknown;
+        break;
+      }
+      e = launch_gemm_votes(sl.d_gc, v.act8_kind, v.lits, v.classes, v.clauses, v.tol,
+                            (uint32_t)k, sj[i].sums + s0 * v.classes, sl.st);
+    }
+  }
   if (e == cudaSuccess)
     e = launch_predict_small_multi((const SmallJob *)(sl.d_jobs + o_mj), nsmall, small_blocks,
                                    sl.st);
@@ -266,6 +312,9 @@ static void free_server(tm_server *s) {
     if (sl.d_jobs) cudaFree(sl.d_jobs);
     if (sl.d_x) cudaFree(sl.d_x);
     if (sl.d_sums) cudaFree(sl.d_sums);
+    if (sl.d_x8) cudaFree(sl.d_x8);
+    if (sl.d_gc) cudaFree(sl.d_gc);
+    if (sl.d_ws) cudaFree(sl.d_ws);
   }
   for (auto *qq : {&s->queue, &s->squeue})
     for (Request *r : *qq) s->live.erase(r->id), delete r;
@@ -294,6 +343,11 @@ extern "C" int tm_serve_open(const tm_server_config *cfg, tm_machine *const *mac
       delete s;
       return tmb_fail(TM_ERR_ARG, "serve_open: machine on another device");
     }
+    rc = tmb_machine_act8(machines[i], &v);  // resident action bytes for large requests
+    if (rc) {
+      delete s;
+      return rc;
+    }
     s->mv.push_back(v);
   }
   // a slot holds up to max_batch_samples of the widest machine, plus the
@@ -307,7 +361,16 @@ extern "C" int tm_serve_open(const tm_server_config *cfg, tm_machine *const *mac
   }
   s->cap_jobs = round_up(P * sizeof(ServeJob), 256) + round_up(2 * P * sizeof(SmallJob), 256) +
                 P * sizeof(PredictJob);
-  const uint64_t per_slot = s->cap_in + s->cap_x + s->cap_sums + s->cap_out + s->cap_jobs;
+  // the GEMM path: sample bytes of one chunk of the widest machine, the
+  // products, the workspace
+  uint64_t cap_x8 = 0;
+  for (const MachineView &v : s->mv)
+    if (v.act8)
+      cap_x8 = std::max<uint64_t>(cap_x8, gemm_chunk((uint64_t)v.classes * v.clauses) *
+                                              (uint64_t)v.W * 32);
+  const uint64_t cap_gemm = cap_x8 ? cap_x8 + TM_SERVE_GEMM_C + TM_SERVE_GEMM_WS : 0;
+  const uint64_t per_slot =
+      s->cap_in + s->cap_x + s->cap_sums + s->cap_out + s->cap_jobs + cap_gemm;
   uint64_t nslots = s->cfg.hbm_budget_bytes ? s->cfg.hbm_budget_bytes / per_slot : s->cfg.max_inflight;
   nslots = std::min<uint64_t>(nslots, s->cfg.max_inflight);
   if (nslots == 0) {
@@ -334,9 +397,28 @@ extern "C" int tm_serve_open(const tm_server_config *cfg, tm_machine *const *mac
               tmb_dev_malloc((void **)&sl.d_jobs, s->cap_jobs) == cudaSuccess &&
               tmb_dev_malloc((void **)&sl.d_x, s->cap_x) == cudaSuccess &&
               tmb_dev_malloc((void **)&sl.d_sums, s->cap_sums) == cudaSuccess;
+    if (ok && cap_x8)
+      ok = tmb_dev_malloc((void **)&sl.d_x8, cap_x8) == cudaSuccess &&
+           tmb_dev_malloc(&sl.d_gc, TM_SERVE_GEMM_C) == cudaSuccess &&
+           tmb_dev_malloc((void **)&sl.d_ws, TM_SERVE_GEMM_WS) == cudaSuccess;
     if (!ok) {
       free_server(s);
       return tmb_fail(TM_ERR_OOM, "serve_open: device allocation failed");
+    }
+  }
+  // a machine whose shape the GEMM library cannot take serves every size
+  // with the bitwise kernels (one trial product per machine, on slot 0)
+  for (MachineView &v : s->mv) {
+    if (!v.act8) continue;
+    const uint64_t M = (uint64_t)v.classes * v.clauses;
+    Slot &s0 = s->slots[0];
+    const int g = gemm_clause_products(v.device, v.act8_kind, v.act8, s0.d_x8, s0.d_gc, M,
+                                       gemm_chunk(M), (uint64_t)v.W * 32, s0.d_ws,
+                                       TM_SERVE_GEMM_WS, s0.st);
+    if (g < 0) v.act8 = nullptr;
+    else if (g > 0 || cudaStreamSynchronize(s0.st) != cudaSuccess) {
+      free_server(s);
+      return tmb_fail(TM_ERR_CUDA, "serve_open: the GEMM library failed");
     }
   }
   s->worker = std::thread(worker_main, s);

@@ -185,3 +185,51 @@ def test_small_requests_of_many_machines_share_launches(tm):
         got = out.view(np.int64) if info["type"] == 0 else out
         assert np.array_equal(got, ms[k].predict(x, n))
     assert L.tm_serve_close(srv) == 0
+
+
+def test_large_requests_through_gemm_match_oracle(tm):
+    """Requests large enough for the 8-bit GEMM path (packed with small
+    ones in the same slots) give the oracle's bitwise predictions: a
+    classifier on 1,024-word rows and an encoder on 256-word rows, random
+    actions of clauses short enough that the votes depend on the exact
+    failed-literal counts."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from test_gpu_gemm_predict import _machine_pair
+    L = tm.lib()
+    pairs = [_machine_pair(tm, "classifier", 20, 16384, 64, 0.0005, 21),
+             _machine_pair(tm, "encoder", 24, 4096, 48, 0.004, 22)]
+    ms = [t for _, t, _ in pairs]
+    infos = [t.info() for t in ms]
+    rc, srv = _open(tm, ms, budget=1 << 31, inflight=3, batch=2048)
+    assert rc == 0, L.tm_last_error()
+    rng = np.random.default_rng(23)
+    reqs = []
+    for n in (300, 2000, 7, 1000, 40, 1500, 1, 600):
+        for k in range(2):
+            feats = infos[k]["features"]
+            b = rng.random((n, feats)) < 0.02
+            x = np.packbits(np.concatenate([b, ~b], axis=1), axis=1, bitorder="little").ravel()
+            rid = ctypes.c_uint64()
+            assert L.tm_serve_submit(srv, k, x.ctypes.data, n, ctypes.byref(rid)) == 0
+            reqs.append((k, n, x, rid.value))
+    for k, n, x, rid in reqs:
+        info = infos[k]
+        out = np.zeros(n * (8 if info["type"] == 0 else info["class_chunks"]), dtype=np.uint8)
+        assert L.tm_serve_poll(srv, rid, out.ctypes.data, out.ctypes.data, 60_000_000) == 1
+        got = out.view(np.int64) if info["type"] == 0 else out
+        want = np.asarray(pairs[k][0].predict(x, n)).ravel()
+        if info["type"] == 0:
+            assert np.array_equal(got, want), (k, n)
+        else:
+            # codes compared within the hidden bits of each sample's last byte
+            nb = info["class_chunks"]
+            mask = np.full(nb, 0xFF, dtype=np.uint8)
+            if info["classes"] % 8:
+                mask[-1] = (1 << (info["classes"] % 8)) - 1
+            assert np.array_equal(got.reshape(n, nb) & mask,
+                                  want.astype(np.uint8).reshape(n, nb) & mask), (k, n)
+    assert L.tm_serve_close(srv) == 0
+    for t in ms:
+        t.destroy()
