@@ -181,7 +181,12 @@ int tm_train_batch_search(tm_machine *const *machines, const tm_train_args *args
 
 /* machine:predict(problems, n) / (problems, dim_offsets, n): capi.c:1088-1110.
  * Classifier: out_classes[n] (int64, argmax, ties to the lowest class).
- * Encoder: out_codes[n * ceil(hidden/8)]. */
+ * Encoder: out_codes[n * ceil(hidden/8)].
+ * Up to 32 samples run a kernel that reads every clause row once; large
+ * predicts of dense machines run as an 8-bit tensor-core GEMM of action and
+ * literal bytes (exact integer accumulation: the same results), which keeps
+ * a byte copy of the actions on the device (classes x clauses x 32 row
+ * words bytes) until the automata change. */
 int tm_predict(tm_machine *m, const uint8_t *problems, const int64_t *dim_offsets, uint64_t n,
                int64_t *out_classes, uint8_t *out_codes, int32_t on_device);
 
@@ -389,11 +394,14 @@ int tm_reset_stats(tm_machine *m);
  * predict requests at any time, and packs queued requests -- for any of its
  * machines, in arrival order -- into shared device launches as launch slots
  * and its device-memory budget allow; each request completes with exactly
- * the result tm_predict gives for it alone. */
+ * the result tm_predict gives for it alone.  Large requests of dense
+ * machines run as the 8-bit GEMM tm_predict uses: the server holds each
+ * dense machine's action bytes (outside hbm_budget_bytes) while open, and
+ * the machines must not train meanwhile. */
 typedef struct tm_server tm_server;
 
 typedef struct tm_server_config {
-  uint64_t hbm_budget_bytes;   /* staging memory of the launch slots (inputs + outputs) */
+  uint64_t hbm_budget_bytes;   /* memory of the launch slots (inputs, outputs, GEMM chunks) */
   uint32_t max_inflight;       /* launch slots on the device at once */
   uint32_t max_batch_samples;  /* samples packed into one launch slot */
   int32_t device;
