@@ -366,8 +366,9 @@ extern "C" int tm_serve_open(const tm_server_config *cfg, tm_machine *const *mac
   uint64_t cap_x8 = 0;
   for (const MachineView &v : s->mv)
     if (v.act8)
-      cap_x8 = std::max<uint64_t>(cap_x8, gemm_chunk((uint64_t)v.classes * v.clauses) *
-                                              (uint64_t)v.W * 32);
+      cap_x8 = std::max<uint64_t>(
+          cap_x8, std::min<uint64_t>(gemm_chunk((uint64_t)v.classes * v.clauses), B) *
+                      (uint64_t)v.W * 32);
   const uint64_t cap_gemm = cap_x8 ? cap_x8 + TM_SERVE_GEMM_C + TM_SERVE_GEMM_WS : 0;
   const uint64_t per_slot =
       s->cap_in + s->cap_x + s->cap_sums + s->cap_out + s->cap_jobs + cap_gemm;
@@ -413,8 +414,8 @@ extern "C" int tm_serve_open(const tm_server_config *cfg, tm_machine *const *mac
     const uint64_t M = (uint64_t)v.classes * v.clauses;
     Slot &s0 = s->slots[0];
     const int g = gemm_clause_products(v.device, v.act8_kind, v.act8, s0.d_x8, s0.d_gc, M,
-                                       gemm_chunk(M), (uint64_t)v.W * 32, s0.d_ws,
-                                       TM_SERVE_GEMM_WS, s0.st);
+                                       std::min<uint64_t>(gemm_chunk(M), B),
+                                       (uint64_t)v.W * 32, s0.d_ws, TM_SERVE_GEMM_WS, s0.st);
     if (g < 0) v.act8 = nullptr;
     else if (g > 0 || cudaStreamSynchronize(s0.st) != cudaSuccess) {
       free_server(s);
