@@ -964,7 +964,7 @@ def main():
                     help="c1/c0/c2: comma-separated batch sizes; print each predict's kernel time")
     ap.add_argument("--requests", type=int, default=2000, help="serve: requests")
     ap.add_argument("--rate", type=float, default=5000.0, help="serve: arrivals per second")
-    ap.add_argument("--hbm-budget", type=int, default=2048, help="serve: staging MB")
+    ap.add_argument("--hbm-budget", type=int, default=4096, help="serve: launch-slot memory, MB")
     ap.add_argument("--sustainable-rate", type=float, default=150.0,
                     help="serve: second, sustainable arrival rate")
     args = ap.parse_args()

@@ -83,7 +83,7 @@ uint64_t round_up(uint64_t v, uint64_t a) { return (v + a - 1) / a * a; }
 
 // The GEMM path of a slot: products of at most TM_SERVE_GEMM_C bytes per
 // library call, its workspace.
-constexpr uint64_t TM_SERVE_GEMM_C = 64ull << 20;
+constexpr uint64_t TM_SERVE_GEMM_C = 256ull << 20;
 constexpr size_t TM_SERVE_GEMM_WS = 32u << 20;
 
 // Samples per GEMM call for a machine of M clauses (a multiple of 64).
