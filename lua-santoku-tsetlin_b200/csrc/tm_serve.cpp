@@ -363,13 +363,19 @@ extern "C" int tm_serve_open(const tm_server_config *cfg, tm_machine *const *mac
                 P * sizeof(PredictJob);
   // the GEMM path: sample bytes of one chunk of the widest machine, the
   // products, the workspace
-  uint64_t cap_x8 = 0;
-  for (const MachineView &v : s->mv)
-    if (v.act8)
-      cap_x8 = std::max<uint64_t>(
-          cap_x8, std::min<uint64_t>(gemm_chunk((uint64_t)v.classes * v.clauses), B) *
-                      (uint64_t)v.W * 32);
-  const uint64_t cap_gemm = cap_x8 ? cap_x8 + TM_SERVE_GEMM_C + TM_SERVE_GEMM_WS : 0;
+  // (only machines whose requests of up to max_batch_samples can reach it)
+  uint64_t cap_x8 = 0, cap_gc = 0;
+  for (MachineView &v : s->mv) {
+    if (!gemm_request(v, B)) {
+      v.act8 = nullptr;
+      continue;
+    }
+    const uint64_t M = (uint64_t)v.classes * v.clauses;
+    const uint64_t nc = std::min<uint64_t>(gemm_chunk(M), B);
+    cap_x8 = std::max<uint64_t>(cap_x8, nc * (uint64_t)v.W * 32);
+    cap_gc = std::max<uint64_t>(cap_gc, nc * M * 4);
+  }
+  const uint64_t cap_gemm = cap_x8 ? cap_x8 + cap_gc + TM_SERVE_GEMM_WS : 0;
   const uint64_t per_slot =
       s->cap_in + s->cap_x + s->cap_sums + s->cap_out + s->cap_jobs + cap_gemm;
   uint64_t nslots = s->cfg.hbm_budget_bytes ? s->cfg.hbm_budget_bytes / per_slot : s->cfg.max_inflight;
@@ -400,7 +406,7 @@ extern "C" int tm_serve_open(const tm_server_config *cfg, tm_machine *const *mac
               tmb_dev_malloc((void **)&sl.d_sums, s->cap_sums) == cudaSuccess;
     if (ok && cap_x8)
       ok = tmb_dev_malloc((void **)&sl.d_x8, cap_x8) == cudaSuccess &&
-           tmb_dev_malloc(&sl.d_gc, TM_SERVE_GEMM_C) == cudaSuccess &&
+           tmb_dev_malloc(&sl.d_gc, cap_gc) == cudaSuccess &&
            tmb_dev_malloc((void **)&sl.d_ws, TM_SERVE_GEMM_WS) == cudaSuccess;
     if (!ok) {
       free_server(s);
