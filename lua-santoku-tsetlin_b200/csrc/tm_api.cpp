@@ -1723,13 +1723,15 @@ static int predict_gemm(tm_machine *m, uint64_t n) {
     if (kind <= 0) return 1;
     int rc = ensure_act8(m, kind);
     if (rc) return rc;
-    // samples per chunk: products of at most 512 MB, in multiples of 64
+    // samples per chunk: products of at most 512 MB, in multiples of 64;
+    // each product's width rounded up to a bucket (gemm_bucket), whose
+    // columns past the chunk's samples are not read
     uint64_t nc = ((512ull << 20) / (4 * M)) / 64 * 64;
     nc = std::max<uint64_t>(nc, 64);
-    nc = std::min<uint64_t>(nc, n);
+    const uint64_t cap = gemm_bucket(std::min<uint64_t>(nc, n), nc);
     const size_t ws_bytes = 32u << 20;
-    CK(m->x8.ensure(nc * K));
-    CK(m->gemm_c.ensure(nc * M * 4));
+    CK(m->x8.ensure(cap * K));
+    CK(m->gemm_c.ensure(cap * M * 4));
     CK(m->gemm_ws.ensure(ws_bytes));
     bool retry = false;
     for (uint64_t s0 = 0; s0 < n; s0 += nc) {
@@ -1737,8 +1739,8 @@ static int predict_gemm(tm_machine *m, uint64_t n) {
       CK(launch_expand_bits(m->x.as<uint32_t>() + s0 * c0.Wp, k, c0.Wp, c0.W, 0xFFFFFFFFu, kind,
                             m->x8.as<uint8_t>(), m->st));
       const int g = gemm_clause_products(m->device, kind, m->act8.as<uint8_t>(),
-                                         m->x8.as<uint8_t>(), m->gemm_c.p, M, k, K,
-                                         m->gemm_ws.p, ws_bytes, m->st);
+                                         m->x8.as<uint8_t>(), m->gemm_c.p, M,
+                                         gemm_bucket(k, nc), K, m->gemm_ws.p, ws_bytes, m->st);
       if (g < 0 && s0 == 0) {  // no algorithm: the other encoding, then the bitwise kernels
         kind = kind == TM_GEMM_INT8 ? TM_GEMM_FP8 : -1;
         retry = true;

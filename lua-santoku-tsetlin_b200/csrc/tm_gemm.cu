@@ -17,6 +17,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 
+#include <map>
 #include <mutex>
 
 #include "tm_internal.h"
@@ -99,9 +100,35 @@ std::mutex g_lt_mu;
 cublasLtHandle_t g_lt[64];
 int g_lt_state[64];  // 0 not created, 1 ready
 
+// The library's choice per (device, encoding, M, N, K): asked once per shape
+// (products of few distinct widths are asked for: callers round N up to a
+// bucket).  found == 0 records a shape without an algorithm.
+struct AlgoKey {
+  int dev, kind;
+  uint64_t M, N, K;
+  bool operator<(const AlgoKey &o) const {
+    if (dev != o.dev) return dev < o.dev;
+    if (kind != o.kind) return kind < o.kind;
+    if (M != o.M) return M < o.M;
+    if (N != o.N) return N < o.N;
+    return K < o.K;
+  }
+};
+struct AlgoVal {
+  cublasLtMatmulAlgo_t algo;
+  int found;
+};
+std::map<AlgoKey, AlgoVal> g_algos;
+
 }  // namespace
 
 uint32_t gemm_byte_one(int kind) { return kind == TM_GEMM_FP8 ? 0x38u : 0x01u; }
+
+uint64_t gemm_bucket(uint64_t k, uint64_t cap) {
+  uint64_t b = 64;
+  while (b < k) b <<= 1;
+  return b < cap ? b : cap;
+}
 
 cudaError_t launch_expand_bits(const uint32_t *src, uint64_t rows, uint32_t stride, uint32_t W,
                                uint32_t last_mask, int kind, uint8_t *dst, cudaStream_t st) {
@@ -169,12 +196,28 @@ int gemm_clause_products(int dev, int kind, const uint8_t *A, const uint8_t *B, 
                                              &ws_bytes, sizeof ws_bytes);
   cublasLtMatmulHeuristicResult_t h{};
   int found = 0;
-  if (s == CUBLAS_STATUS_SUCCESS)
+  const AlgoKey key{dev, kind, M, N, K};
+  bool cached = false;
+  {
+    std::lock_guard<std::mutex> lk(g_lt_mu);
+    auto it = g_algos.find(key);
+    if (it != g_algos.end()) {
+      h.algo = it->second.algo;
+      found = it->second.found;
+      cached = true;
+    }
+  }
+  if (!cached && s == CUBLAS_STATUS_SUCCESS) {
     s = cublasLtMatmulAlgoGetHeuristic(lt, op, la, lb, lc, lc, pref, 1, &h, &found);
+    if (s == CUBLAS_STATUS_SUCCESS) {
+      std::lock_guard<std::mutex> lk(g_lt_mu);
+      g_algos[key] = AlgoVal{h.algo, found};
+    }
+  }
   {
     // TSETLIN_B200_GEMM_LOG=1: the library's answer for each shape on stderr
     const char *lg = getenv("TSETLIN_B200_GEMM_LOG");
-    if (lg && lg[0] == '1')
+    if (lg && lg[0] == '1' && !cached)
       fprintf(stderr, "tsetlin_b200 gemm: %s M=%llu N=%llu K=%llu status=%d algorithms=%d\n",
               fp8 ? "e4m3" : "int8", (unsigned long long)M, (unsigned long long)N,
               (unsigned long long)K, (int)s, found);

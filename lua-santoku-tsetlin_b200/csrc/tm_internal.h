@@ -135,6 +135,11 @@ cudaError_t launch_gemm_votes(const void *C, int kind, const int32_t *lits, uint
 int gemm_clause_products(int dev, int kind, const uint8_t *A, const uint8_t *B, void *C,
                          uint64_t M, uint64_t N, uint64_t K, void *ws, size_t ws_bytes,
                          cudaStream_t st);
+// The product width for k samples: the next power of two from 64, at most
+// `cap` (the chunk size).  Products are asked for in these few widths (the
+// columns past k are not read), so the library's choice and its kernels are
+// set up once per width.
+uint64_t gemm_bucket(uint64_t k, uint64_t cap);
 // The fused train kernels report through err[0] (status bits) and
 // err[2..3], a 64-bit count of active (unit, sample) steps -- the samples
 // each unit actually trained on after negative sampling.

@@ -222,8 +222,9 @@ static cudaError_t launch_slot(tm_server *s, Slot &sl) {
       e = launch_expand_bits(sj[i].x + s0 * v.Wp, k, v.Wp, v.W, 0xFFFFFFFFu, v.act8_kind,
                              sl.d_x8, sl.st);
       if (e != cudaSuccess) break;
-      const int g = gemm_clause_products(v.device, v.act8_kind, v.act8, sl.d_x8, sl.d_gc, M, k, K,
-                                         sl.d_ws, TM_SERVE_GEMM_WS, sl.st);
+      const int g = gemm_clause_products(v.device, v.act8_kind, v.act8, sl.d_x8, sl.d_gc, M,
+                                         gemm_bucket(k, std::min<uint64_t>(nc, s->cfg.max_batch_samples)),
+                                         K, sl.d_ws, TM_SERVE_GEMM_WS, sl.st);
       if (g != 0) {
         e = cudaErrorUnknown;
         break;
@@ -413,19 +414,28 @@ extern "C" int tm_serve_open(const tm_server_config *cfg, tm_machine *const *mac
       return tmb_fail(TM_ERR_OOM, "serve_open: device allocation failed");
     }
   }
-  // a machine whose shape the GEMM library cannot take serves every size
-  // with the bitwise kernels (one trial product per machine, on slot 0)
+  // every product width a machine's requests can use is run once on slot 0
+  // (the library's choice and its kernels are set up before the first
+  // request); a machine whose shape the library cannot take serves every
+  // size with the bitwise kernels
   for (MachineView &v : s->mv) {
     if (!v.act8) continue;
     const uint64_t M = (uint64_t)v.classes * v.clauses;
+    const uint64_t cap = std::min<uint64_t>(gemm_chunk(M), B);
     Slot &s0 = s->slots[0];
-    const int g = gemm_clause_products(v.device, v.act8_kind, v.act8, s0.d_x8, s0.d_gc, M,
-                                       std::min<uint64_t>(gemm_chunk(M), B),
-                                       (uint64_t)v.W * 32, s0.d_ws, TM_SERVE_GEMM_WS, s0.st);
-    if (g < 0) v.act8 = nullptr;
-    else if (g > 0 || cudaStreamSynchronize(s0.st) != cudaSuccess) {
-      free_server(s);
-      return tmb_fail(TM_ERR_CUDA, "serve_open: the GEMM library failed");
+    for (uint64_t w = 64;; w = std::min<uint64_t>(2 * w, cap)) {
+      const uint64_t N = gemm_bucket(w, cap);
+      const int g = gemm_clause_products(v.device, v.act8_kind, v.act8, s0.d_x8, s0.d_gc, M, N,
+                                         (uint64_t)v.W * 32, s0.d_ws, TM_SERVE_GEMM_WS, s0.st);
+      if (g < 0) {
+        v.act8 = nullptr;
+        break;
+      }
+      if (g > 0 || cudaStreamSynchronize(s0.st) != cudaSuccess) {
+        free_server(s);
+        return tmb_fail(TM_ERR_CUDA, "serve_open: the GEMM library failed");
+      }
+      if (N >= cap) break;
     }
   }
   s->worker = std::thread(worker_main, s);
