@@ -872,6 +872,19 @@ def serve_at(args, L, tm, machines, pools, rng, rate, requests=None):
     srv = ctypes.c_void_p()
     assert L.tm_serve_open(ctypes.byref(cfg), hs, len(machines), ctypes.byref(srv)) == 0, \
         L.tm_last_error()
+    # warm-up, untimed: a request of each size class for every machine, so
+    # that first-use costs (kernel loading, library set-up) stay out of the
+    # measured latencies, as they do for the serial form, which runs later
+    nwarm = 0
+    for k in range(len(machines)):
+        for s_ in (1, 40, 300, 4096):
+            x = np.ascontiguousarray(pools[k][:s_]).ravel()
+            rid = ctypes.c_uint64()
+            assert L.tm_serve_submit(srv, k, x.ctypes.data, s_, ctypes.byref(rid)) == 0
+            out = np.zeros(s_ * 32, dtype=np.int64)
+            assert L.tm_serve_poll(srv, rid.value, out.ctypes.data, out.ctypes.data,
+                                   60_000_000) == 1
+            nwarm += 1
     ids = [0] * nreq
     t0 = time.perf_counter()
 
@@ -888,10 +901,11 @@ def serve_at(args, L, tm, machines, pools, rng, rate, requests=None):
     th = threading.Thread(target=submit)
     th.start()
     th.join()
-    lat, acc_sizes, acc_arrive = [], [], []
+    lat, acc_sizes, acc_arrive, acc_which = [], [], [], []
     for i in range(nreq):
         if ids[i] is None:
             continue
+        acc_which.append(int(which[i]))
         out = np.zeros(int(sizes[i]) * 32, dtype=np.int64)
         assert L.tm_serve_poll(srv, ids[i], out.ctypes.data, out.ctypes.data, 60_000_000) == 1
         us = ctypes.c_double()
@@ -914,7 +928,7 @@ def serve_at(args, L, tm, machines, pools, rng, rate, requests=None):
     total = int(sizes.sum())
     out = {
         "metric": "serve p99 ms", "value": float(np.percentile(lat, 99)), "unit": "ms",
-        "n_gpus": 1, "steps": nreq, "warmup": 0, "higher_is_better": False,
+        "n_gpus": 1, "steps": nreq, "warmup": nwarm, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": {"workload": "predict-serving", "machines": len(machines),
                    "shapes": "6 plain classifiers, 5 large sparse classifiers, 5 encoders",
@@ -928,6 +942,9 @@ def serve_at(args, L, tm, machines, pools, rng, rate, requests=None):
                            "p99_ms": float(np.percentile([v for v, z in zip(lat, acc_sizes)
                                                           if z <= 256] or [0], 99))},
         "accepted": len(lat), "refused_queue_full": nreq - len(lat),
+        "slowest": [{"machine": acc_which[j], "samples": acc_sizes[j],
+                     "latency_ms": lat[j], "arrival_s": float(acc_arrive[j])}
+                    for j in np.argsort(lat)[::-1][:6]],
         "offered_samples_per_s": float(sizes.sum() / arrive[-1]),
         "samples_per_s": float(sum(acc_sizes)) / makespan,
         "serial": {"p50_ms": float(np.percentile(lat_s, 50)),
