@@ -169,6 +169,27 @@ static void invalidate_derived(tm_machine *m) {
   m->act8_valid = false;
 }
 
+// ---- large-batch predict as a GEMM ------------------------------------------
+// The 8-bit encoding the GEMM uses on each device: 0 not yet tried, a
+// TM_GEMM_* kind, or -1 when the library offers neither (the bitwise
+// kernels then serve every size).  TSETLIN_B200_GEMM=off|int8|fp8 overrides
+// the choice at the first large predict of the process.
+static std::mutex g_gemm_mu;
+static int g_gemm_kind[64];
+
+static int gemm_kind_of(int dev) {
+  std::lock_guard<std::mutex> lk(g_gemm_mu);
+  if (dev < 0 || dev >= 64) return -1;
+  if (g_gemm_kind[dev] == 0) {
+    const char *e = getenv("TSETLIN_B200_GEMM");
+    if (e && !strcmp(e, "off")) g_gemm_kind[dev] = -1;
+    else if (e && !strcmp(e, "fp8")) g_gemm_kind[dev] = TM_GEMM_FP8;
+    else g_gemm_kind[dev] = TM_GEMM_INT8;
+  }
+  return g_gemm_kind[dev];
+}
+
+
 constexpr uint64_t TM_PIN_STAGE = 256 << 10;
 
 // The input half of the machine's pinned staging buffer, ready to be
@@ -1342,6 +1363,58 @@ static int search_round(tm_machine *const *ms, const tm_train_args *args, uint32
     CK(cudaMemsetAsync(m->sums.p, 0, nt * m->classes * 4, st));
     if (sa->patience) CK(m->ckpt.ensure(std::max<uint64_t>(m->act_words, 4) * 4));
   }
+  // ---- the holdout predict of large dense machines as the 8-bit GEMM ---------
+  // Their holdout rows are expanded to bytes once; in every epoch the graph
+  // expands the trained actions and runs the products and the vote epilogue
+  // (gated by the machine's live flag, like the bitwise predict).  Each
+  // product width is tried once here, outside the capture: a machine whose
+  // shape the library cannot take keeps the bitwise predict.
+  const int gkind = gemm_kind_of(m0->device);
+  const size_t gws = 32u << 20;
+  std::vector<char> use_gemm(count, 0);
+  std::vector<uint64_t> gchunk(count, 0);
+  {
+    uint64_t cmax = 0;
+    for (uint32_t i = 0; i < count; i++) {
+      tm_machine *m = ms[i];
+      const ClassDev &c0 = m->cls[0];
+      const uint64_t M = (uint64_t)m->classes * m->clauses;
+      if (gkind <= 0 || m->individualized || nt <= TM_SMALL_N_MAX ||
+          M * nt * c0.W < (1ull << 28))
+        continue;
+      uint64_t nc = ((512ull << 20) / (4 * M)) / 64 * 64;
+      nc = std::max<uint64_t>(nc, 64);
+      gchunk[i] = nc;
+      cmax = std::max<uint64_t>(cmax, gemm_bucket(std::min<uint64_t>(nc, nt), nc) * M * 4);
+      use_gemm[i] = 1;
+    }
+    if (cmax) {
+      CK(m0->gemm_c.ensure(cmax));
+      CK(m0->gemm_ws.ensure(gws));
+    }
+    for (uint32_t i = 0; i < count; i++) {
+      if (!use_gemm[i]) continue;
+      tm_machine *m = ms[i];
+      const ClassDev &c0 = m->cls[0];
+      const uint64_t M = (uint64_t)m->classes * m->clauses, K = (uint64_t)c0.W * 32;
+      const uint64_t nc = gchunk[i];
+      CK(m->act8.ensure(M * K));
+      // rows past nt: the last product's bucket reads them (its columns
+      // there are not used)
+      CK(m->x8.ensure((nt + gemm_bucket(std::min<uint64_t>(nc, nt), nc)) * K));
+      CK(launch_expand_bits(m->x.as<uint32_t>(), nt, c0.Wp, c0.W, 0xFFFFFFFFu, gkind,
+                            m->x8.as<uint8_t>(), st));
+      for (uint64_t s0 = 0; s0 < nt && use_gemm[i]; s0 += nc) {
+        const uint64_t k = std::min<uint64_t>(nc, nt - s0);
+        const int g = gemm_clause_products(m0->device, gkind, m->act8.as<uint8_t>(),
+                                           m->x8.as<uint8_t>() + s0 * K, m0->gemm_c.p, M,
+                                           gemm_bucket(k, nc), K, m0->gemm_ws.p, gws, st);
+        if (g < 0) use_gemm[i] = 0;
+        else if (g > 0) return fail(TM_ERR_CUDA, "search: cuBLASLt matmul failed (status %d)", g);
+      }
+    }
+    CK(cudaStreamSynchronize(st));
+  }
   // ---- device tables ---------------------------------------------------------
   auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
   const size_t o_scores = al(count * sizeof(SearchState));
@@ -1364,7 +1437,7 @@ static int search_round(tm_machine *const *ms, const tm_train_args *args, uint32
   std::vector<LitsJob> lj(count), ljf(count);
   std::vector<ScoreJob> sj(count);
   std::vector<CopyJob> cj(count), rj(count);
-  uint32_t tiles = 0;
+  uint32_t tiles = 0, tiles_f = 0;  // per-epoch predict (GEMM machines apart), final pass
   for (uint32_t i = 0; i < count; i++) {
     tm_machine *m = ms[i];
     SearchState &S = hs[i];
@@ -1387,9 +1460,12 @@ static int search_round(tm_machine *const *ms, const tm_train_args *args, uint32
     P.tol = m->tol;
     P.n = (uint32_t)nt;
     P.classes = m->classes;
+    const uint32_t jt = predict_job_tiles((uint32_t)nt, m->classes, m->clauses, &P.stiles, &P.tpc);
     P.tile0 = tiles;
-    tiles += predict_job_tiles((uint32_t)nt, m->classes, m->clauses, &P.stiles, &P.tpc);
+    if (!use_gemm[i]) tiles += jt;  // a GEMM machine's job has no tiles: never picked
     pjf[i] = P;
+    pjf[i].tile0 = tiles_f;
+    tiles_f += jt;
     pjf[i].gate = &d_state[i].has_ckpt;
     lj[i] = LitsJob{m->d_act, m->d_cls, m->d_lits, &d_state[i].live, m->classes, m->clauses};
     ljf[i] = lj[i];
@@ -1524,8 +1600,32 @@ static int search_round(tm_machine *const *ms, const tm_train_args *args, uint32
     if (ce == cudaSuccess && timing) ce = cudaEventRecordWithFlags(tk1, st, cudaEventRecordExternal);
     if (ce == cudaSuccess)
       ce = launch_lits_multi((const LitsJob *)(base + o_lj), count, maxC, st);
-    if (ce == cudaSuccess)
+    if (ce == cudaSuccess && tiles)
       ce = launch_predict_multi((const PredictJob *)(base + o_pj), count, tiles, st);
+    for (uint32_t i = 0; i < count && ce == cudaSuccess; i++) {
+      if (!use_gemm[i]) continue;
+      tm_machine *m = ms[i];
+      const ClassDev &c0 = m->cls[0];
+      const uint64_t M = (uint64_t)m->classes * m->clauses, K = (uint64_t)c0.W * 32;
+      const uint64_t nc = gchunk[i];
+      ce = launch_expand_bits(m->d_act + c0.act_off, M, c0.Wp, c0.W, c0.emask, gkind,
+                              m->act8.as<uint8_t>(), st);
+      launches++;
+      for (uint64_t s0 = 0; s0 < nt && ce == cudaSuccess; s0 += nc) {
+        const uint64_t k = std::min<uint64_t>(nc, nt - s0);
+        const int g = gemm_clause_products(m0->device, gkind, m->act8.as<uint8_t>(),
+                                           m->x8.as<uint8_t>() + s0 * K, m0->gemm_c.p, M,
+                                           gemm_bucket(k, nc), K, m0->gemm_ws.p, gws, st);
+        if (g != 0) {
+          ce = cudaErrorUnknown;
+          break;
+        }
+        ce = launch_gemm_votes(m0->gemm_c.p, gkind, m->d_lits, m->classes, m->clauses, m->tol,
+                               (uint32_t)k, m->sums.as<int32_t>() + s0 * m->classes, st,
+                               &d_state[i].live);
+        launches += 2;
+      }
+    }
     if (ce == cudaSuccess)
       ce = launch_search_score((const ScoreJob *)(base + o_sj), d_state, d_scores, Es, count,
                                maxC, 0, st);
@@ -1608,7 +1708,7 @@ static int search_round(tm_machine *const *ms, const tm_train_args *args, uint32
   if (sa->patience) {
     CK(launch_copy_multi((const CopyJob *)(base + o_rj), count, st));
     CK(launch_lits_multi((const LitsJob *)(base + o_ljf), count, maxC, st));
-    CK(launch_predict_multi((const PredictJob *)(base + o_pjf), count, tiles, st));
+    CK(launch_predict_multi((const PredictJob *)(base + o_pjf), count, tiles_f, st));
     CK(launch_search_score((const ScoreJob *)(base + o_sj), d_state, d_scores, Es, count, maxC, 1,
                            st));
     m0->stats.kernel_launches += 4;
@@ -1662,27 +1762,6 @@ static int ensure_lits(tm_machine *m) {
   m->lits_valid = true;
   return TM_OK;
 }
-
-// ---- large-batch predict as a GEMM ------------------------------------------
-// The 8-bit encoding the GEMM uses on each device: 0 not yet tried, a
-// TM_GEMM_* kind, or -1 when the library offers neither (the bitwise
-// kernels then serve every size).  TSETLIN_B200_GEMM=off|int8|fp8 overrides
-// the choice at the first large predict of the process.
-static std::mutex g_gemm_mu;
-static int g_gemm_kind[64];
-
-static int gemm_kind_of(int dev) {
-  std::lock_guard<std::mutex> lk(g_gemm_mu);
-  if (dev < 0 || dev >= 64) return -1;
-  if (g_gemm_kind[dev] == 0) {
-    const char *e = getenv("TSETLIN_B200_GEMM");
-    if (e && !strcmp(e, "off")) g_gemm_kind[dev] = -1;
-    else if (e && !strcmp(e, "fp8")) g_gemm_kind[dev] = TM_GEMM_FP8;
-    else g_gemm_kind[dev] = TM_GEMM_INT8;
-  }
-  return g_gemm_kind[dev];
-}
-
 
 // Whether a predict of n samples goes through the GEMM: dense machines,
 // past the small-batch kernel's sizes, and enough bitwise work (clauses x

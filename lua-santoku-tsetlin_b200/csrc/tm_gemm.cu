@@ -64,7 +64,8 @@ __global__ void k_expand_bits(const uint32_t *__restrict__ src, uint64_t rows, u
 template <typename T>
 __global__ void k_gemm_votes(const T *__restrict__ C, const int32_t *__restrict__ lits,
                              uint32_t classes, uint32_t clauses, uint32_t tol, uint32_t N,
-                             int32_t *__restrict__ sums) {
+                             int32_t *__restrict__ sums, const uint32_t *__restrict__ gate) {
+  if (gate && *gate == 0) return;  // a search machine that stopped training keeps its sums
   const uint32_t lane = threadIdx.x & 31;
   const uint64_t M = (uint64_t)classes * clauses;
   const uint64_t items = (uint64_t)N * classes;
@@ -140,14 +141,15 @@ cudaError_t launch_expand_bits(const uint32_t *src, uint64_t rows, uint32_t stri
 
 cudaError_t launch_gemm_votes(const void *C, int kind, const int32_t *lits, uint32_t classes,
                               uint32_t clauses, uint32_t tol, uint32_t N, int32_t *sums,
-                              cudaStream_t st) {
+                              cudaStream_t st, const uint32_t *gate) {
   if (!N) return cudaSuccess;
   const int g = grid_for((uint64_t)N * classes * 32, 256);
   if (kind == TM_GEMM_FP8)
-    k_gemm_votes<float><<<g, 256, 0, st>>>((const float *)C, lits, classes, clauses, tol, N, sums);
+    k_gemm_votes<float><<<g, 256, 0, st>>>((const float *)C, lits, classes, clauses, tol, N, sums,
+                                           gate);
   else
     k_gemm_votes<int32_t><<<g, 256, 0, st>>>((const int32_t *)C, lits, classes, clauses, tol, N,
-                                             sums);
+                                             sums, gate);
   return cudaGetLastError();
 }
 

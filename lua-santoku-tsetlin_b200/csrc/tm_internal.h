@@ -129,9 +129,10 @@ constexpr int TM_GEMM_INT8 = 1;  // int8 operands, int32 accumulation
 constexpr int TM_GEMM_FP8 = 2;   // e4m3 operands, fp32 accumulation
 cudaError_t launch_expand_bits(const uint32_t *src, uint64_t rows, uint32_t stride, uint32_t W,
                                uint32_t last_mask, int kind, uint8_t *dst, cudaStream_t st);
+// gate (optional, device): the kernel writes nothing while *gate == 0
 cudaError_t launch_gemm_votes(const void *C, int kind, const int32_t *lits, uint32_t classes,
                               uint32_t clauses, uint32_t tol, uint32_t N, int32_t *sums,
-                              cudaStream_t st);
+                              cudaStream_t st, const uint32_t *gate = nullptr);
 int gemm_clause_products(int dev, int kind, const uint8_t *A, const uint8_t *B, void *C,
                          uint64_t M, uint64_t N, uint64_t K, void *ws, size_t ws_bytes,
                          cudaStream_t st);
