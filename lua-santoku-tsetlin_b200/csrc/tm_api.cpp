@@ -324,6 +324,7 @@ static int check_limits(tm_machine *m) {
 // clauses per warp, or mode 4 with one of its configurations.
 static bool variant_ok(int mode, int cpw) {
   if (mode == TM_MODE_WPT) return cpw >= 1 && cpw <= wpt_configs();
+  if (mode == TM_MODE_WARP) return cpw >= 1 && cpw <= 4;  // 4: refused by the launch plan
   return mode >= -1 && mode <= TM_MODE_WARP && (cpw == 1 || cpw == 2 || cpw == 4);
 }
 
@@ -647,8 +648,11 @@ struct TrainPlan {
 
 // Fills `p` for `mode` (and `cpw` clauses per warp) when that variant can
 // run this launch.
-// Units per CTA of the one-warp-per-unit kernel for its variant number.
-static int warp_units_per_cta(int cpw) { return cpw == 2 ? 1 : 4; }
+// The one-warp-per-unit kernel's variant number (cpw): 1 four units per CTA,
+// 2 one unit per CTA, 3 one unit per CTA in at most 96 registers; its units
+// per CTA and its launch form.
+static int warp_units_per_cta(int cpw) { return cpw == 1 ? 4 : 1; }
+static int warp_form(int cpw) { return cpw - 1; }
 
 static bool plan_mode(int mode, const TrainShape &sh, TrainPlan &p, int cpw = 1) {
   p = TrainPlan{};
@@ -664,12 +668,13 @@ static bool plan_mode(int mode, const TrainShape &sh, TrainPlan &p, int cpw = 1)
     return true;
   }
   if (mode == TM_MODE_WARP) {
-    // cpw selects the units per CTA: 1 -> four, 2 -> one (8-bit automata)
-    if (sh.Wpmax > 64 || sh.Bmax > 8 || (cpw != 1 && cpw != 2)) return false;
-    if (cpw == 2 && (sh.Bmin != 8 || sh.Bmax != 8)) return false;
+    // cpw: 1 four units per CTA; 2 one; 3 one in at most 96 registers (2
+    // and 3: 8-bit automata)
+    if (sh.Wpmax > 64 || sh.Bmax > 8 || cpw < 1 || cpw > 3) return false;
+    if (cpw != 1 && (sh.Bmin != 8 || sh.Bmax != 8)) return false;
     const int wpc = warp_units_per_cta(cpw);
     size_t wsm = 0;
-    const int occ = train_warp_occupancy(sh.Wpmax, sh.Bmin, sh.Bmax, sh.smax, wpc, &wsm);
+    const int occ = train_warp_occupancy(sh.Wpmax, sh.Bmin, sh.Bmax, sh.smax, warp_form(cpw), &wsm);
     if (occ <= 0 || (int)wsm > sh.optin) return false;
     p.grid = (int)std::min<uint64_t>((sh.units + wpc - 1) / wpc, (uint64_t)sh.sms * occ);
     return true;
@@ -745,7 +750,7 @@ static int launch_plan(const TrainPlan &p, const TrainShape &sh, const std::vect
   if (p.mode == TM_MODE_WARP)
     CK(launch_train_warp((const TrainDev *)base, (const WorkItem *)(base + off_w),
                          (uint32_t)work.size(), counter, e0, e1, sh.Wpmax, sh.Bmin, sh.Bmax,
-                         sh.smax, warp_units_per_cta(p.cpw), p.grid, st,
+                         sh.smax, warp_form(p.cpw), p.grid, st,
                          (unsigned long long *)(err + 2)));
   else if (p.mode == TM_MODE_WPT)
     CK(launch_train_wpt(p.cpw, (const TrainDev *)base, (const WorkItem *)(base + off_w),
@@ -816,7 +821,7 @@ static int autotune_plan(std::vector<TrainJob> &jobs, const std::vector<TrainDev
       }
       continue;
     }
-    for (int cpw : {1, 2, 4}) {
+    for (int cpw : {1, 2, 3, 4}) {
       TrainPlan p;
       if (plan_mode(mode, sh, p, cpw)) cand.push_back(p);
     }
@@ -1518,31 +1523,102 @@ static int search_round(tm_machine *const *ms, const tm_train_args *args, uint32
     CK(launch_perm(kv.first.first, 0, (uint32_t)kv.first.second,
                    m0->perm.as<uint32_t>() + kv.second, m0->perm_scratch.p, m0->perm_scratch.cap,
                    st, d_epoch));
-  TrainPlan plan;
-  bool tuned = false;
+  // Units of rows of at most 32 words train in a launch of their own, next
+  // to the others' (two kernels of one graph at once): a launch's shared
+  // memory slices are sized by its widest row, so narrow units in the same
+  // launch as wide ones would hold as few units per SM as the wide ones.
+  std::vector<WorkItem> work_n;
+  TrainShape sh_n = sh;
+  {
+    std::vector<WorkItem> wide;
+    for (const WorkItem &wi : work)
+      (jobs[wi.m].cls[wi.h].Wp <= 32 ? work_n : wide).push_back(wi);
+    if (!work_n.empty() && !wide.empty()) {
+      auto shape_of = [&](const std::vector<WorkItem> &w, TrainShape &out) {
+        out = sh;
+        out.Wpmax = 4;
+        out.Bmin = 32;
+        out.Bmax = 2;
+        out.smax = 0;
+        for (const WorkItem &wi : w) {
+          const ClassDev &c = jobs[wi.m].cls[wi.h];
+          const uint32_t B = jobs[wi.m].m->B;
+          out.Wpmax = std::max(out.Wpmax, c.Wp);
+          out.smax = std::max(out.smax, c.s_picks);
+          out.Bmin = std::min(out.Bmin, B);
+          out.Bmax = std::max(out.Bmax, B);
+        }
+        out.units = (uint32_t)w.size();
+      };
+      shape_of(work_n, sh_n);
+      shape_of(wide, sh);
+      work.swap(wide);
+    } else {
+      work_n.clear();
+    }
+  }
+  TrainPlan plan, plan_n;
+  bool tuned = false, tuned_n = false;
   if (!work.empty()) {
     // trial launches of the tuner also read the gates and the epoch counter
     CK(cudaStreamSynchronize(st));
     rc = choose_plan(jobs, td, work, sh, 0, m0, plan, tuned);
     if (rc) return rc;
+    if (!work_n.empty()) {
+      rc = choose_plan(jobs, td, work_n, sh_n, 0, m0, plan_n, tuned_n);
+      if (rc) return rc;
+    }
     m0->last_mode = plan.mode;
     m0->stats.train_mode = plan.mode;
     m0->stats.train_autotuned = tuned ? 1 : 0;
     m0->stats.train_cpw = plan.cpw;
-    m0->stats.train_resident = resident_units(plan);
+    m0->stats.train_resident = resident_units(plan) + (work_n.empty() ? 0 : resident_units(plan_n));
   }
   const size_t tbytes = td.size() * sizeof(TrainDev);
   const size_t off_w = (tbytes + 255) & ~(size_t)255;
-  const size_t off_c = (off_w + work.size() * sizeof(WorkItem) + 255) & ~(size_t)255;
+  const size_t off_wn = (off_w + work.size() * sizeof(WorkItem) + 255) & ~(size_t)255;
+  const size_t off_c = (off_wn + work_n.size() * sizeof(WorkItem) + 255) & ~(size_t)255;
   CK(m0->tdev.ensure(off_c + 256));
   uint8_t *tbase = m0->tdev.as<uint8_t>();
   CK(cudaMemcpyAsync(tbase, td.data(), tbytes, cudaMemcpyHostToDevice, st));
   if (!work.empty())
     CK(cudaMemcpyAsync(tbase + off_w, work.data(), work.size() * sizeof(WorkItem),
                        cudaMemcpyHostToDevice, st));
-  uint32_t *counter = (uint32_t *)(tbase + off_c);
+  if (!work_n.empty())
+    CK(cudaMemcpyAsync(tbase + off_wn, work_n.data(), work_n.size() * sizeof(WorkItem),
+                       cudaMemcpyHostToDevice, st));
+  uint32_t *counter = (uint32_t *)(tbase + off_c), *counter_n = counter + 1;
   TrainSmem lay = plan.lay;
   lay.wait_limit = m0->row_wait;
+  TrainSmem lay_n = plan_n.lay;
+  lay_n.wait_limit = m0->row_wait;
+  // the second launch's stream and the events that fork it off and join it
+  cudaStream_t st_n = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  if (!work_n.empty()) {
+    if (cudaStreamCreateWithFlags(&st_n, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming) != cudaSuccess) {
+      if (st_n) cudaStreamDestroy(st_n);
+      if (ev_fork) cudaEventDestroy(ev_fork);
+      if (ev_join) cudaEventDestroy(ev_join);
+      return fail(TM_ERR_CUDA, "search: stream creation failed");
+    }
+  }
+  // one train launch of a plan over a work list
+  auto launch_group = [&](const TrainPlan &pl, const TrainShape &shp, const TrainSmem &ly,
+                          const WorkItem *wk, uint32_t nw, uint32_t *ctr,
+                          cudaStream_t s_) -> cudaError_t {
+    if (pl.mode == TM_MODE_WARP)
+      return launch_train_warp((const TrainDev *)tbase, wk, nw, ctr, 0, 1, shp.Wpmax, shp.Bmin,
+                               shp.Bmax, shp.smax, warp_form(pl.cpw), pl.grid, s_,
+                               (unsigned long long *)(d_err + 2));
+    if (pl.mode == TM_MODE_WPT)
+      return launch_train_wpt(pl.cpw, (const TrainDev *)tbase, wk, nw, ctr, 0, 1, shp.Wpmax,
+                              shp.smax, m0->row_wait, pl.grid, d_err, s_);
+    return launch_train((const TrainDev *)tbase, wk, nw, ctr, 0, 1, ly, pl.mode, shp.Bmin,
+                        shp.Bmax, pl.cpw, pl.grid, d_err, s_);
+  };
   // ---- pinned mirror of the states, events around the train kernel -----------
   SearchState *h_state = nullptr;
   CK(cudaHostAlloc((void **)&h_state, count * sizeof(SearchState) + 64, cudaHostAllocDefault));
@@ -1551,6 +1627,9 @@ static int search_round(tm_machine *const *ms, const tm_train_args *args, uint32
   cudaEvent_t tk0 = nullptr, tk1 = nullptr;
   if (timing && (cudaEventCreate(&tk0) != cudaSuccess || cudaEventCreate(&tk1) != cudaSuccess)) {
     cudaFreeHost(h_state);
+    if (st_n) cudaStreamDestroy(st_n);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
     return fail(TM_ERR_CUDA, "search: event creation failed");
   }
   cudaGraph_t graph = nullptr;
@@ -1565,6 +1644,11 @@ static int search_round(tm_machine *const *ms, const tm_train_args *args, uint32
     tk0 = tk1 = nullptr;
     if (h_state) cudaFreeHost(h_state);
     h_state = nullptr;
+    if (st_n) cudaStreamDestroy(st_n);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    st_n = nullptr;
+    ev_fork = ev_join = nullptr;
   };
   // ---- capture one epoch ------------------------------------------------------
   uint64_t launches = 0;
@@ -1577,26 +1661,26 @@ static int search_round(tm_machine *const *ms, const tm_train_args *args, uint32
                        m0->perm_scratch.cap, st, d_epoch);
       launches += 1 + kSortKernels;
     }
-    if (ce == cudaSuccess) ce = cudaMemsetAsync(counter, 0, 4, st);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(counter, 0, 8, st);  // both work counters
     // external event records: real events inside the graph, so that the
-    // train kernel's time can be read after each replay
+    // train kernels' time can be read after each replay
     if (ce == cudaSuccess && timing) ce = cudaEventRecordWithFlags(tk0, st, cudaEventRecordExternal);
-    if (ce == cudaSuccess && !work.empty()) {
-      if (plan.mode == TM_MODE_WARP)
-        ce = launch_train_warp((const TrainDev *)tbase, (const WorkItem *)(tbase + off_w),
-                               (uint32_t)work.size(), counter, 0, 1, sh.Wpmax, sh.Bmin, sh.Bmax,
-                               sh.smax, warp_units_per_cta(plan.cpw), plan.grid, st,
-                               (unsigned long long *)(d_err + 2));
-      else if (plan.mode == TM_MODE_WPT)
-        ce = launch_train_wpt(plan.cpw, (const TrainDev *)tbase, (const WorkItem *)(tbase + off_w),
-                              (uint32_t)work.size(), counter, 0, 1, sh.Wpmax, sh.smax,
-                              m0->row_wait, plan.grid, d_err, st);
-      else
-        ce = launch_train((const TrainDev *)tbase, (const WorkItem *)(tbase + off_w),
-                          (uint32_t)work.size(), counter, 0, 1, lay, plan.mode, sh.Bmin, sh.Bmax,
-                          plan.cpw, plan.grid, d_err, st);
+    if (ce == cudaSuccess && !work_n.empty()) {
+      // the narrow rows' launch on a second stream of the capture
+      ce = cudaEventRecord(ev_fork, st);
+      if (ce == cudaSuccess) ce = cudaStreamWaitEvent(st_n, ev_fork, 0);
+      if (ce == cudaSuccess)
+        ce = launch_group(plan_n, sh_n, lay_n, (const WorkItem *)(tbase + off_wn),
+                          (uint32_t)work_n.size(), counter_n, st_n);
+      if (ce == cudaSuccess) ce = cudaEventRecord(ev_join, st_n);
       launches++;
     }
+    if (ce == cudaSuccess && !work.empty()) {
+      ce = launch_group(plan, sh, lay, (const WorkItem *)(tbase + off_w), (uint32_t)work.size(),
+                        counter, st);
+      launches++;
+    }
+    if (ce == cudaSuccess && !work_n.empty()) ce = cudaStreamWaitEvent(st, ev_join, 0);
     if (ce == cudaSuccess && timing) ce = cudaEventRecordWithFlags(tk1, st, cudaEventRecordExternal);
     if (ce == cudaSuccess)
       ce = launch_lits_multi((const LitsJob *)(base + o_lj), count, maxC, st);
