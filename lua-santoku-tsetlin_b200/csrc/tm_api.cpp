@@ -324,7 +324,6 @@ static int check_limits(tm_machine *m) {
 // clauses per warp, or mode 4 with one of its configurations.
 static bool variant_ok(int mode, int cpw) {
   if (mode == TM_MODE_WPT) return cpw >= 1 && cpw <= wpt_configs();
-  if (mode == TM_MODE_WARP) return cpw >= 1 && cpw <= 4;  // 4: refused by the launch plan
   return mode >= -1 && mode <= TM_MODE_WARP && (cpw == 1 || cpw == 2 || cpw == 4);
 }
 
@@ -648,11 +647,9 @@ struct TrainPlan {
 
 // Fills `p` for `mode` (and `cpw` clauses per warp) when that variant can
 // run this launch.
-// The one-warp-per-unit kernel's variant number (cpw): 1 four units per CTA,
-// 2 one unit per CTA, 3 one unit per CTA in at most 96 registers; its units
-// per CTA and its launch form.
-static int warp_units_per_cta(int cpw) { return cpw == 1 ? 4 : 1; }
-static int warp_form(int cpw) { return cpw - 1; }
+// Units per CTA of the one-warp-per-unit kernel for its variant number
+// (cpw): 1 four units per CTA, 2 one unit per CTA.
+static int warp_units_per_cta(int cpw) { return cpw == 2 ? 1 : 4; }
 
 static bool plan_mode(int mode, const TrainShape &sh, TrainPlan &p, int cpw = 1) {
   p = TrainPlan{};
@@ -668,13 +665,12 @@ static bool plan_mode(int mode, const TrainShape &sh, TrainPlan &p, int cpw = 1)
     return true;
   }
   if (mode == TM_MODE_WARP) {
-    // cpw: 1 four units per CTA; 2 one; 3 one in at most 96 registers (2
-    // and 3: 8-bit automata)
-    if (sh.Wpmax > 64 || sh.Bmax > 8 || cpw < 1 || cpw > 3) return false;
-    if (cpw != 1 && (sh.Bmin != 8 || sh.Bmax != 8)) return false;
+    // cpw selects the units per CTA: 1 -> four, 2 -> one (8-bit automata)
+    if (sh.Wpmax > 64 || sh.Bmax > 8 || (cpw != 1 && cpw != 2)) return false;
+    if (cpw == 2 && (sh.Bmin != 8 || sh.Bmax != 8)) return false;
     const int wpc = warp_units_per_cta(cpw);
     size_t wsm = 0;
-    const int occ = train_warp_occupancy(sh.Wpmax, sh.Bmin, sh.Bmax, sh.smax, warp_form(cpw), &wsm);
+    const int occ = train_warp_occupancy(sh.Wpmax, sh.Bmin, sh.Bmax, sh.smax, wpc, &wsm);
     if (occ <= 0 || (int)wsm > sh.optin) return false;
     p.grid = (int)std::min<uint64_t>((sh.units + wpc - 1) / wpc, (uint64_t)sh.sms * occ);
     return true;
@@ -750,7 +746,7 @@ static int launch_plan(const TrainPlan &p, const TrainShape &sh, const std::vect
   if (p.mode == TM_MODE_WARP)
     CK(launch_train_warp((const TrainDev *)base, (const WorkItem *)(base + off_w),
                          (uint32_t)work.size(), counter, e0, e1, sh.Wpmax, sh.Bmin, sh.Bmax,
-                         sh.smax, warp_form(p.cpw), p.grid, st,
+                         sh.smax, warp_units_per_cta(p.cpw), p.grid, st,
                          (unsigned long long *)(err + 2)));
   else if (p.mode == TM_MODE_WPT)
     CK(launch_train_wpt(p.cpw, (const TrainDev *)base, (const WorkItem *)(base + off_w),
@@ -821,7 +817,7 @@ static int autotune_plan(std::vector<TrainJob> &jobs, const std::vector<TrainDev
       }
       continue;
     }
-    for (int cpw : {1, 2, 3, 4}) {
+    for (int cpw : {1, 2, 4}) {
       TrainPlan p;
       if (plan_mode(mode, sh, p, cpw)) cand.push_back(p);
     }
@@ -1611,7 +1607,7 @@ static int search_round(tm_machine *const *ms, const tm_train_args *args, uint32
                           cudaStream_t s_) -> cudaError_t {
     if (pl.mode == TM_MODE_WARP)
       return launch_train_warp((const TrainDev *)tbase, wk, nw, ctr, 0, 1, shp.Wpmax, shp.Bmin,
-                               shp.Bmax, shp.smax, warp_form(pl.cpw), pl.grid, s_,
+                               shp.Bmax, shp.smax, warp_units_per_cta(pl.cpw), pl.grid, s_,
                                (unsigned long long *)(d_err + 2));
     if (pl.mode == TM_MODE_WPT)
       return launch_train_wpt(pl.cpw, (const TrainDev *)tbase, wk, nw, ctr, 0, 1, shp.Wpmax,

@@ -115,15 +115,14 @@ cudaError_t launch_train(const TrainDev *machines, const WorkItem *work, uint32_
 int train_occupancy(const TrainSmem &lay, int mode, uint32_t Bmin, uint32_t Bmax, int cpw);
 // threads per CTA of a train-kernel variant (cpw: clauses per warp)
 int train_threads(int mode, int cpw);
-// k_train_warp: one warp per unit for rows of at most 64 words and B <= 8;
-// form 0: four units per CTA, 1: one unit per CTA, 2: one unit per CTA in at
-// most 96 registers (forms 1 and 2: 8-bit automata)
+// k_train_warp: one warp per unit for rows of at most 64 words and B <= 8,
+// wpc (4 or 1) units per CTA
 constexpr int TM_MODE_WARP = 3;
-int train_warp_occupancy(uint32_t Wpmax, uint32_t Bmin, uint32_t Bmax, uint32_t smax, int form,
+int train_warp_occupancy(uint32_t Wpmax, uint32_t Bmin, uint32_t Bmax, uint32_t smax, int wpc,
                          size_t *smem_bytes);
 cudaError_t launch_train_warp(const TrainDev *machines, const WorkItem *work, uint32_t nwork,
                               uint32_t *counter, uint32_t e_begin, uint32_t e_end, uint32_t Wpmax,
-                              uint32_t Bmin, uint32_t Bmax, uint32_t smax, int form, int grid,
+                              uint32_t Bmin, uint32_t Bmax, uint32_t smax, int wpc, int grid,
                               cudaStream_t st, unsigned long long *pairs);
 // Large-batch predict as an 8-bit GEMM (tm_gemm.cu)
 constexpr int TM_GEMM_INT8 = 1;  // int8 operands, int32 accumulation

@@ -662,11 +662,12 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
 // warps (units) share a CTA: 4, or 1 so that the SM's shared memory is
 // divided among units without rounding to CTAs of four.
 // ---------------------------------------------------------------------------
-template <int BM, bool EXACT>
-__device__ __forceinline__ void train_warp_body(
-    const TrainDev *__restrict__ machines, const WorkItem *__restrict__ work, uint32_t nwork,
-    uint32_t *__restrict__ counter, uint32_t e_begin, uint32_t e_end, uint32_t slice_words,
-    uint32_t ib_words, uint32_t ovf_cap, uint32_t stride, unsigned long long *__restrict__ pairs) {
+template <int BM, bool EXACT, int WPC>
+__global__ void __launch_bounds__(WPC * 32)
+    k_train_warp(const TrainDev *__restrict__ machines, const WorkItem *__restrict__ work,
+                 uint32_t nwork, uint32_t *__restrict__ counter, uint32_t e_begin, uint32_t e_end,
+                 uint32_t slice_words, uint32_t ib_words, uint32_t ovf_cap, uint32_t stride,
+                 unsigned long long *__restrict__ pairs) {
   extern __shared__ __align__(128) uint8_t smem[];
   const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   // stride: words per warp, a multiple of 32 (16-byte alignment of every slice)
@@ -895,82 +896,64 @@ __device__ __forceinline__ void train_warp_body(
   }
 }
 
-#define TM_TRAIN_WARP_PARAMS                                                                  \
-  const TrainDev *__restrict__ machines, const WorkItem *__restrict__ work, uint32_t nwork,     \
-      uint32_t *__restrict__ counter, uint32_t e_begin, uint32_t e_end, uint32_t slice_words,   \
-      uint32_t ib_words, uint32_t ovf_cap, uint32_t stride, unsigned long long *__restrict__ pairs
-#define TM_TRAIN_WARP_ARGS \
-  machines, work, nwork, counter, e_begin, e_end, slice_words, ib_words, ovf_cap, stride, pairs
-
-// WPC units (warps) per CTA: 4, or 1 so that the SM's shared memory is
-// divided among units without rounding to CTAs of four.
-template <int BM, bool EXACT, int WPC>
-__global__ void __launch_bounds__(WPC * 32) k_train_warp(TM_TRAIN_WARP_PARAMS) {
-  train_warp_body<BM, EXACT>(TM_TRAIN_WARP_ARGS);
-}
-
-// One unit per CTA in at most 96 registers (five warps per scheduler, 20
-// units per SM) for rows narrow enough that shared memory holds that many.
-template <int BM, bool EXACT>
-__global__ void __launch_bounds__(32, 20) k_train_warp_r96(TM_TRAIN_WARP_PARAMS) {
-  train_warp_body<BM, EXACT>(TM_TRAIN_WARP_ARGS);
-}
-
 // shared memory per warp of k_train_warp, in words (a multiple of 32)
 static uint32_t warp_slice_words(uint32_t Wpmax, uint32_t Bmax, uint32_t ib_words,
                                  uint32_t ovf_cap) {
   return (8 * Bmax * Wpmax + 2 * ib_words + ovf_cap + 32 + 31) / 32 * 32;
 }
 
-template <typename K>
-static int occ_of_kernel(K k, int threads, size_t bytes) {
-  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+template <int WPC>
+static int warp_occ(bool exact, size_t bytes) {
+  cudaFuncSetAttribute(k_train_warp<7, false, WPC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)bytes);
+  cudaFuncSetAttribute(k_train_warp<7, true, WPC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)bytes);
   int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, threads, bytes) != cudaSuccess) {
-    cudaGetLastError();
-    return 0;
-  }
+  if (exact)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_train_warp<7, true, WPC>, WPC * 32, bytes);
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_train_warp<7, false, WPC>, WPC * 32, bytes);
   return nb;
 }
 
-// form 0: four units per CTA; 1: one unit per CTA; 2: one unit per CTA in
-// at most 96 registers (forms 1 and 2: 8-bit automata only)
-static int warp_form_occ(int form, bool exact, size_t bytes) {
-  if (form == 0)
-    return exact ? occ_of_kernel(k_train_warp<7, true, 4>, 128, bytes)
-                 : occ_of_kernel(k_train_warp<7, false, 4>, 128, bytes);
-  if (!exact) return 0;
-  return form == 1 ? occ_of_kernel(k_train_warp<7, true, 1>, 32, bytes)
-                   : occ_of_kernel(k_train_warp_r96<7, true>, 32, bytes);
-}
-
-int train_warp_occupancy(uint32_t Wpmax, uint32_t Bmin, uint32_t Bmax, uint32_t smax, int form,
+int train_warp_occupancy(uint32_t Wpmax, uint32_t Bmin, uint32_t Bmax, uint32_t smax, int wpc,
                          size_t *smem_bytes) {
   const uint32_t ovf_cap = smax / 4 > 0 ? smax / 4 : 1;
-  const size_t bytes = (size_t)(form == 0 ? 4 : 1) * warp_slice_words(Wpmax, Bmax, Wpmax, ovf_cap) * 4;
+  const size_t bytes = (size_t)wpc * warp_slice_words(Wpmax, Bmax, Wpmax, ovf_cap) * 4;
   *smem_bytes = bytes;
-  return warp_form_occ(form, Bmin == 8 && Bmax == 8, bytes);
+  const bool exact = Bmin == 8 && Bmax == 8;
+  return wpc == 1 ? warp_occ<1>(exact, bytes) : warp_occ<4>(exact, bytes);
+}
+
+template <int WPC>
+static void warp_launch(bool exact, int grid, size_t bytes, cudaStream_t st,
+                        const TrainDev *machines, const WorkItem *work, uint32_t nwork,
+                        uint32_t *counter, uint32_t e_begin, uint32_t e_end, uint32_t slice,
+                        uint32_t Wpmax, uint32_t ovf_cap, uint32_t stride,
+                        unsigned long long *pairs) {
+  if (exact)
+    k_train_warp<7, true, WPC><<<grid, WPC * 32, bytes, st>>>(
+        machines, work, nwork, counter, e_begin, e_end, slice, Wpmax, ovf_cap, stride, pairs);
+  else
+    k_train_warp<7, false, WPC><<<grid, WPC * 32, bytes, st>>>(
+        machines, work, nwork, counter, e_begin, e_end, slice, Wpmax, ovf_cap, stride, pairs);
 }
 
 cudaError_t launch_train_warp(const TrainDev *machines, const WorkItem *work, uint32_t nwork,
                               uint32_t *counter, uint32_t e_begin, uint32_t e_end, uint32_t Wpmax,
-                              uint32_t Bmin, uint32_t Bmax, uint32_t smax, int form, int grid,
+                              uint32_t Bmin, uint32_t Bmax, uint32_t smax, int wpc, int grid,
                               cudaStream_t st, unsigned long long *pairs) {
   const uint32_t ovf_cap = smax / 4 > 0 ? smax / 4 : 1;
-  const uint32_t slice_words = 8 * Bmax * Wpmax;
+  const uint32_t slice = 8 * Bmax * Wpmax;
   const uint32_t stride = warp_slice_words(Wpmax, Bmax, Wpmax, ovf_cap);
-  const uint32_t ib_words = Wpmax;
-  const size_t bytes = (size_t)(form == 0 ? 4 : 1) * stride * 4;
+  const size_t bytes = (size_t)wpc * stride * 4;
   const bool exact = Bmin == 8 && Bmax == 8;
-  if (form != 0 && !exact) return cudaErrorInvalidValue;
-  if (form == 0 && exact)
-    k_train_warp<7, true, 4><<<grid, 128, bytes, st>>>(TM_TRAIN_WARP_ARGS);
-  else if (form == 0)
-    k_train_warp<7, false, 4><<<grid, 128, bytes, st>>>(TM_TRAIN_WARP_ARGS);
-  else if (form == 1)
-    k_train_warp<7, true, 1><<<grid, 32, bytes, st>>>(TM_TRAIN_WARP_ARGS);
+  if (wpc == 1)
+    warp_launch<1>(exact, grid, bytes, st, machines, work, nwork, counter, e_begin, e_end, slice,
+                   Wpmax, ovf_cap, stride, pairs);
   else
-    k_train_warp_r96<7, true><<<grid, 32, bytes, st>>>(TM_TRAIN_WARP_ARGS);
+    warp_launch<4>(exact, grid, bytes, st, machines, work, nwork, counter, e_begin, e_end, slice,
+                   Wpmax, ovf_cap, stride, pairs);
   return cudaGetLastError();
 }
 

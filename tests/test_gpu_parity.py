@@ -448,7 +448,7 @@ def test_every_train_variant_matches_oracle(tm, features):
     want = (m.actions(), m.state())
     variants = [(0, 1), (0, 2), (0, 4), (1, 1), (1, 2), (1, 4), (2, 1)]
     if features <= 1024:
-        variants += [(3, 1), (3, 2), (3, 3)]
+        variants += [(3, 1), (3, 2)]
     # the word-per-thread kernel's configurations that hold these rows
     # (4500 features: 282 words -> 512 threads x 2 words; 784: 52 words)
     wp = ((2 * features + 31) // 32 + 3) // 4 * 4
