@@ -1563,6 +1563,12 @@ static int search_round(tm_machine *const *ms, const tm_train_args *args, uint32
     if (!work_n.empty()) {
       rc = choose_plan(jobs, td, work_n, sh_n, 0, m0, plan_n, tuned_n);
       if (rc) return rc;
+      // planning sets each kernel's dynamic shared-memory limit; when both
+      // launches use one kernel it must end at the wide rows' size
+      TrainPlan again;
+      if (!plan_mode(plan_n.mode, sh_n, again, plan_n.cpw) ||
+          !plan_mode(plan.mode, sh, again, plan.cpw))
+        return fail(TM_ERR_STATE, "search: a train variant no longer fits its launch");
     }
     m0->last_mode = plan.mode;
     m0->stats.train_mode = plan.mode;
