@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <map>
+#include <tuple>
 #include <atomic>
 #include <mutex>
 #include <string>
@@ -153,6 +154,11 @@ struct tm_machine {
   DevBuf act8, x8, gemm_c, gemm_ws;
   bool act8_valid = false;
   int act8_kind = 0;
+  // (owner of a search round) the GEMM predict's action-byte scratch, shared
+  // by the round's machines one after another, and the holdout bytes of
+  // each distinct holdout row layout
+  DevBuf search_act8;
+  std::vector<DevBuf> search_x8;
   // pinned staging of small host requests (TM_PIN_STAGE bytes each way):
   // inputs go host -> pin -> device, outputs device -> pin -> host, so that
   // a one-sample predict makes no pageable (synchronously staged) copy.
@@ -433,8 +439,10 @@ extern "C" void tm_destroy(tm_machine *m) {
   free_device(m);
   for (DevBuf *b : {&m->x, &m->tx, &m->raw, &m->labels, &m->codes, &m->perm, &m->perm_scratch, &m->sums,
                     &m->outc, &m->work, &m->tdev, &m->cls_job, &m->errf, &m->ckpt, &m->search,
-                    &m->search_truth, &m->act8, &m->x8, &m->gemm_c, &m->gemm_ws})
+                    &m->search_truth, &m->act8, &m->x8, &m->gemm_c, &m->gemm_ws,
+                    &m->search_act8})
     b->release();
+  for (DevBuf &b : m->search_x8) b.release();
   if (m->ev0) cudaEventDestroy(m->ev0);
   if (m->ev1) cudaEventDestroy(m->ev1);
   if (m->pin_ev) cudaEventDestroy(m->pin_ev);
@@ -1374,6 +1382,7 @@ static int search_round(tm_machine *const *ms, const tm_train_args *args, uint32
   const size_t gws = 32u << 20;
   std::vector<char> use_gemm(count, 0);
   std::vector<uint64_t> gchunk(count, 0);
+  std::vector<uint8_t *> gx8(count, nullptr);
   {
     uint64_t cmax = 0;
     for (uint32_t i = 0; i < count; i++) {
@@ -1389,27 +1398,55 @@ static int search_round(tm_machine *const *ms, const tm_train_args *args, uint32
       cmax = std::max<uint64_t>(cmax, gemm_bucket(std::min<uint64_t>(nc, nt), nc) * M * 4);
       use_gemm[i] = 1;
     }
+    uint64_t amax = 0;
+    for (uint32_t i = 0; i < count; i++)
+      if (use_gemm[i])
+        amax = std::max<uint64_t>(amax, (uint64_t)ms[i]->classes * ms[i]->clauses *
+                                            ms[i]->cls[0].W * 32);
     if (cmax) {
       CK(m0->gemm_c.ensure(cmax));
       CK(m0->gemm_ws.ensure(gws));
+      CK(m0->search_act8.ensure(amax));
+    }
+    // one byte copy of the holdout per distinct row layout (the machines'
+    // staged rows of one source and row width are the same)
+    std::map<std::tuple<const void *, uint32_t, uint32_t>, size_t> x8_of;
+    for (uint32_t i = 0; i < count; i++) {
+      if (!use_gemm[i]) continue;
+      tm_machine *m = ms[i];
+      const ClassDev &c0 = m->cls[0];
+      const uint64_t K = (uint64_t)c0.W * 32;
+      const void *src = sa->test_each && sa->test_each[i] ? (const void *)sa->test_each[i]
+                                                          : (const void *)sa->test_problems;
+      const auto key = std::make_tuple(src, c0.Wp, c0.W);
+      if (x8_of.count(key)) continue;
+      const size_t at = x8_of.size();
+      x8_of[key] = at;
+      if (m0->search_x8.size() <= at) m0->search_x8.resize(at + 1);
+      // rows past nt: the last product's bucket reads them (its columns
+      // there are not used); sized for the largest chunk of any machine
+      uint64_t pad = 0;
+      for (uint32_t j = 0; j < count; j++)
+        if (use_gemm[j])
+          pad = std::max<uint64_t>(pad, gemm_bucket(std::min<uint64_t>(gchunk[j], nt), gchunk[j]));
+      CK(m0->search_x8[at].ensure((nt + pad) * K));
+      CK(launch_expand_bits(m->x.as<uint32_t>(), nt, c0.Wp, c0.W, 0xFFFFFFFFu, gkind,
+                            m0->search_x8[at].as<uint8_t>(), st));
     }
     for (uint32_t i = 0; i < count; i++) {
       if (!use_gemm[i]) continue;
       tm_machine *m = ms[i];
       const ClassDev &c0 = m->cls[0];
+      const void *src = sa->test_each && sa->test_each[i] ? (const void *)sa->test_each[i]
+                                                          : (const void *)sa->test_problems;
+      gx8[i] = m0->search_x8[x8_of[std::make_tuple(src, c0.Wp, c0.W)]].as<uint8_t>();
       const uint64_t M = (uint64_t)m->classes * m->clauses, K = (uint64_t)c0.W * 32;
       const uint64_t nc = gchunk[i];
-      CK(m->act8.ensure(M * K));
-      // rows past nt: the last product's bucket reads them (its columns
-      // there are not used)
-      CK(m->x8.ensure((nt + gemm_bucket(std::min<uint64_t>(nc, nt), nc)) * K));
-      CK(launch_expand_bits(m->x.as<uint32_t>(), nt, c0.Wp, c0.W, 0xFFFFFFFFu, gkind,
-                            m->x8.as<uint8_t>(), st));
       for (uint64_t s0 = 0; s0 < nt && use_gemm[i]; s0 += nc) {
         const uint64_t k = std::min<uint64_t>(nc, nt - s0);
-        const int g = gemm_clause_products(m0->device, gkind, m->act8.as<uint8_t>(),
-                                           m->x8.as<uint8_t>() + s0 * K, m0->gemm_c.p, M,
-                                           gemm_bucket(k, nc), K, m0->gemm_ws.p, gws, st);
+        const int g = gemm_clause_products(m0->device, gkind, m0->search_act8.as<uint8_t>(),
+                                           gx8[i] + s0 * K, m0->gemm_c.p, M, gemm_bucket(k, nc),
+                                           K, m0->gemm_ws.p, gws, st);
         if (g < 0) use_gemm[i] = 0;
         else if (g > 0) return fail(TM_ERR_CUDA, "search: cuBLASLt matmul failed (status %d)", g);
       }
@@ -1695,12 +1732,12 @@ static int search_round(tm_machine *const *ms, const tm_train_args *args, uint32
       const uint64_t M = (uint64_t)m->classes * m->clauses, K = (uint64_t)c0.W * 32;
       const uint64_t nc = gchunk[i];
       ce = launch_expand_bits(m->d_act + c0.act_off, M, c0.Wp, c0.W, c0.emask, gkind,
-                              m->act8.as<uint8_t>(), st);
+                              m0->search_act8.as<uint8_t>(), st);
       launches++;
       for (uint64_t s0 = 0; s0 < nt && ce == cudaSuccess; s0 += nc) {
         const uint64_t k = std::min<uint64_t>(nc, nt - s0);
-        const int g = gemm_clause_products(m0->device, gkind, m->act8.as<uint8_t>(),
-                                           m->x8.as<uint8_t>() + s0 * K, m0->gemm_c.p, M,
+        const int g = gemm_clause_products(m0->device, gkind, m0->search_act8.as<uint8_t>(),
+                                           gx8[i] + s0 * K, m0->gemm_c.p, M,
                                            gemm_bucket(k, nc), K, m0->gemm_ws.p, gws, st);
         if (g != 0) {
           ce = cudaErrorUnknown;
