@@ -1746,7 +1746,7 @@ static int search_round(tm_machine *const *ms, const tm_train_args *args, uint32
         ce = launch_gemm_votes(m0->gemm_c.p, gkind, m->d_lits, m->classes, m->clauses, m->tol,
                                (uint32_t)k, m->sums.as<int32_t>() + s0 * m->classes, st,
                                &d_state[i].live);
-        launches += 2;
+        launches++;  // the epilogue (the GEMM is the library's)
       }
     }
     if (ce == cudaSuccess)
@@ -1951,7 +1951,7 @@ static int predict_gemm(tm_machine *m, uint64_t n) {
       if (g != 0) return fail(TM_ERR_CUDA, "predict: cuBLASLt matmul failed (status %d)", g);
       CK(launch_gemm_votes(m->gemm_c.p, kind, m->d_lits, m->classes, m->clauses, m->tol,
                            (uint32_t)k, m->sums.as<int32_t>() + s0 * m->classes, m->st));
-      note_launch(m, 3);
+      note_launch(m, 2);  // the expansion and the epilogue (the GEMM is the library's)
     }
     if (!retry) return TM_OK;
   }
