@@ -337,9 +337,14 @@ def run_reference(args, w):
         vals.append(cpu_step(w, d, threads))
     v = float(np.median([r["value"] for r in vals]))
     step_s = float(np.median([r["step_s"] for r in vals]))
+    # a step is the bounded sample: ms_per_step is its measured time (so
+    # steps x ms_per_step is the arm's own wall time); the full workload's
+    # equivalent step, from which `value` is computed, is reported beside it
+    meas = float(sum(r["measured_s"] for r in vals))
     out = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws,
-        "steps": len(vals), "warmup": 0, "ms_per_step": step_s * 1e3, "higher_is_better": True,
+        "steps": len(vals), "warmup": 0, "ms_per_step": meas / len(vals) * 1e3,
+        "scaled_ms_per_step": step_s * 1e3, "higher_is_better": True,
         "scaling": "strong", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": config_of(w, ws),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": vals[0]["cores"],
@@ -809,10 +814,14 @@ def run_search_reference(args):
             break
     v = float(np.median([r["value"] for r in vals]))
     step_s = float(np.median([r["step_s"] for r in vals]))
+    meas = float(sum(r["measured_s"] for r in vals))
     out = {
         "impl": "reference", "metric": METRIC + " (batched vs plain, equal accuracy)",
         "value": v, "unit": UNIT, "n_gpus": ws, "steps": len(vals), "warmup": 0,
-        "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "strong",
+        # the bounded sample's measured time per step; the full epoch's
+        # equivalent (from which `value` is computed) beside it
+        "ms_per_step": meas / len(vals) * 1e3, "scaled_ms_per_step": step_s * 1e3,
+        "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": search_config(ws, allp, SEARCH["n_train"]),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": vals[0]["cores"],
