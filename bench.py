@@ -375,7 +375,8 @@ def run_ours(args, w):
     torch.cuda.set_device(dev)
     d = make_data(w, 0)
     n, nt = w["n_train"], w["n_test"]
-    # class-sharded: every rank predicts its share of the test set
+    # one machine trained class-sharded; every rank (holding the whole
+    # trained machine after the exchange) predicts its share of the test set
     lo_s, hi_s = multi.class_range(nt, ws, rank)
     lab_key = "y" if w["kind"] == "classifier" else "codes"
     # device-resident inputs (value) and pinned host inputs (e2e)
