@@ -359,9 +359,11 @@ typedef struct tm_stats {
  * 1 (default, or TSETLIN_B200_AUTOTUNE at create): the first train call of
  * a launch shape times every feasible variant on a short trial (up to 2,048
  * samples of epoch 0 on up to 32 units per SM taken evenly from the launch's
- * work list), then the three fastest on a longer one (up to 8,192 samples,
- * 64 units per SM) -- every trial on automata reset to the initial state,
- * which are reset again afterwards -- and caches the fastest for
+ * work list, from the initial automata), then the three fastest on a longer
+ * one (8,192 samples, 64 units per SM: positions 8,192-16,383 of epoch 0
+ * from the automata as the first 8,192 leave them, or the first 8,192 from
+ * the initial state for shorter launches) -- the automata are reset to the
+ * initial state afterwards -- and caches the fastest for
  * the process; 2: tune on every train call.  No counterpart in the
  * reference (it has one CPU code path). */
 int tm_set_autotune(tm_machine *m, int32_t mode);

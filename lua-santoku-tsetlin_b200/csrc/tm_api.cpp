@@ -8,6 +8,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <functional>
 #include <map>
 #include <tuple>
 #include <atomic>
@@ -159,6 +160,8 @@ struct tm_machine {
   // each distinct holdout row layout
   DevBuf search_act8;
   std::vector<DevBuf> search_x8;
+  // the autotuner's snapshot of the automata between its trials
+  DevBuf tune_snap;
   // pinned staging of small host requests (TM_PIN_STAGE bytes each way):
   // inputs go host -> pin -> device, outputs device -> pin -> host, so that
   // a one-sample predict makes no pageable (synchronously staged) copy.
@@ -440,7 +443,7 @@ extern "C" void tm_destroy(tm_machine *m) {
   for (DevBuf *b : {&m->x, &m->tx, &m->raw, &m->labels, &m->codes, &m->perm, &m->perm_scratch, &m->sums,
                     &m->outc, &m->work, &m->tdev, &m->cls_job, &m->errf, &m->ckpt, &m->search,
                     &m->search_truth, &m->act8, &m->x8, &m->gemm_c, &m->gemm_ws,
-                    &m->search_act8})
+                    &m->search_act8, &m->tune_snap})
     b->release();
   for (DevBuf &b : m->search_x8) b.release();
   if (m->ev0) cudaEventDestroy(m->ev0);
@@ -866,6 +869,9 @@ static int autotune_plan(std::vector<TrainJob> &jobs, const std::vector<TrainDev
   const bool tune_log = tl && tl[0] == '1';
   // the trials' (unit, sample) steps are not the caller's training
   const uint64_t pairs0 = m0->stats.train_active_pairs;
+  // the automata every trial starts from: reset (the initial state) or a
+  // snapshot taken part-way into epoch 0
+  std::function<int()> prepare = reset;
   auto timed = [&](size_t i, const std::vector<TrainDev> &tt, const std::vector<WorkItem> &tw,
                    int stage, float &tmin) -> int {
     TrainShape tsh = sh;
@@ -875,7 +881,7 @@ static int autotune_plan(std::vector<TrainJob> &jobs, const std::vector<TrainDev
     if (!plan_mode(cand[i].mode, tsh, p, cand[i].cpw)) return TM_OK;
     float t = 0;
     for (int rep = 0; rep < 2; rep++) {
-      int rc = reset();
+      int rc = prepare();
       if (rc) return rc;
       uint32_t herr = 0;
       rc = launch_plan(p, tsh, tt, tw, 0, 1, m0, &t, &herr);
@@ -902,8 +908,65 @@ static int autotune_plan(std::vector<TrainJob> &jobs, const std::vector<TrainDev
   std::sort(first.begin(), first.end());
   int best = first.empty() ? -1 : (int)first[0].second;
   if (first.size() > 1) {
-    const std::vector<TrainDev> tt = trial_rows(8192);
+    // The second trial times positions [W, W + T) of epoch 0 from the
+    // automata as the first W positions leave them (any variant gives the
+    // same automata): past the first samples, whose empty clauses make for
+    // another mix of feedback than the rest of an epoch.  Launches of fewer
+    // than W + T samples time the first T from the initial state.
+    const uint32_t W = 8192, T = 8192;
     const std::vector<WorkItem> tw = trial_units(64);
+    std::vector<TrainDev> tt;
+    uint32_t nmax = 0;
+    for (const auto &t : td) nmax = std::max(nmax, t.n);
+    uint64_t snap_bytes = 0;
+    for (const auto &J : jobs) snap_bytes += ((uint64_t)J.m->act_words + J.m->cnt_words) * 4;
+    bool steady = nmax >= W + T && snap_bytes > 0;
+    if (steady) {
+      TrainShape tsh = sh;
+      tsh.units = (uint32_t)tw.size();
+      TrainPlan p0;
+      steady = plan_mode(cand[first[0].second].mode, tsh, p0, cand[first[0].second].cpw) &&
+               m0->tune_snap.ensure(snap_bytes) == cudaSuccess;
+      if (!steady) cudaGetLastError();
+      if (steady) {
+        int rc = reset();
+        if (rc) return rc;
+        uint32_t herr = 0;
+        float tw0 = 0;
+        rc = launch_plan(p0, tsh, trial_rows(W), tw, 0, 1, m0, &tw0, &herr);
+        if (rc) return rc;
+        if (herr) return fail(TM_ERR_DEVICE, "train: a sample copy did not complete (status %u)", herr);
+        uint64_t o = 0;
+        for (auto &J : jobs) {
+          const uint64_t ab = (uint64_t)J.m->act_words * 4, cb = (uint64_t)J.m->cnt_words * 4;
+          CK(cudaMemcpyAsync(m0->tune_snap.as<uint8_t>() + o, J.m->d_act, ab,
+                             cudaMemcpyDeviceToDevice, m0->st));
+          if (cb)
+            CK(cudaMemcpyAsync(m0->tune_snap.as<uint8_t>() + o + ab, J.m->d_cnt, cb,
+                               cudaMemcpyDeviceToDevice, m0->st));
+          o += ab + cb;
+        }
+        prepare = [&]() -> int {
+          uint64_t q = 0;
+          for (auto &J : jobs) {
+            const uint64_t ab = (uint64_t)J.m->act_words * 4, cb = (uint64_t)J.m->cnt_words * 4;
+            CK(cudaMemcpyAsync(J.m->d_act, m0->tune_snap.as<uint8_t>() + q, ab,
+                               cudaMemcpyDeviceToDevice, m0->st));
+            if (cb)
+              CK(cudaMemcpyAsync(J.m->d_cnt, m0->tune_snap.as<uint8_t>() + q + ab, cb,
+                                 cudaMemcpyDeviceToDevice, m0->st));
+            q += ab + cb;
+          }
+          return TM_OK;
+        };
+        tt = td;
+        for (auto &t : tt) {
+          t.perm += W;
+          t.n = t.n > W ? std::min<uint32_t>(t.n - W, T) : 0;
+        }
+      }
+    }
+    if (!steady) tt = trial_rows(T);
     float best_ms = -1;
     for (size_t r = 0; r < first.size() && r < 3; r++) {
       float tmin = -1;
@@ -916,6 +979,7 @@ static int autotune_plan(std::vector<TrainJob> &jobs, const std::vector<TrainDev
     }
   }
   m0->stats.train_active_pairs = pairs0;
+  m0->tune_snap.release();
   // back to the initial state
   {
     int rc = reset();
