@@ -6,15 +6,17 @@ Metric: "TM train+predict samples/s (batched vs plain, equal accuracy)".
 Default workload (N = 1): the batched hyper-parameter search -- 64
 classifiers of uneven size (clauses per class log-uniform over 64..4,096,
 specificity U[2, 40], target U[20, 400], negated literals on or off) on
-plain-classifier data (10 classes, 784 features, class prototypes with 10 %
-bit flips) scaled to 60,000 train and 15,000 holdout samples.  A search
+plain-classifier data (10 classes, 784 features, class prototypes with 40 %
+bit flips: a trained machine scores about 98 % macro F1) scaled to 60,000
+train and 15,000 holdout samples.  A search
 round trains all 64 for 10 epochs and scores each on the holdout after
 every epoch (the reference's search loop, optimize.lua:424-471, with
 train_tm's epoch logic, :586-653; search metric = macro F1 of
 evaluator.class_accuracy).  One step is one epoch of the round: all 64
 machines train one epoch over the 60,000 samples, then predict and score
 the 15,000 holdout samples -- `tm_train_batch_search`, one CUDA graph
-replay per epoch.  `value` counts machine-samples (train + holdout) per
+replay per epoch (the train kernels of the two row widths on two streams,
+the holdout predict of the large machines as 8-bit GEMM nodes).  `value` counts machine-samples (train + holdout) per
 second over K consecutive epochs; rounds restart after 10 epochs and their
 set-up (machine creation, staging, graph capture) is inside the timed
 region.  `plain` is the same round run the reference's way: one machine at
@@ -23,8 +25,9 @@ a time, one launch per epoch, the metric on the host between epochs.
 (they are bit-identical).
 
 Other workloads (--workload): c1 / c0 / c2 -- one machine, one step = one
-training epoch from the initial state + predict of the test set; serve --
-resident machines under Poisson requests.
+training epoch from the initial state + predict of the test set (large
+predicts as the 8-bit GEMM); serve -- resident machines under Poisson
+requests.
 
 Arms:
   default           the CUDA library through the C ABI (santoku_tsetlin)
