@@ -914,7 +914,7 @@ def serve_at(args, L, tm, machines, pools, rng, rate, requests=None):
     th = threading.Thread(target=submit)
     th.start()
     th.join()
-    lat, acc_sizes, acc_arrive, acc_which = [], [], [], []
+    lat, acc_sizes, acc_arrive, acc_which, phases = [], [], [], [], []
     for i in range(nreq):
         if ids[i] is None:
             continue
@@ -924,6 +924,9 @@ def serve_at(args, L, tm, machines, pools, rng, rate, requests=None):
         us = ctypes.c_double()
         L.tm_serve_latency_us(srv, ids[i], ctypes.byref(us))
         lat.append(us.value / 1e3)
+        ph = (ctypes.c_double * 3)()
+        L.tm_serve_phases_us(srv, ids[i], ph)
+        phases.append([v / 1e3 for v in ph])
         acc_sizes.append(int(sizes[i]))
         acc_arrive.append(arrive[i])
     makespan = float(np.max(np.array(acc_arrive) + np.array(lat) / 1e3))
@@ -956,8 +959,15 @@ def serve_at(args, L, tm, machines, pools, rng, rate, requests=None):
                                                           if z <= 256] or [0], 99))},
         "accepted": len(lat), "refused_queue_full": nreq - len(lat),
         "slowest": [{"machine": acc_which[j], "samples": acc_sizes[j],
-                     "latency_ms": lat[j], "arrival_s": float(acc_arrive[j])}
+                     "latency_ms": lat[j], "arrival_s": float(acc_arrive[j]),
+                     "queue_ms": phases[j][0], "host_launch_ms": phases[j][1],
+                     "device_ms": phases[j][2]}
                     for j in np.argsort(lat)[::-1][:6]],
+        # each phase's own p99 over the accepted requests: the wait in the
+        # queue, the worker's staging and launch calls, the device work and
+        # the completion callback
+        "phase_p99_ms": {k: float(np.percentile([p[i] for p in phases], 99))
+                         for i, k in enumerate(("queue", "host_launch", "device"))},
         "offered_samples_per_s": float(sizes.sum() / arrive[-1]),
         "samples_per_s": float(sum(acc_sizes)) / makespan,
         "serial": {"p50_ms": float(np.percentile(lat_s, 50)),

@@ -428,6 +428,11 @@ int tm_serve_poll(tm_server *s, uint64_t id, int64_t *out_classes, uint8_t *out_
 /* submit -> done latency of a completed request, microseconds (also after
  * it was polled, for the last 65,536 polled requests) */
 int tm_serve_latency_us(tm_server *s, uint64_t id, double *us);
+/* the same request's latency in three phases, microseconds: out[0] the wait
+ * in the queue (submit -> taken by the worker), out[1] the host's staging
+ * and launch calls for its launch slot, out[2] the device work and the
+ * completion (launches queued -> done); they add up to the latency */
+int tm_serve_phases_us(tm_server *s, uint64_t id, double *out);
 /* out[5]: queued requests, queued samples, requests not yet polled, busy
  * launch slots, launch slots */
 int tm_serve_stats(tm_server *s, uint64_t *out);

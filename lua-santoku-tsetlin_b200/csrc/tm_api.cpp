@@ -1473,8 +1473,8 @@ static int search_round(tm_machine *const *ms, const tm_train_args *args, uint32
       CK(m0->search_act8.ensure(amax));
     }
     // one byte copy of the holdout per distinct row layout (the machines'
-    // staged rows of one source and row width are the same)
-    std::map<std::tuple<const void *, uint32_t, uint32_t>, size_t> x8_of;
+    // staged rows of one source, feature count and row width are the same)
+    std::map<std::tuple<const void *, uint64_t, uint32_t, uint32_t>, size_t> x8_of;
     for (uint32_t i = 0; i < count; i++) {
       if (!use_gemm[i]) continue;
       tm_machine *m = ms[i];
@@ -1482,7 +1482,7 @@ static int search_round(tm_machine *const *ms, const tm_train_args *args, uint32
       const uint64_t K = (uint64_t)c0.W * 32;
       const void *src = sa->test_each && sa->test_each[i] ? (const void *)sa->test_each[i]
                                                           : (const void *)sa->test_problems;
-      const auto key = std::make_tuple(src, c0.Wp, c0.W);
+      const auto key = std::make_tuple(src, (uint64_t)m->features, c0.Wp, c0.W);
       if (x8_of.count(key)) continue;
       const size_t at = x8_of.size();
       x8_of[key] = at;
@@ -1503,7 +1503,8 @@ static int search_round(tm_machine *const *ms, const tm_train_args *args, uint32
       const ClassDev &c0 = m->cls[0];
       const void *src = sa->test_each && sa->test_each[i] ? (const void *)sa->test_each[i]
                                                           : (const void *)sa->test_problems;
-      gx8[i] = m0->search_x8[x8_of[std::make_tuple(src, c0.Wp, c0.W)]].as<uint8_t>();
+      gx8[i] = m0->search_x8[x8_of[std::make_tuple(src, (uint64_t)m->features, c0.Wp, c0.W)]]
+                   .as<uint8_t>();
       const uint64_t M = (uint64_t)m->classes * m->clauses, K = (uint64_t)c0.W * 32;
       const uint64_t nc = gchunk[i];
       for (uint64_t s0 = 0; s0 < nt && use_gemm[i]; s0 += nc) {
@@ -1961,10 +1962,6 @@ static bool gemm_wanted(tm_machine *m, uint64_t n) {
   return gemm_kind_of(m->device) > 0;
 }
 
-// The vote sums of the n staged rows (m->x) through the GEMM.  Returns
-// TM_OK, a TM_ERR_* code, or 1 when the library has no algorithm for this
-// shape in either encoding (nothing was written; the caller uses the
-// bitwise kernels).
 // The action bytes of a dense machine in `kind`'s encoding (queued on the
 // machine's stream).
 static int ensure_act8(tm_machine *m, int kind) {
@@ -1981,6 +1978,10 @@ static int ensure_act8(tm_machine *m, int kind) {
   return TM_OK;
 }
 
+// The vote sums of the n staged rows (m->x) through the GEMM.  Returns
+// TM_OK, a TM_ERR_* code, or 1 when the library has no algorithm for this
+// shape in either encoding (no vote sum was written; the caller uses the
+// bitwise kernels).
 static int predict_gemm(tm_machine *m, uint64_t n) {
   const ClassDev &c0 = m->cls[0];
   const uint64_t M = (uint64_t)m->classes * m->clauses, K = (uint64_t)c0.W * 32;

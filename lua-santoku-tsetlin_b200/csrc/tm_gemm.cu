@@ -101,18 +101,21 @@ std::mutex g_lt_mu;
 cublasLtHandle_t g_lt[64];
 int g_lt_state[64];  // 0 not created, 1 ready
 
-// The library's choice per (device, encoding, M, N, K): asked once per shape
-// (products of few distinct widths are asked for: callers round N up to a
-// bucket).  found == 0 records a shape without an algorithm.
+// The library's choice per (device, encoding, M, N, K, workspace bytes):
+// asked once per shape (products of few distinct widths are asked for:
+// callers round N up to a bucket); the workspace limit is part of the key,
+// so an algorithm chosen under a larger workspace is never run with a
+// smaller one.  found == 0 records a shape without an algorithm.
 struct AlgoKey {
   int dev, kind;
-  uint64_t M, N, K;
+  uint64_t M, N, K, ws;
   bool operator<(const AlgoKey &o) const {
     if (dev != o.dev) return dev < o.dev;
     if (kind != o.kind) return kind < o.kind;
     if (M != o.M) return M < o.M;
     if (N != o.N) return N < o.N;
-    return K < o.K;
+    if (K != o.K) return K < o.K;
+    return ws < o.ws;
   }
 };
 struct AlgoVal {
@@ -198,7 +201,7 @@ int gemm_clause_products(int dev, int kind, const uint8_t *A, const uint8_t *B, 
                                              &ws_bytes, sizeof ws_bytes);
   cublasLtMatmulHeuristicResult_t h{};
   int found = 0;
-  const AlgoKey key{dev, kind, M, N, K};
+  const AlgoKey key{dev, kind, M, N, K, (uint64_t)ws_bytes};
   bool cached = false;
   {
     std::lock_guard<std::mutex> lk(g_lt_mu);

@@ -58,9 +58,25 @@ struct Request {
   uint64_t n;
   std::vector<uint8_t> input;   // dropped once staged
   std::vector<uint8_t> result;  // int64 classes or code bytes
-  clk::time_point t_submit, t_done;
+  // submitted; taken by the worker; its slot's launches queued; completed
+  clk::time_point t_submit, t_taken, t_launched, t_done;
   bool done = false;
 };
+
+// A request's phases, microseconds: submit -> done, the wait in the queue
+// (submit -> taken), the host's staging and launch calls (taken ->
+// launched), the device work and the completion (launched -> done).
+struct Times {
+  double total, queue, launch, device;
+};
+
+Times times_of(const Request &r) {
+  auto us = [](clk::time_point a, clk::time_point b) {
+    return std::chrono::duration<double, std::micro>(b - a).count();
+  };
+  return Times{us(r.t_submit, r.t_done), us(r.t_submit, r.t_taken), us(r.t_taken, r.t_launched),
+               us(r.t_launched, r.t_done)};
+}
 
 struct Slot {
   tm_server *srv = nullptr;
@@ -112,7 +128,7 @@ struct tm_server {
   std::deque<Request *> squeue;   // small requests, arrival order
   uint64_t queued_samples = 0;
   std::unordered_map<uint64_t, Request *> live;  // submitted, not yet polled done
-  std::unordered_map<uint64_t, double> latency;   // polled: submit -> done, microseconds
+  std::unordered_map<uint64_t, Times> latency;    // polled requests' phases
   std::deque<uint64_t> latency_order;
   uint64_t next_id = 1;
   bool stop = false;
@@ -151,6 +167,8 @@ static void CUDART_CB slot_done(void *p) {
 // slot_done).
 static cudaError_t launch_slot(tm_server *s, Slot &sl) {
   const uint32_t R = (uint32_t)sl.reqs.size();
+  const clk::time_point taken = clk::now();
+  for (Request *r : sl.reqs) r->t_taken = taken;
   ServeJob *sj = (ServeJob *)sl.h_jobs;
   SmallJob *mj = (SmallJob *)(sl.h_jobs + round_up(TM_SERVE_MAX_PACK * sizeof(ServeJob), 256));
   PredictJob *pj = (PredictJob *)((uint8_t *)mj +
@@ -240,6 +258,9 @@ static cudaError_t launch_slot(tm_server *s, Slot &sl) {
     e = launch_predict_multi((const PredictJob *)(sl.d_jobs + o_pj), npred, tiles, sl.st);
   if (e == cudaSuccess) e = launch_serve_finalize((const ServeJob *)sl.d_jobs, R, sl.st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(sl.h_out, sl.d_out, o_off, cudaMemcpyDeviceToHost, sl.st);
+  // before the completion is queued: slot_done may run as soon as it is
+  const clk::time_point launched = clk::now();
+  for (Request *r : sl.reqs) r->t_launched = launched;
   if (e == cudaSuccess) e = cudaLaunchHostFunc(sl.st, slot_done, &sl);
   return e;
 }
@@ -492,7 +513,7 @@ extern "C" int tm_serve_poll(tm_server *s, uint64_t id, int64_t *out_classes, ui
   if (v.type == TM_CLASSIFIER && out_classes) memcpy(out_classes, r->result.data(), r->result.size());
   if (v.type == TM_ENCODER && out_codes) memcpy(out_codes, r->result.data(), r->result.size());
   // the request is released; its latency stays queryable for a while
-  s->latency[id] = std::chrono::duration<double, std::micro>(r->t_done - r->t_submit).count();
+  s->latency[id] = times_of(*r);
   s->latency_order.push_back(id);
   while (s->latency_order.size() > TM_SERVE_LATENCY_KEEP) {
     s->latency.erase(s->latency_order.front());
@@ -503,19 +524,38 @@ extern "C" int tm_serve_poll(tm_server *s, uint64_t id, int64_t *out_classes, ui
   return 1;
 }
 
-extern "C" int tm_serve_latency_us(tm_server *s, uint64_t id, double *us) {
-  if (!s || !us) return tmb_fail(TM_ERR_ARG, "serve_latency_us: bad arguments");
-  std::lock_guard<std::mutex> lk(s->mu);
+static int find_times(tm_server *s, uint64_t id, Times *t, const char *who) {
   auto lt = s->latency.find(id);
   if (lt != s->latency.end()) {
-    *us = lt->second;
+    *t = lt->second;
     return TM_OK;
   }
   auto it = s->live.find(id);
-  if (it == s->live.end() || !it->second->done)
-    return tmb_fail(TM_ERR_ARG, "serve_latency_us: request not done");
-  *us = std::chrono::duration<double, std::micro>(it->second->t_done - it->second->t_submit).count();
+  if (it == s->live.end() || !it->second->done) {
+    char msg[64];
+    snprintf(msg, sizeof msg, "%s: request not done", who);
+    return tmb_fail(TM_ERR_ARG, msg);
+  }
+  *t = times_of(*it->second);
   return TM_OK;
+}
+
+extern "C" int tm_serve_latency_us(tm_server *s, uint64_t id, double *us) {
+  if (!s || !us) return tmb_fail(TM_ERR_ARG, "serve_latency_us: bad arguments");
+  std::lock_guard<std::mutex> lk(s->mu);
+  Times t;
+  const int rc = find_times(s, id, &t, "serve_latency_us");
+  if (!rc) *us = t.total;
+  return rc;
+}
+
+extern "C" int tm_serve_phases_us(tm_server *s, uint64_t id, double *out) {
+  if (!s || !out) return tmb_fail(TM_ERR_ARG, "serve_phases_us: bad arguments");
+  std::lock_guard<std::mutex> lk(s->mu);
+  Times t;
+  const int rc = find_times(s, id, &t, "serve_phases_us");
+  if (!rc) out[0] = t.queue, out[1] = t.launch, out[2] = t.device;
+  return rc;
 }
 
 extern "C" int tm_serve_stats(tm_server *s, uint64_t *out) {

@@ -170,7 +170,7 @@ EXPORTS = (
     "tm_destroy", "tm_last_error", "tm_align", "tm_get_info", "tm_export_state",
     "tm_import_state", "tm_export_classes", "tm_import_classes", "tm_class_accuracy", "tm_encoding_accuracy", "tm_bits_to_cvec", "tm_bits_to_cvec_ind",
     "tm_predict_noalloc", "tm_int_peaks", "tm_debug_fail_alloc", "tm_set_autotune", "tm_force_variant", "tm_stats_enable", "tm_get_stats", "tm_reset_stats", "tm_serve_open", "tm_serve_submit", "tm_serve_poll",
-    "tm_serve_latency_us", "tm_serve_stats", "tm_serve_close",
+    "tm_serve_latency_us", "tm_serve_phases_us", "tm_serve_stats", "tm_serve_close",
 )
 
 
@@ -231,6 +231,7 @@ def lib():
     L.tm_serve_submit.argtypes = [vp, u32, vp, u64, ctypes.POINTER(u64)]
     L.tm_serve_poll.argtypes = [vp, u64, vp, vp, u64]
     L.tm_serve_latency_us.argtypes = [vp, u64, ctypes.POINTER(ctypes.c_double)]
+    L.tm_serve_phases_us.argtypes = [vp, u64, ctypes.POINTER(ctypes.c_double)]
     L.tm_serve_stats.argtypes = [vp, vp]
     L.tm_serve_close.argtypes = [vp]
     _lib = L
