@@ -924,7 +924,7 @@ def serve_at(args, L, tm, machines, pools, rng, rate, requests=None):
         us = ctypes.c_double()
         L.tm_serve_latency_us(srv, ids[i], ctypes.byref(us))
         lat.append(us.value / 1e3)
-        ph = (ctypes.c_double * 3)()
+        ph = (ctypes.c_double * 4)()
         L.tm_serve_phases_us(srv, ids[i], ph)
         phases.append([v / 1e3 for v in ph])
         acc_sizes.append(int(sizes[i]))
@@ -961,13 +961,15 @@ def serve_at(args, L, tm, machines, pools, rng, rate, requests=None):
         "slowest": [{"machine": acc_which[j], "samples": acc_sizes[j],
                      "latency_ms": lat[j], "arrival_s": float(acc_arrive[j]),
                      "queue_ms": phases[j][0], "host_launch_ms": phases[j][1],
-                     "device_ms": phases[j][2]}
+                     "device_ms": phases[j][2], "launch_gpu_span_ms": phases[j][3]}
                     for j in np.argsort(lat)[::-1][:6]],
         # each phase's own p99 over the accepted requests: the wait in the
         # queue, the worker's staging and launch calls, the device work and
-        # the completion callback
+        # the completion; and of the launches' device spans (CUDA events
+        # around each launch)
         "phase_p99_ms": {k: float(np.percentile([p[i] for p in phases], 99))
-                         for i, k in enumerate(("queue", "host_launch", "device"))},
+                         for i, k in enumerate(("queue", "host_launch", "device",
+                                                "launch_gpu_span"))},
         "offered_samples_per_s": float(sizes.sum() / arrive[-1]),
         "samples_per_s": float(sum(acc_sizes)) / makespan,
         "serial": {"p50_ms": float(np.percentile(lat_s, 50)),

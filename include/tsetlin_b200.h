@@ -428,10 +428,12 @@ int tm_serve_poll(tm_server *s, uint64_t id, int64_t *out_classes, uint8_t *out_
 /* submit -> done latency of a completed request, microseconds (also after
  * it was polled, for the last 65,536 polled requests) */
 int tm_serve_latency_us(tm_server *s, uint64_t id, double *us);
-/* the same request's latency in three phases, microseconds: out[0] the wait
- * in the queue (submit -> taken by the worker), out[1] the host's staging
- * and launch calls for its launch slot, out[2] the device work and the
- * completion (launches queued -> done); they add up to the latency */
+/* out[4], microseconds: the same request's latency in three phases --
+ * out[0] the wait in the queue (submit -> taken by the worker), out[1] the
+ * host's staging and launch calls for its launch slot, out[2] the device
+ * work and the completion (launches queued -> done), which add up to the
+ * latency -- and out[3] the device span of its launch, from the copy in to
+ * the end of the copy out, measured with CUDA events */
 int tm_serve_phases_us(tm_server *s, uint64_t id, double *out);
 /* out[5]: queued requests, queued samples, requests not yet polled, busy
  * launch slots, launch slots */

@@ -14,8 +14,10 @@
 // (requests of at most 32 samples as warp-per-clause jobs reading each
 // clause row once, larger ones as 64 x 64 tiles; each kind for all requests
 // and machines in one launch), the finalize of every request and one copy
-// of the results.  A host function queued behind the copy completes the
-// slot's requests and frees the slot the moment the GPU is done.  Requests
+// of the results.  Each slot has a completion thread: it sleeps on a CUDA
+// event recorded behind the copy, then completes the slot's requests and
+// frees the slot (the two events around the launch also give its device
+// span).  Requests
 // that arrive while slots are busy are admitted as slots free up, and the
 // slots' streams overlap on the device.  Predict is independent per
 // sample, so each request's result is the same alone or packed with
@@ -60,6 +62,7 @@ struct Request {
   std::vector<uint8_t> result;  // int64 classes or code bytes
   // submitted; taken by the worker; its slot's launches queued; completed
   clk::time_point t_submit, t_taken, t_launched, t_done;
+  double gpu_us = 0;  // the device span of its launch (CUDA events)
   bool done = false;
 };
 
@@ -67,7 +70,7 @@ struct Request {
 // (submit -> taken), the host's staging and launch calls (taken ->
 // launched), the device work and the completion (launched -> done).
 struct Times {
-  double total, queue, launch, device;
+  double total, queue, launch, device, gpu;
 };
 
 Times times_of(const Request &r) {
@@ -75,7 +78,7 @@ Times times_of(const Request &r) {
     return std::chrono::duration<double, std::micro>(b - a).count();
   };
   return Times{us(r.t_submit, r.t_done), us(r.t_submit, r.t_taken), us(r.t_taken, r.t_launched),
-               us(r.t_launched, r.t_done)};
+               us(r.t_launched, r.t_done), r.gpu_us};
 }
 
 struct Slot {
@@ -89,10 +92,15 @@ struct Slot {
   // clause x sample products, the library's workspace
   uint8_t *d_x8 = nullptr, *d_ws = nullptr;
   void *d_gc = nullptr;
+  // recorded before the copy in and after the copy out (the completion
+  // thread sleeps on ev1)
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::thread done_thread;
   std::vector<Request *> reqs;
   std::vector<uint64_t> out_off;  // each request's result offset in h_out
   bool busy = false;
-  bool high = false;  // a high-priority stream, kept for small requests
+  bool launched = false;  // queued launches wait for the completion thread
+  bool high = false;      // a high-priority stream, kept for small requests
 };
 
 uint64_t round_up(uint64_t v, uint64_t a) { return (v + a - 1) / a * a; }
@@ -123,7 +131,7 @@ struct tm_server {
   std::vector<Slot> slots;
   uint64_t cap_in = 0, cap_out = 0, cap_x = 0, cap_sums = 0, cap_jobs = 0;
   std::mutex mu;
-  std::condition_variable cv_work, cv_done;
+  std::condition_variable cv_work, cv_done, cv_launched;
   std::deque<Request *> queue;    // large requests, arrival order
   std::deque<Request *> squeue;   // small requests, arrival order
   uint64_t queued_samples = 0;
@@ -132,6 +140,7 @@ struct tm_server {
   std::deque<uint64_t> latency_order;
   uint64_t next_id = 1;
   bool stop = false;
+  bool closing = false;  // the completion threads end once their slot is idle
   std::thread worker;
   int error = 0;
 };
@@ -140,31 +149,47 @@ static uint64_t out_bytes(const MachineView &v, uint64_t n) {
   return v.type == TM_CLASSIFIER ? n * 8 : n * v.class_chunks;
 }
 
-// CUDA runs this on its own thread once the slot's result copy is done: it
-// completes the slot's requests and frees the slot (no CUDA calls here).
-static void CUDART_CB slot_done(void *p) {
-  Slot *sl = (Slot *)p;
-  tm_server *s = sl->srv;
-  const clk::time_point now = clk::now();
-  {
-    std::lock_guard<std::mutex> lk(s->mu);
-    for (size_t i = 0; i < sl->reqs.size(); i++) {
-      Request *r = sl->reqs[i];
-      const uint64_t b = out_bytes(s->mv[r->machine], r->n);
-      r->result.assign(sl->h_out + sl->out_off[i], sl->h_out + sl->out_off[i] + b);
-      r->t_done = now;
-      r->done = true;
+// A slot's completion thread: for every launch of the slot, it waits (asleep)
+// for the event recorded behind the result copy, then completes the
+// launch's requests and frees the slot.  It ends when the server closes and
+// the slot holds no launch.
+static void slot_main(tm_server *s, Slot *sl) {
+  cudaSetDevice(s->cfg.device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  while (true) {
+    s->cv_launched.wait(lk, [&] { return sl->launched || s->closing; });
+    if (!sl->launched) break;
+    lk.unlock();
+    cudaError_t e = cudaEventSynchronize(sl->ev1);
+    const clk::time_point now = clk::now();
+    float ms = 0;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, sl->ev0, sl->ev1);
+    lk.lock();
+    if (e != cudaSuccess) {
+      // the requests stay not done; polls report the failure
+      s->error = TM_ERR_CUDA;
+      s->stop = true;
+    } else {
+      for (size_t i = 0; i < sl->reqs.size(); i++) {
+        Request *r = sl->reqs[i];
+        const uint64_t b = out_bytes(s->mv[r->machine], r->n);
+        r->result.assign(sl->h_out + sl->out_off[i], sl->h_out + sl->out_off[i] + b);
+        r->t_done = now;
+        r->gpu_us = 1e3 * ms;
+        r->done = true;
+      }
+      sl->busy = false;
     }
     sl->reqs.clear();
-    sl->busy = false;
+    sl->launched = false;
+    s->cv_done.notify_all();
+    s->cv_work.notify_all();
   }
-  s->cv_done.notify_all();
-  s->cv_work.notify_one();
 }
 
 // Stages the slot's requests and queues its launches (called without the
-// server lock: the slot and its requests belong to the worker until
-// slot_done).
+// server lock: the slot and its requests belong to the worker until the
+// slot's completion thread takes them).
 static cudaError_t launch_slot(tm_server *s, Slot &sl) {
   const uint32_t R = (uint32_t)sl.reqs.size();
   const clk::time_point taken = clk::now();
@@ -222,7 +247,9 @@ static cudaError_t launch_slot(tm_server *s, Slot &sl) {
     s_off = round_up(s_off + r->n * v.classes, 4);
     o_off = round_up(o_off + out_bytes(v, r->n), 16);
   }
-  cudaError_t e = cudaMemcpyAsync(sl.d_raw, sl.h_in, in_off, cudaMemcpyHostToDevice, sl.st);
+  cudaError_t e = cudaEventRecord(sl.ev0, sl.st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(sl.d_raw, sl.h_in, in_off, cudaMemcpyHostToDevice, sl.st);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(sl.d_jobs, sl.h_jobs, o_pj + npred * sizeof(PredictJob),
                         cudaMemcpyHostToDevice, sl.st);
@@ -258,10 +285,9 @@ static cudaError_t launch_slot(tm_server *s, Slot &sl) {
     e = launch_predict_multi((const PredictJob *)(sl.d_jobs + o_pj), npred, tiles, sl.st);
   if (e == cudaSuccess) e = launch_serve_finalize((const ServeJob *)sl.d_jobs, R, sl.st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(sl.h_out, sl.d_out, o_off, cudaMemcpyDeviceToHost, sl.st);
-  // before the completion is queued: slot_done may run as soon as it is
+  if (e == cudaSuccess) e = cudaEventRecord(sl.ev1, sl.st);
   const clk::time_point launched = clk::now();
   for (Request *r : sl.reqs) r->t_launched = launched;
-  if (e == cudaSuccess) e = cudaLaunchHostFunc(sl.st, slot_done, &sl);
   return e;
 }
 
@@ -316,15 +342,39 @@ static void worker_main(tm_server *s) {
       s->stop = true;
       break;
     }
+    sl.launched = true;  // to the slot's completion thread
+    s->cv_launched.notify_all();
   }
   lk.unlock();
-  // drain: every queued launch completes its requests through slot_done
+  // drain: every queued launch completes its requests through its slot's
+  // completion thread
   for (Slot &sl : s->slots) cudaStreamSynchronize(sl.st);
   s->cv_done.notify_all();
 }
 
+// Ends the worker and the completion threads (queued launches complete
+// first).
+static void stop_threads(tm_server *s) {
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv_work.notify_all();
+  if (s->worker.joinable()) s->worker.join();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->closing = true;
+  }
+  s->cv_launched.notify_all();
+  for (Slot &sl : s->slots)
+    if (sl.done_thread.joinable()) sl.done_thread.join();
+}
+
 static void free_server(tm_server *s) {
+  stop_threads(s);
   for (Slot &sl : s->slots) {
+    if (sl.ev0) cudaEventDestroy(sl.ev0);
+    if (sl.ev1) cudaEventDestroy(sl.ev1);
     if (sl.st) cudaStreamDestroy(sl.st);
     if (sl.h_in) cudaFreeHost(sl.h_in);
     if (sl.h_out) cudaFreeHost(sl.h_out);
@@ -418,6 +468,8 @@ extern "C" int tm_serve_open(const tm_server_config *cfg, tm_machine *const *mac
     sl.high = i < nhigh;
     bool ok = cudaStreamCreateWithPriority(&sl.st, cudaStreamNonBlocking,
                                            sl.high ? prio_hi : prio_lo) == cudaSuccess &&
+              cudaEventCreate(&sl.ev0) == cudaSuccess &&
+              cudaEventCreateWithFlags(&sl.ev1, cudaEventBlockingSync) == cudaSuccess &&
               cudaHostAlloc(&sl.h_in, s->cap_in, cudaHostAllocDefault) == cudaSuccess &&
               cudaHostAlloc(&sl.h_out, s->cap_out, cudaHostAllocDefault) == cudaSuccess &&
               cudaHostAlloc(&sl.h_jobs, s->cap_jobs, cudaHostAllocDefault) == cudaSuccess &&
@@ -459,6 +511,7 @@ extern "C" int tm_serve_open(const tm_server_config *cfg, tm_machine *const *mac
       if (N >= cap) break;
     }
   }
+  for (Slot &sl : s->slots) sl.done_thread = std::thread(slot_main, s, &sl);
   s->worker = std::thread(worker_main, s);
   *out = s;
   return TM_OK;
@@ -554,7 +607,7 @@ extern "C" int tm_serve_phases_us(tm_server *s, uint64_t id, double *out) {
   std::lock_guard<std::mutex> lk(s->mu);
   Times t;
   const int rc = find_times(s, id, &t, "serve_phases_us");
-  if (!rc) out[0] = t.queue, out[1] = t.launch, out[2] = t.device;
+  if (!rc) out[0] = t.queue, out[1] = t.launch, out[2] = t.device, out[3] = t.gpu;
   return rc;
 }
 
@@ -573,12 +626,7 @@ extern "C" int tm_serve_stats(tm_server *s, uint64_t *out) {
 
 extern "C" int tm_serve_close(tm_server *s) {
   if (!s) return TM_OK;
-  {
-    std::lock_guard<std::mutex> lk(s->mu);
-    s->stop = true;
-  }
-  s->cv_work.notify_all();
-  if (s->worker.joinable()) s->worker.join();
+  stop_threads(s);
   const int err = s->error;
   free_server(s);
   return err ? tmb_fail(err, "serve: a launch failed") : TM_OK;

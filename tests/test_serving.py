@@ -93,10 +93,12 @@ def test_alone_equals_mixed(tm):
         assert L.tm_serve_latency_us(srv, ids[i], ctypes.byref(us)) == 0
         lat.append(us.value)
         # the three phases (queue wait, host launch calls, device work and
-        # completion) are non-negative and add up to the latency
-        ph = (ctypes.c_double * 3)()
+        # completion) are non-negative and add up to the latency; the
+        # launch's device span is positive
+        ph = (ctypes.c_double * 4)()
         assert L.tm_serve_phases_us(srv, ids[i], ph) == 0
-        assert min(ph) >= 0 and abs(sum(ph) - us.value) <= 1e-6 * us.value + 1e-3
+        assert min(ph[:3]) >= 0 and abs(sum(ph[:3]) - us.value) <= 1e-6 * us.value + 1e-3
+        assert ph[3] > 0
     assert all(v > 0 for v in lat)
     # a polled request is released: its id is unknown to a second poll, its
     # latency stays readable, and nothing is left waiting
