@@ -277,7 +277,6 @@ __global__ void __launch_bounds__(PAIR ? 2 * TM_TRAIN_THREADS : TM_TRAIN_THREADS
       __syncthreads();
     }
     uint32_t *act_j = act + lc * Wp;
-    uint32_t *cnt_j = cnt + (size_t)lc * m * Wp;
     bool dirty[CPW];         // this warp's clauses changed since their literal counts were taken
     uint32_t lit_cache[CPW];  // their literal counts when clean
 #pragma unroll
