@@ -869,6 +869,35 @@ def run_serve(args):
     print(json.dumps(out), flush=True)
 
 
+class Heartbeat:
+    """A host thread that sleeps 1 ms at a time and records every wake-up
+    that came more than 10 ms late: times when this process did not run (or
+    its interpreter lock was held) for that long.  Beside the requests'
+    latencies it tells a pause of the whole process from one of the GPU."""
+
+    def __init__(self, t0):
+        import threading
+        self.t0, self.gaps, self.stop = t0, [], False
+        self.th = threading.Thread(target=self.run, daemon=True)
+        self.th.start()
+
+    def run(self):
+        last = time.perf_counter()
+        while not self.stop:
+            time.sleep(0.001)
+            now = time.perf_counter()
+            if now - last > 0.010:
+                self.gaps.append((last - self.t0, (now - last) * 1e3))
+            last = now
+
+    def finish(self, k=5):
+        self.stop = True
+        self.th.join()
+        return {"late_wakeups_over_10ms": len(self.gaps),
+                "largest": [{"at_s": float(a), "gap_ms": float(g)}
+                            for a, g in sorted(self.gaps, key=lambda v: -v[1])[:k]]}
+
+
 def serve_at(args, L, tm, machines, pools, rng, rate, requests=None):
     import ctypes
     import threading
@@ -900,6 +929,7 @@ def serve_at(args, L, tm, machines, pools, rng, rate, requests=None):
             nwarm += 1
     ids = [0] * nreq
     t0 = time.perf_counter()
+    hb = Heartbeat(t0)
 
     def submit():
         for i in range(nreq):
@@ -930,10 +960,12 @@ def serve_at(args, L, tm, machines, pools, rng, rate, requests=None):
         acc_sizes.append(int(sizes[i]))
         acc_arrive.append(arrive[i])
     makespan = float(np.max(np.array(acc_arrive) + np.array(lat) / 1e3))
+    host_server = hb.finish()
     L.tm_serve_close(srv)
     # serial per-request predict under the same arrivals
     lat_s = []
     t0 = time.perf_counter()
+    hb = Heartbeat(t0)
     for i in range(nreq):
         d = t0 + arrive[i] - time.perf_counter()
         if d > 0:
@@ -941,6 +973,7 @@ def serve_at(args, L, tm, machines, pools, rng, rate, requests=None):
         machines[which[i]].predict(inputs[i], int(sizes[i]))
         lat_s.append((time.perf_counter() - (t0 + arrive[i])) * 1e3)
     t_end_s = time.perf_counter()
+    host_serial = hb.finish()
     total = int(sizes.sum())
     out = {
         "metric": "serve p99 ms", "value": float(np.percentile(lat, 99)), "unit": "ms",
@@ -970,6 +1003,9 @@ def serve_at(args, L, tm, machines, pools, rng, rate, requests=None):
         "phase_p99_ms": {k: float(np.percentile([p[i] for p in phases], 99))
                          for i, k in enumerate(("queue", "host_launch", "device",
                                                 "launch_gpu_span"))},
+        # late wake-ups of a 1 ms host heartbeat while the server ran and
+        # while the serial form ran (seconds from each form's start)
+        "host_heartbeat": {"server": host_server, "serial": host_serial},
         "offered_samples_per_s": float(sizes.sum() / arrive[-1]),
         "samples_per_s": float(sum(acc_sizes)) / makespan,
         "serial": {"p50_ms": float(np.percentile(lat_s, 50)),
