@@ -40,6 +40,24 @@ def test_python_mirror_lists_every_declared_symbol():
     assert set(declared()) == set(tm.EXPORTS)
 
 
+def test_python_mirror_types_every_argument():
+    """Every entry point that takes arguments has its ctypes argument types
+    set in the mirror (an untyped pointer argument would be converted as a
+    C int), with as many types as the header declares parameters."""
+    import santoku_tsetlin as tm
+    txt = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    L = tm.lib()
+    for name in declared():
+        m = re.search(r"\b%s\s*\(([^)]*)\)" % name, txt)
+        params = m.group(1).strip()
+        n = 0 if params in ("", "void") else params.count(",") + 1
+        f = getattr(L, name)
+        if n == 0:
+            assert not f.argtypes, name
+        else:
+            assert f.argtypes is not None and len(f.argtypes) == n, (name, n, f.argtypes)
+
+
 def test_align_and_errors_without_gpu(so):
     import santoku_tsetlin as tm
     assert tm.lib().tm_align() == 8 == tm.align
