@@ -4,6 +4,8 @@ TEST INFRASTRUCTURE ONLY (the checker for tm_class_accuracy,
 tm_encoding_accuracy, tm_bits_to_cvec and tm_bits_to_cvec_ind).  Counting uses numpy; the
 floating-point finish is a plain Python loop in the reference's order, so
 every operation rounds once, as in the reference's C without contraction.
+The two metrics are pinned to the reference's own functions, compiled by
+eval_harness.c (fixtures in tests/golden/evaluator.npz).
 """
 import math
 

@@ -6,8 +6,14 @@
   actions, count planes, vote sums, predictions, persisted bytes.
 * Where the reference harness is built (oracle/_ref), random machines
   cross-checked oracle vs reference code in both draw modes.
+* The evaluator restatement (oracle/evaluator_ref.py, the checker of the
+  device metrics) against the reference's own tm_class_accuracy and
+  tm_encoding_accuracy (evaluator/capi.c:119-202, 497-574): bit for bit on
+  the fixtures tests/golden/make_golden_evaluator.py recorded from them,
+  and, where the evaluator harness is built (oracle/_ref/libeval_ref.so),
+  on fresh random cases.
 """
-import glob
+import ctypes
 import hashlib
 import os
 import sys
@@ -21,7 +27,6 @@ from cases import CASES, make_inputs  # noqa: E402
 
 import oracle as O  # noqa: E402
 
-FIXTURES = sorted(glob.glob(os.path.join(HERE, "golden", "*.npz")))
 
 
 def test_philox_known_answers(oracle_lib):
@@ -162,3 +167,65 @@ def test_bits_to_cvec_ind_restatement_matches_fixture_layout(case):
         got, doff = R.bits_to_cvec_ind(np.concatenate(lists), io, fo, n, True)
         assert np.array_equal(doff[:-1], offs)
         assert np.array_equal(got, x)
+
+
+def _class_vec(r):
+    return np.array([r["precision"], r["recall"], r["f1"]] +
+                    [v for c in r["classes"] for v in (c["precision"], c["recall"], c["f1"])])
+
+
+def _enc_vec(r):
+    return np.array([r["mean_hamming"], r["ber_min"], r["ber_max"], r["ber_std"]] + r["bits"])
+
+
+def test_evaluator_restatement_matches_reference_fixtures():
+    """Every recorded case of the reference's evaluator reproduced to the
+    last bit: per-class and macro precision / recall / F1 (out-of-range
+    predictions and labels skipped, classes without support at 0), and
+    mean Hamming accuracy, the per-bit error rates, their extremes and
+    standard deviation (one bit: 0)."""
+    import evaluator_ref as R
+    z = np.load(os.path.join(HERE, "golden", "evaluator.npz"))
+    kinds = {"class": (R.class_accuracy, _class_vec), "enc": (R.encoding_accuracy, _enc_vec)}
+    seen = 0
+    for key in sorted(k for k in z.files if k.endswith("_out")):
+        kind, k = key.split("_")[:2]
+        fn, vec = kinds[kind]
+        n, dims = (int(v) for v in z["%s_%s_meta" % (kind, k)])
+        got = vec(fn(z["%s_%s_pred" % (kind, k)], z["%s_%s_true" % (kind, k)], n, dims))
+        assert np.array_equal(got, z[key]), key
+        seen += 1
+    assert seen >= 14
+
+
+EVAL_SO = os.path.join(os.path.dirname(HERE), "oracle", "_ref", "libeval_ref.so")
+
+
+@pytest.mark.skipif(not os.path.exists(EVAL_SO), reason="evaluator harness not built")
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_evaluator_restatement_vs_reference_random(seed):
+    import evaluator_ref as R
+    L = ctypes.CDLL(EVAL_SO)
+    vp = ctypes.c_void_p
+    rng = np.random.default_rng(seed)
+    for _ in range(40):
+        classes, n = int(rng.integers(1, 50)), int(rng.integers(1, 4000))
+        yt = rng.integers(0, classes + 1, size=n).astype(np.int64)
+        yp = np.where(rng.random(n) < rng.random(), yt,
+                      rng.integers(-3, classes + 3, size=n)).astype(np.int64)
+        out = np.zeros(3 + 3 * classes)
+        L.ref_eval_class_accuracy(yp.ctypes.data_as(vp), yt.ctypes.data_as(vp),
+                                  ctypes.c_uint32(n), ctypes.c_uint32(classes),
+                                  out.ctypes.data_as(vp))
+        assert np.array_equal(_class_vec(R.class_accuracy(yp, yt, n, classes)), out)
+        hidden, n = int(rng.integers(1, 400)), int(rng.integers(1, 2000))
+        nb = (hidden + 7) // 8
+        e = rng.integers(0, 256, size=n * nb, dtype=np.uint8)
+        p = e.copy()
+        sel = rng.random(n * nb) < rng.random()
+        p[sel] ^= rng.integers(1, 256, size=int(sel.sum()), dtype=np.uint8)
+        out = np.zeros(4 + hidden)
+        L.ref_eval_encoding_accuracy(p.ctypes.data_as(vp), e.ctypes.data_as(vp),
+                                     ctypes.c_uint32(n), ctypes.c_uint32(hidden),
+                                     out.ctypes.data_as(vp))
+        assert np.array_equal(_enc_vec(R.encoding_accuracy(p, e, n, hidden)), out)
