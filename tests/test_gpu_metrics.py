@@ -1,7 +1,8 @@
 """Device evaluator metrics and input packing against their CPU
 restatements (oracle/evaluator_ref.py): counts exact, doubles equal to the
 last bit (both evaluate the reference's formulas in its order with one
-rounding per operation), packed rows bit-exact."""
+rounding per operation), packed rows bit-exact; and the metrics against the
+outputs recorded from the reference's own evaluator functions."""
 import numpy as np
 import pytest
 
@@ -31,6 +32,29 @@ def test_encoding_accuracy(tm, n, hidden):
     got = tm.encoding_accuracy(p, e, n, hidden)
     want = R.encoding_accuracy(p, e, n, hidden)
     assert got == want
+
+
+def test_metrics_match_reference_fixtures(tm):
+    """The device metrics against the outputs recorded from the reference's
+    own tm_class_accuracy and tm_encoding_accuracy (evaluator/capi.c:119-202,
+    497-574; tests/golden/make_golden_evaluator.py): every number equal, on
+    cases with out-of-range predictions, a class without support, one class,
+    one hidden bit and codes with no or every byte changed."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                             "evaluator.npz"))
+    for key in sorted(k for k in z.files if k.endswith("_out")):
+        kind, k = key.split("_")[:2]
+        n, dims = (int(v) for v in z["%s_%s_meta" % (kind, k)])
+        p, t = z["%s_%s_pred" % (kind, k)], z["%s_%s_true" % (kind, k)]
+        if kind == "class":
+            r = tm.class_accuracy(p, t, n, dims)
+            got = [r["precision"], r["recall"], r["f1"]] + \
+                [v for c in r["classes"] for v in (c["precision"], c["recall"], c["f1"])]
+        else:
+            r = tm.encoding_accuracy(p, t, n, dims)
+            got = [r["mean_hamming"], r["ber_min"], r["ber_max"], r["ber_std"]] + list(r["bits"])
+        assert np.array_equal(np.array(got, dtype=np.float64), z[key]), key
 
 
 @pytest.mark.parametrize("n,features,flip", [(3, 5, True), (100, 784, True), (57, 100, False),
