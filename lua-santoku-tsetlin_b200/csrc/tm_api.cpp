@@ -71,19 +71,6 @@ extern "C" const char *tm_last_error(void) { return g_err.c_str(); }
 extern "C" uint32_t tm_align(void) { return 8; }
 extern "C" void tm_free(void *p) { free(p); }
 
-struct DevGuard {
-  int prev = -1;
-  explicit DevGuard(int d) {
-    cudaGetDevice(&prev);
-    if (prev != d) cudaSetDevice(d);
-  }
-  ~DevGuard() {
-    int cur;
-    cudaGetDevice(&cur);
-    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
-  }
-};
-
 // Grow-only device buffer.
 struct DevBuf {
   void *p = nullptr;

@@ -287,6 +287,25 @@ struct MachineView {
   int act8_kind;        // their TM_GEMM_* encoding
 };
 
+// Makes `d` the calling thread's current device for the guard's scope and
+// gives the caller's device back at its end (an entry point leaves the
+// caller's current device as it found it).  `err` is the result of
+// switching.
+struct DevGuard {
+  int prev = -1;
+  cudaError_t err = cudaSuccess;
+  explicit DevGuard(int d) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != d) err = cudaSetDevice(d);
+  }
+  ~DevGuard() {
+    int cur;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+  DevGuard(const DevGuard &) = delete;
+  DevGuard &operator=(const DevGuard &) = delete;
+};
+
 }  // namespace tmb
 
 struct tm_machine;

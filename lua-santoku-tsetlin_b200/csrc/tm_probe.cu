@@ -92,7 +92,8 @@ int time_peak(K kern, int sms, uint32_t iters, uint32_t *d_out, double *ops_per_
 
 extern "C" int tm_int_peaks(int32_t device, double *out) {
   if (!out) return tmb_fail(TM_ERR_ARG, "int_peaks: null output");
-  if (cudaSetDevice(device) != cudaSuccess) return tmb_fail(TM_ERR_CUDA, "int_peaks: bad device");
+  tmb::DevGuard guard(device);
+  if (guard.err != cudaSuccess) return tmb_fail(TM_ERR_CUDA, "int_peaks: bad device");
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   if (sms <= 0) return tmb_fail(TM_ERR_CUDA, "int_peaks: no multiprocessors");

@@ -372,6 +372,7 @@ static void stop_threads(tm_server *s) {
 
 static void free_server(tm_server *s) {
   stop_threads(s);
+  DevGuard guard(s->cfg.device);
   for (Slot &sl : s->slots) {
     if (sl.ev0) cudaEventDestroy(sl.ev0);
     if (sl.ev1) cudaEventDestroy(sl.ev1);
@@ -403,7 +404,7 @@ extern "C" int tm_serve_open(const tm_server_config *cfg, tm_machine *const *mac
   if (!s->cfg.max_batch_samples) s->cfg.max_batch_samples = 8192;
   if (!s->cfg.max_inflight) s->cfg.max_inflight = 4;
   if (!s->cfg.max_queued_samples) s->cfg.max_queued_samples = 64ull * s->cfg.max_batch_samples;
-  cudaSetDevice(s->cfg.device);
+  DevGuard guard(s->cfg.device);
   for (uint32_t i = 0; i < count; i++) {
     MachineView v{};
     int rc = tmb_machine_view(machines[i], &v, "serving");

@@ -459,7 +459,8 @@ extern "C" int tm_class_accuracy(const int64_t *predicted, const int64_t *expect
                                  uint32_t classes, int32_t on_device, int32_t device, double *out) {
   if (!out || (n && (!predicted || !expected))) return tmb_fail(TM_ERR_ARG, "class_accuracy: bad arguments");
   if (classes == 0) return tmb_fail(TM_ERR_ARG, "class_accuracy: n_classes must be > 0");
-  CKU(cudaSetDevice(device));
+  tmb::DevGuard guard(device);
+  CKU(guard.err);
   DevScratch buf;
   const size_t cnt = 3 * (size_t)classes * 8, outb = (3 + 3 * (size_t)classes) * 8;
   const size_t inb = on_device ? 0 : 2 * n * 8;
@@ -486,7 +487,8 @@ extern "C" int tm_encoding_accuracy(const uint8_t *predicted, const uint8_t *exp
                                     uint32_t hidden, int32_t on_device, int32_t device, double *out) {
   if (!out || !n || !predicted || !expected) return tmb_fail(TM_ERR_ARG, "encoding_accuracy: bad arguments");
   if (hidden == 0) return tmb_fail(TM_ERR_ARG, "encoding_accuracy: n_hidden must be > 0");
-  CKU(cudaSetDevice(device));
+  tmb::DevGuard guard(device);
+  CKU(guard.err);
   const uint64_t nb = (hidden + 7) / 8;
   DevScratch buf;
   const size_t cnt = (size_t)hidden * 8, outb = (4 + (size_t)hidden) * 8;
@@ -514,7 +516,8 @@ extern "C" int tm_bits_to_cvec(const int64_t *set_bits, uint64_t n_set, uint64_t
                                uint32_t features, int32_t flip, int32_t on_device, int32_t device,
                                uint8_t *out) {
   if (!out || (n_set && !set_bits) || features == 0) return tmb_fail(TM_ERR_ARG, "bits_to_cvec: bad arguments");
-  CKU(cudaSetDevice(device));
+  tmb::DevGuard guard(device);
+  CKU(guard.err);
   const uint64_t row_bits = flip ? 2ull * features : features;
   const uint32_t nb = (uint32_t)((row_bits + 7) / 8);
   const uint32_t rw = (uint32_t)((row_bits + 31) / 32);
@@ -570,7 +573,8 @@ extern "C" int tm_bits_to_cvec_ind(const int64_t *set_bits, const int64_t *ind_o
   if (out_cap < bytes) return tmb_fail(TM_ERR_ARG, "bits_to_cvec_ind: output too small");
   const uint64_t n_set = (uint64_t)(ind_offsets[dims] - ind_offsets[0]);
   if (n_set && !set_bits) return tmb_fail(TM_ERR_ARG, "bits_to_cvec_ind: bad arguments");
-  CKU(cudaSetDevice(device));
+  tmb::DevGuard guard(device);
+  CKU(guard.err);
   DevScratch buf;
   const size_t meta_b = meta.size() * 8, stage_b = ((words * 4 + 255) / 256) * 256;
   const size_t idx_b = on_device ? 0 : n_set * 8, out_b = on_device ? 0 : bytes;
