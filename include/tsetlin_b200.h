@@ -17,7 +17,8 @@
  *   - Buffers belong to the caller.  `on_device` = 1 means the pointers are
  *     CUDA device pointers on the machine's device; 0 means host memory.
  *   - A machine lives on one device.  Calls on one machine are not
- *     thread-safe; calls on different machines are.
+ *     thread-safe; calls on different machines are.  Every entry point
+ *     leaves the calling thread's current CUDA device as it found it.
  */
 #ifndef TSETLIN_B200_H
 #define TSETLIN_B200_H
