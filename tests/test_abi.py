@@ -90,3 +90,23 @@ def test_load_rejects_bad_data(so):
         tm.load(np.array([0, 0, 0, 0, 1, 0], dtype=np.uint8).tobytes(), True)
     with pytest.raises(tm.TsetlinError, match="cannot open"):
         tm.load("/nonexistent/model.bin")
+
+
+def test_package_fails_loudly_without_the_library(tmp_path):
+    """The package has no CPU fallback: without the built CUDA library every
+    call raises instead of computing something another way."""
+    import subprocess
+    import sys
+    code = (
+        "import sys; sys.path.insert(0, %r)\n"
+        "import santoku_tsetlin as tm\n"
+        "tm.LIB_PATH = %r\n"
+        "try:\n"
+        "    tm.create('classifier', dict(classes=2, features=8, clauses=8,\n"
+        "              clause_tolerance=4, clause_maximum=4, specificity=2.0))\n"
+        "except tm.TsetlinError as e:\n"
+        "    print('RAISED', e)\n"
+    ) % (os.path.join(ROOT, "lua-santoku-tsetlin_b200"), str(tmp_path / "missing.so"))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "RAISED" in r.stdout and "not built" in r.stdout
