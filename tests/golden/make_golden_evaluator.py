@@ -96,7 +96,8 @@ def main():
         rec["enc_%d_meta" % k] = np.array([n, hidden], dtype=np.int64)
         rec["enc_%d_out" % k] = ref_encoding(L, pred, true, n, hidden)
     np.savez_compressed(os.path.join(HERE, "evaluator.npz"), **rec)
-    print("wrote", os.path.join(HERE, "evaluator.npz"), len(rec) // 4 * 1, "cases")
+    print("wrote", os.path.join(HERE, "evaluator.npz"), len(CLASS_CASES) + len(ENC_CASES),
+          "cases")
 
 
 if __name__ == "__main__":
